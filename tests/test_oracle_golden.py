@@ -1,0 +1,154 @@
+"""Pin the CPU oracle against golden vectors produced by the reference itself."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import entropy, fit, primitives, quadtree, rate, render
+from oracle.primitives import Prim, Record, prims_from_pack
+
+
+def _pack(g: dict, prefix: str) -> dict:
+    return {k[len(prefix):]: v for k, v in g.items() if k.startswith(prefix)}
+
+
+def render_cases(g):
+    pk = _pack(g, "p_")
+    for i in range(len(g["tile_size"])):
+        prims = prims_from_pack(pk, int(pk["offsets"][i]), int(pk["offsets"][i + 1]))
+        ts = int(g["tile_size"][i])
+        src_size = int(g["source_size"][i])
+        res = tuple(int(v) for v in g["residual"][i]) if g["has_residual"][i] else None
+        a, b = int(g["px_offsets"][i]), int(g["px_offsets"][i + 1])
+        yield i, prims, ts, src_size, res, g["image"][a:b].reshape(ts, ts, 3), float(g["mse"][i])
+
+
+def golden_src(i: int, ts: int) -> np.ndarray:
+    return np.random.default_rng(1000 + i).random((ts, ts, 3), dtype=np.float32)
+
+
+def test_render_tile_matches_reference_exactly(golden):
+    g = golden("render_tiles.npz")
+    n = 0
+    for i, prims, ts, src_size, res, want, mse in render_cases(g):
+        got = render.render_tile(prims, ts, residual_rgb=res, source_size=None if src_size == ts else src_size)
+        np.testing.assert_array_equal(got, want, err_msg=f"case {i}")
+        assert float(np.mean((golden_src(i, ts) - got) ** 2)) == mse
+        n += 1
+    assert n > 100
+
+
+def test_render_scene_matches_reference_exactly(golden):
+    g = golden("render_scene.npz")
+    for name in ("a", "b"):
+        w, h = (int(v) for v in g[f"{name}_dims"])
+        qts = [quadtree.QTile(int(x), int(y), int(s)) for x, y, s in g[f"{name}_qt"]]
+        pk = _pack(g, f"{name}_p_")
+        recs = [Record(prims_from_pack(pk, int(pk["offsets"][i]), int(pk["offsets"][i + 1])),
+                       tuple(int(v) for v in g[f"{name}_residual"][i])) for i in range(len(qts))]
+        res1 = list(g[f"{name}_res1"])
+        off = 0
+        for tw, th, use_res1 in g[f"{name}_targets"]:
+            img = render.render_scene_adaptive(recs, qts, w, h, res1 if use_res1 else None, 4, int(tw), int(th))
+            want = g[f"{name}_images"][off:off + img.size].reshape(img.shape)
+            off += img.size
+            np.testing.assert_array_equal(img, want, err_msg=f"{name} target {tw}x{th}")
+        assert off == g[f"{name}_images"].size
+
+
+def test_rate_model_matches_reference(golden):
+    g = golden("rate.npz")
+    for q, lam in zip(g["quality"], g["lam"]):
+        assert rate.tile_lambda(int(q)) == lam
+    np.testing.assert_array_equal(rate.LUT, g["lut"])
+    for kinds, (inc_res, inc_res1, grid), bits in zip(g["stack_kinds"], g["stack_meta"], g["bits"]):
+        prims = [Prim(int(k)) for k in kinds if k >= 0]
+        assert rate.estimate_bits(prims, bool(inc_res), bool(inc_res1), int(grid)) == bits
+    assert rate.tile_lambda(75) == pytest.approx(6.76e-5, rel=1e-12)
+
+
+def test_entropy_matches_reference_bit_exact(golden):
+    g = golden("entropy.npz")
+    pay, po, enc, eo = g["payload"], g["payload_off"], g["encoded"], g["encoded_off"]
+    for i in range(len(po) - 1):
+        data = pay[po[i]:po[i + 1]].tobytes()
+        want = enc[eo[i]:eo[i + 1]].tobytes()
+        assert entropy.encode_bytes(data) == want, f"payload {i}"
+        assert entropy.decode_bytes(want) == data
+    raw = g["prim_raw"].tobytes()
+    toc = [int(v) for v in g["toc"]]
+    for n, key in ((64, "64"), (7, "7")):
+        coded, entries = entropy.build_prim_chunks(raw, toc, n)
+        assert coded == g["coded" + key].tobytes()
+        assert [tuple(e) for e in entries] == [tuple(int(v) for v in e) for e in g["entries" + key]]
+        assert entropy.decode_prim_payload(coded, toc, entries) == raw
+
+
+def test_quantize_and_serialize_match_reference(golden):
+    g = golden("quant.npz")
+    a = _pack(g, "in_")
+    q = _pack(g, "q_")
+    n = len(a["kind"])
+    raw_prims = prims_from_pack(a, 0, n)
+    want_q = prims_from_pack(q, 0, n)
+    for p, w in zip(raw_prims, want_q):
+        got = primitives.quantize_primitive(p) if p.kind != 5 else p
+        assert got.kind == w.kind
+        assert got.geom == pytest.approx(w.geom, abs=0) and got.color0 == w.color0 and got.alpha == w.alpha
+        assert got.color1 == w.color1
+    counts = g["tile_counts"]
+    recs, k = [], 0
+    for c in counts:
+        recs.append(Record(raw_prims[k:k + int(c)]))
+        k += int(c)
+    blob, toc = primitives.encode_tiles(recs)
+    assert blob == g["tiles_raw"].tobytes()
+    assert toc == [int(v) for v in g["toc"]]
+    back = primitives.decode_tiles(blob, toc)
+    assert [len(r.primitives) for r in back] == [int(c) for c in counts]
+
+
+def test_quadtree_matches_reference(golden):
+    from weft_b200.synth import make_image_linear
+
+    g = golden("quadtree.npz")
+    for name in ("a", "b"):
+        w, h, n, seed = (int(v) for v in g[name + "_dims"])
+        img = make_image_linear(w, h, n, seed)
+        for thr in (0.12, 0.08, 0.03):
+            key = f"{name}_{int(thr * 100):02d}"
+            tiles = quadtree.decompose(img, split_threshold=thr, min_tile=8, max_tile=32)
+            np.testing.assert_array_equal(np.array([(t.x, t.y, t.size) for t in tiles], np.int32), g[key])
+            assert quadtree.pack_qtree(tiles) == g[key + "_packed"].tobytes()
+            assert [(t.x, t.y, t.size) for t in quadtree.unpack_qtree(g[key + "_packed"].tobytes())] == \
+                [tuple(int(v) for v in r) for r in g[key]]
+
+
+def _fit_inputs(g):
+    qt = g["qt"]
+    img = g["image"]
+    tiles = [quadtree.QTile(int(x), int(y), int(s)) for x, y, s in qt]
+    patches = quadtree.extract(img, tiles)
+    pool = _pack(g, "pool_")
+    pools = [prims_from_pack(pool, int(pool["offsets"][i]), int(pool["offsets"][i + 1])) for i in range(len(tiles))]
+    rs = _pack(g, "rs_")
+    reseeds: dict[int, list] = {}
+    for j, ti in enumerate(g["reseed_tile"]):
+        reseeds.setdefault(int(ti), []).append(prims_from_pack(rs, int(rs["offsets"][j]), int(rs["offsets"][j + 1])))
+    return tiles, patches, pools, reseeds
+
+
+@pytest.mark.parametrize("name", ["fit_small.npz", "fit_hq.npz"])
+def test_greedy_fit_matches_reference_selection(golden, name):
+    g = golden(name)
+    tiles, patches, pools, reseeds = _fit_inputs(g)
+    queue = {k: list(v) for k, v in reseeds.items()}
+
+    def reseed(i, patch, pred):
+        return queue[i].pop(0)
+
+    sel, cur, stats = fit.greedy_fit(patches, [t.size for t in tiles], pools, int(g["quality"]), reseed)
+    want = [[int(v) for v in row if v >= 0] for row in g["selected"]]
+    assert sel == want
+    assert all(len(v) == 0 for v in queue.values())

@@ -1,0 +1,117 @@
+"""ctypes binding of libweftk.so (the C ABI declared in include/weftk.h).
+
+The library is loaded lazily on first use.  There is no fallback: if the
+shared library is missing or no sm_100 GPU is present, the call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libweftk.so")
+
+
+class WeftkError(RuntimeError):
+    """Raised when a libweftk entry point returns a non-zero status."""
+
+
+class WeftPrim(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("geom", ctypes.c_float * 7), ("color0", ctypes.c_float * 3),
+                ("color1", ctypes.c_float * 3), ("alpha", ctypes.c_float)]
+
+
+class WeftEval(ctypes.Structure):
+    _fields_ = [("prim_offset", ctypes.c_int32), ("prim_count", ctypes.c_int32),
+                ("tile_offset", ctypes.c_int32), ("tile_size", ctypes.c_int32)]
+
+
+class WeftTileDecodeDesc(ctypes.Structure):
+    _fields_ = [("prim_offset", ctypes.c_int32), ("prim_count", ctypes.c_int32), ("target_x0", ctypes.c_int32),
+                ("target_y0", ctypes.c_int32), ("target_w", ctypes.c_int32), ("target_h", ctypes.c_int32),
+                ("source_size", ctypes.c_int32), ("res1_index", ctypes.c_int32), ("res0_r", ctypes.c_float),
+                ("res0_g", ctypes.c_float), ("res0_b", ctypes.c_float), ("_pad2", ctypes.c_float)]
+
+
+# numpy mirrors of the C structs (same byte layout)
+PRIM_DTYPE = np.dtype([("kind", np.int32), ("geom", np.float32, 7), ("color0", np.float32, 3),
+                       ("color1", np.float32, 3), ("alpha", np.float32)])
+EVAL_DTYPE = np.dtype([("prim_offset", np.int32), ("prim_count", np.int32), ("tile_offset", np.int32),
+                       ("tile_size", np.int32)])
+TILE_DECODE_DTYPE = np.dtype([("prim_offset", np.int32), ("prim_count", np.int32), ("target_x0", np.int32),
+                              ("target_y0", np.int32), ("target_w", np.int32), ("target_h", np.int32),
+                              ("source_size", np.int32), ("res1_index", np.int32), ("res0_r", np.float32),
+                              ("res0_g", np.float32), ("res0_b", np.float32), ("_pad2", np.float32)])
+assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
+assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
+assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+
+# name -> argtypes; every entry point returns int status
+SIGNATURES: dict[str, list] = {
+    "weftk_version": [],
+    "weftk_last_error": [ctypes.c_char_p, ctypes.c_size_t],
+    "weftk_init": [_I],
+    "weftk_device_status": [_P],
+    "weftk_score_evals": [_P, _I, _P, _P, _P, _I, _P],
+    "weftk_score_evals_host": [_P, _I, _P, _I, _P, _I64, _P, _I],
+    "weftk_render_tiles": [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _P],
+    "weftk_render_tiles_host": [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I],
+}
+
+_lock = threading.Lock()
+_lib = None
+_inited_devices: set[int] = set()
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libweftk.so and bind its entry points (no GPU needed)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise WeftkError(f"libweftk.so not found at {path}; run `python -m weft_b200.build`")
+        lib = ctypes.CDLL(path)
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    load().weftk_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise WeftkError(f"{what} failed with status {rc}: {last_error()}")
+
+
+def lib_for_device(device: int = 0) -> ctypes.CDLL:
+    """The bound library with `device` initialised (raises without an sm_100 GPU)."""
+    lib = load()
+    if device not in _inited_devices:
+        check(lib.weftk_init(int(device)), "weftk_init")
+        _inited_devices.add(device)
+    return lib
+
+
+def ptr(a) -> int:
+    """Address of a numpy array or torch tensor (0 for None)."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())

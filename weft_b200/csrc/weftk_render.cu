@@ -1,0 +1,261 @@
+// weftk_render.cu — generic per-eval scoring (batch_tile_objective replacement) and the
+// decoder's primitive walk (decode_tile_pixels / render_scene_adaptive replacement).
+//
+// Generic scoring: one warp per eval; each lane owns 4 pixels of a 128-pixel chunk and
+// composites the whole stack for them in registers; the per-lane squared error of a
+// chunk is summed in float32 and accumulated in float64; one warp reduction per eval.
+//
+// Decode walk: one 256-thread CTA per tile.  The tile's primitives are prepared once
+// into shared memory; warps stride over 128-pixel chunks of the tile's target rect.
+// Output is float32 HWC; consecutive lanes write consecutive pixels of a row.
+#include <cuda_runtime.h>
+
+#include "weftk_common.cuh"
+#include "weftk_prim.cuh"
+
+namespace weftk {
+
+__device__ int g_device_status = 0;  // first error code a kernel hit (0 = none)
+
+__device__ __forceinline__ void report(int code) { atomicCAS(&g_device_status, 0, code); }
+
+__device__ __forceinline__ WeftPrim load_prim(const WeftPrim* p) {
+    WeftPrim r;
+    const float* f = reinterpret_cast<const float*>(p);
+    r.kind = __ldg(reinterpret_cast<const int*>(p));
+#pragma unroll
+    for (int i = 0; i < 7; ++i) r.geom[i] = __ldg(f + 1 + i);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        r.color0[i] = __ldg(f + 8 + i);
+        r.color1[i] = __ldg(f + 11 + i);
+    }
+    r.alpha = __ldg(f + 14);
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+constexpr int SCORE_PPL = 4;
+
+__global__ void __launch_bounds__(256) score_evals_kernel(const WeftEval* __restrict__ evals, int n_evals,
+                                                          const WeftPrim* __restrict__ prims,
+                                                          const float* __restrict__ tiles, float* __restrict__ out,
+                                                          float off) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= n_evals) return;
+    const int4 e = __ldg(reinterpret_cast<const int4*>(evals) + warp);
+    const int ts = e.w, npix = ts * ts;
+    if (ts <= 0 || ts > 64 || e.y < 0) {
+        if (lane == 0) {
+            out[warp] = __int_as_float(0x7fc00000);
+            report(WEFTK_E_ARG);
+        }
+        return;
+    }
+    const float* src = tiles + e.z;
+    double acc = 0.0;
+    for (int base = 0; base < npix; base += 32 * SCORE_PPL) {
+        float fx[SCORE_PPL], fy[SCORE_PPL], cr[SCORE_PPL], cg[SCORE_PPL], cb[SCORE_PPL];
+#pragma unroll
+        for (int j = 0; j < SCORE_PPL; ++j) {
+            int p = base + j * 32 + lane;
+            fx[j] = (float)(p % ts) + off;
+            fy[j] = (float)(p / ts) + off;
+            cr[j] = cg[j] = cb[j] = 0.0f;
+        }
+        for (int k = 0; k < e.y; ++k) {
+            WeftPrim P = load_prim(prims + e.x + k);
+            Prep pr = prep_prim(P);
+            if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // the scorer never evaluates bicubic grids
+            float a[SCORE_PPL], sr[SCORE_PPL], sg[SCORE_PPL], sb[SCORE_PPL];
+            prim_eval<SCORE_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
+#pragma unroll
+            for (int j = 0; j < SCORE_PPL; ++j) {
+                cr[j] = blend(sr[j], a[j], cr[j]);
+                cg[j] = blend(sg[j], a[j], cg[j]);
+                cb[j] = blend(sb[j], a[j], cb[j]);
+            }
+        }
+        float part = 0.0f;
+#pragma unroll
+        for (int j = 0; j < SCORE_PPL; ++j) {
+            int p = base + j * 32 + lane;
+            if (p < npix) {
+                const float* s = src + 3 * p;
+                float dr = clamp01(cr[j]) - __ldg(s), dg = clamp01(cg[j]) - __ldg(s + 1),
+                      db = clamp01(cb[j]) - __ldg(s + 2);
+                part = fmaf(dr, dr, fmaf(dg, dg, fmaf(db, db, part)));
+            }
+        }
+        acc += (double)part;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) out[warp] = (float)(acc / (double)(3 * npix));
+}
+
+constexpr int DEC_PPL = 4;
+constexpr int DEC_THREADS = 256;
+constexpr int MAX_TILE_PRIMS = 48;
+
+__global__ void __launch_bounds__(DEC_THREADS) render_tiles_kernel(
+    const WeftTileDecodeDesc* __restrict__ descs, const WeftPrim* __restrict__ prims,
+    const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1, int n_res1, float* __restrict__ out,
+    int H, int W) {
+    __shared__ Prep sp[MAX_TILE_PRIMS];
+    __shared__ float grid[48];
+    __shared__ float ctrl[48];
+    const WeftTileDecodeDesc d = descs[blockIdx.x];
+    const int n = d.prim_count, w = d.target_w, h = d.target_h;
+    if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || d.source_size <= 0) {
+        if (threadIdx.x == 0) report(WEFTK_E_ARG);
+        return;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
+    const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
+    if (has_res1 && d.res1_index >= n_res1) {
+        if (threadIdx.x == 0) report(WEFTK_E_ARG);
+        return;
+    }
+    if (has_res1 && threadIdx.x < 48) grid[threadIdx.x] = res1[(size_t)d.res1_index * 48 + threadIdx.x];
+    __syncthreads();
+    const bool bic = (n == 1 && sp[0].kind == K_BICUBIC);
+    if (bic) {
+        const int gi = (int)sp[0].q[0];
+        if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
+            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            return;
+        }
+        if (threadIdx.x < 48) ctrl[threadIdx.x] = cp48[(size_t)gi * 48 + threadIdx.x];
+        __syncthreads();
+    }
+    const int side = max(w, h);
+    const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
+    const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int npix = w * h;
+    for (int base = warp * 32 * DEC_PPL; base < npix; base += nwarps * 32 * DEC_PPL) {
+        float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
+        int lx[DEC_PPL], ly[DEC_PPL];
+#pragma unroll
+        for (int j = 0; j < DEC_PPL; ++j) {
+            int p = base + j * 32 + lane;
+            lx[j] = p % w;
+            ly[j] = p / w;
+            fx[j] = __fmul_rn((float)lx[j] + 0.5f, step);
+            fy[j] = __fmul_rn((float)ly[j] + 0.5f, step);
+            cr[j] = cg[j] = cb[j] = 0.0f;
+        }
+        if (bic) {
+#pragma unroll
+            for (int j = 0; j < DEC_PPL; ++j) {
+                double by[4], bx[4];
+                bernstein4(ly[j] < side ? ly[j] : side - 1, side, by);
+                bernstein4(lx[j] < side ? lx[j] : side - 1, side, bx);
+                double o[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) {
+                        double m = 0.0;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) m = fma((double)ctrl[(r * 4 + c) * 3 + ch], bx[c], m);
+                        o[ch] = fma(by[r], m, o[ch]);
+                    }
+                }
+                cr[j] = clamp01((float)o[0]);
+                cg[j] = clamp01((float)o[1]);
+                cb[j] = clamp01((float)o[2]);
+            }
+        } else {
+            for (int k = 0; k < n; ++k) {
+                Prep pr = sp[k];
+                if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
+                float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
+                prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
+#pragma unroll
+                for (int j = 0; j < DEC_PPL; ++j) {
+                    cr[j] = blend(sr[j], a[j], cr[j]);
+                    cg[j] = blend(sg[j], a[j], cg[j]);
+                    cb[j] = blend(sb[j], a[j], cb[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < DEC_PPL; ++j) {
+            int p = base + j * 32 + lane;
+            if (p >= npix) continue;
+            float r = clamp01(cr[j] + d.res0_r), g = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
+            if (has_res1) {
+                // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
+                float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                float gy = fminf(fmaxf(__fsub_rn(__fmul_rn((float)ly[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                int x0 = (int)floorf(gx), y0 = (int)floorf(gy);
+                float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
+                int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
+                float v[3];
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) {
+                    float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
+                    float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
+                    float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
+                    float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
+                    v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
+                }
+                r = clamp01(r + v[0]);
+                g = clamp01(g + v[1]);
+                b = clamp01(b + v[2]);
+            }
+            int gxp = d.target_x0 + lx[j], gyp = d.target_y0 + ly[j];
+            if (gxp >= 0 && gxp < W && gyp >= 0 && gyp < H) {
+                float* o = out + ((size_t)gyp * W + gxp) * 3;
+                o[0] = r;
+                o[1] = g;
+                o[2] = b;
+            }
+        }
+    }
+}
+
+int launch_score_evals(const WeftEval* d_evals, int n_evals, const WeftPrim* d_prims, const float* d_tiles,
+                       float* d_mse, int flags, cudaStream_t stream) {
+    if (n_evals == 0) return WEFTK_OK;
+    WEFTK_REQUIRE(n_evals > 0 && d_evals && d_prims && d_tiles && d_mse, "score_evals: bad arguments");
+    const float off = (flags & WEFTK_SAMPLE_CORNER) ? 0.0f : 0.5f;
+    const int per_block = 256 / 32;
+    score_evals_kernel<<<ceil_div(n_evals, per_block), 256, 0, stream>>>(d_evals, n_evals, d_prims, d_tiles, d_mse,
+                                                                         off);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
+int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const WeftPrim* d_prims,
+                        const float* d_cp48, int n_cp48, const float* d_res1, int n_res1, float* d_out, int out_h,
+                        int out_w, cudaStream_t stream) {
+    if (n_tiles == 0) return WEFTK_OK;
+    WEFTK_REQUIRE(n_tiles > 0 && d_descs && d_out && out_h > 0 && out_w > 0, "render_tiles: bad arguments");
+    WEFTK_REQUIRE(n_cp48 >= 0 && n_res1 >= 0, "render_tiles: negative table size");
+    render_tiles_kernel<<<n_tiles, DEC_THREADS, 0, stream>>>(d_descs, d_prims, d_cp48, n_cp48, d_res1, n_res1, d_out,
+                                                             out_h, out_w);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
+int read_device_status(int* status, bool clear) {
+    int v = 0;
+    WEFTK_CUDA(cudaMemcpyFromSymbol(&v, g_device_status, sizeof(int)));
+    if (clear && v != 0) {
+        int z = 0;
+        WEFTK_CUDA(cudaMemcpyToSymbol(g_device_status, &z, sizeof(int)));
+    }
+    *status = v;
+    return WEFTK_OK;
+}
+
+}  // namespace weftk

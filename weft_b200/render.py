@@ -1,0 +1,141 @@
+"""Decoder primitive walk on the GPU (host side).
+
+``render_scene_adaptive`` keeps the reference's signature and semantics
+(src/weft/render.py:270-358): each quadtree tile's stack is rendered into its
+integer target rect (edges ``round(x * scale)``), sampling the tile's
+``[0, size]`` primitive space at pixel centres of a square ``max(w, h)`` grid
+that is cropped for anisotropic targets; RES0 is added and clipped, then the
+bilinear RES1 grid, then clipped again.  All pixels are produced by
+``weftk_render_tiles`` (one launch for the whole image); the host only packs
+descriptors.
+
+``render_tile`` renders one stack as a single tile (the reference's
+``render_tile``, src/weft/render.py:127-234) through the same kernel.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from ._lib import PRIM_DTYPE, TILE_DECODE_DTYPE
+
+MAX_TILE_PRIMS = 48
+
+
+def pack_records(stacks) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+    """Pack per-tile primitive lists.
+
+    Returns (prims, offsets[n+1], cp48 table (m, 48), counts).  A kind-5
+    (bicubic) primitive carries its 48 control values in the cp48 table and
+    the table index in ``geom[0]``.
+    """
+    n_tot = sum(len(s) for s in stacks)
+    prims = np.zeros(max(1, n_tot), PRIM_DTYPE)
+    counts = np.array([len(s) for s in stacks], np.int64)
+    offsets = np.zeros(len(stacks) + 1, np.int64)
+    np.cumsum(counts, out=offsets[1:])
+    cps = []
+    k = 0
+    for s in stacks:
+        for p in s:
+            rec = prims[k]
+            rec["kind"] = p.kind
+            if p.kind == 5:
+                rec["geom"][0] = float(len(cps))
+                cps.append(np.asarray(p.geom, np.float32).reshape(48))
+            else:
+                g = tuple(p.geom)[:7]
+                rec["geom"][: len(g)] = g
+            rec["color0"] = p.color0
+            if p.color1 is not None:
+                rec["color1"] = p.color1
+            rec["alpha"] = p.alpha
+            k += 1
+    cp48 = np.stack(cps).astype(np.float32) if cps else np.zeros((0, 48), np.float32)
+    return prims, offsets, cp48, counts
+
+
+def res0_float(residual_rgb) -> tuple[float, float, float]:
+    """RES0 int8 bias -> float32 ``r / 255`` as the reference adds it (src/weft/render.py:231-232)."""
+    r = np.asarray(residual_rgb, np.float32) / np.float32(255.0)
+    return float(r[0]), float(r[1]), float(r[2])
+
+
+def tile_rect(qx: int, qy: int, size: int, sx: float, sy: float, scaled: bool) -> tuple[int, int, int, int]:
+    """Target rect of a quad tile (src/weft/render.py:321-334)."""
+    if not scaled:
+        return qx, qy, size, size
+    x0, y0 = int(round(qx * sx)), int(round(qy * sy))
+    x1, y1 = int(round((qx + size) * sx)), int(round((qy + size) * sy))
+    return x0, y0, max(1, x1 - x0), max(1, y1 - y0)
+
+
+def _launch(descs, prims, cp48, res1, out_h, out_w) -> np.ndarray:
+    lib = _lib.lib_for_device(0)
+    descs = np.ascontiguousarray(descs, TILE_DECODE_DTYPE)
+    prims = np.ascontiguousarray(prims, PRIM_DTYPE)
+    cp48 = np.ascontiguousarray(cp48, np.float32)
+    res1 = np.ascontiguousarray(res1, np.float32) if res1 is not None else np.zeros((0, 48), np.float32)
+    out = np.empty((out_h, out_w, 3), np.float32)
+    rc = lib.weftk_render_tiles_host(_lib.ptr(descs), len(descs), _lib.ptr(prims), len(prims), _lib.ptr(cp48),
+                                     len(cp48), _lib.ptr(res1), len(res1), _lib.ptr(out), out_h, out_w, 0)
+    _lib.check(rc, "weftk_render_tiles_host")
+    return out
+
+
+def build_scene(records, quad_tiles, width, height, residual_maps=None, target_width=None, target_height=None):
+    """Descriptor arrays for a scene; returns (descs, prims, cp48, res1, out_h, out_w)."""
+    tw = int(target_width) if target_width is not None else int(width)
+    th = int(target_height) if target_height is not None else int(height)
+    if tw <= 0 or th <= 0:
+        raise ValueError("target dimensions must be > 0")
+    sx, sy = tw / float(width), th / float(height)
+    scaled = not (tw == width and th == height)
+    prims, offsets, cp48, counts = pack_records([r.primitives for r in records])
+    if counts.size and counts.max() > MAX_TILE_PRIMS:
+        raise ValueError(f"a tile has more than {MAX_TILE_PRIMS} primitives")
+    n = len(records)
+    descs = np.zeros(n, TILE_DECODE_DTYPE)
+    rects = np.array([tile_rect(q.x, q.y, q.size, sx, sy, scaled) for q in quad_tiles[:n]], np.int64).reshape(-1, 4)
+    descs["prim_offset"] = offsets[:-1]
+    descs["prim_count"] = counts
+    descs["target_x0"], descs["target_y0"] = rects[:, 0], rects[:, 1]
+    descs["target_w"], descs["target_h"] = rects[:, 2], rects[:, 3]
+    descs["source_size"] = [q.size for q in quad_tiles[:n]]
+    res0 = np.array([r.residual_rgb for r in records], np.float32).reshape(-1, 3) / np.float32(255.0)
+    descs["res0_r"], descs["res0_g"], descs["res0_b"] = res0[:, 0], res0[:, 1], res0[:, 2]
+    res1 = None
+    if residual_maps is not None:
+        m = min(len(residual_maps), n)
+        res1 = np.stack([np.asarray(residual_maps[i], np.float32).reshape(48) for i in range(m)]) if m else None
+        descs["res1_index"] = [i if i < m else -1 for i in range(n)]
+    else:
+        descs["res1_index"] = -1
+    return descs, prims, cp48, res1, th, tw
+
+
+def render_scene_adaptive(records, quad_tiles, width: int, height: int, residual_maps=None,
+                          res1_grid_size: int = 4, target_width: int | None = None,
+                          target_height: int | None = None) -> np.ndarray:
+    """GPU render of a quadtree scene; returns (target_h, target_w, 3) float32 in [0, 1]."""
+    if residual_maps is not None and res1_grid_size != 4:
+        raise ValueError("only 4x4 RES1 grids are supported")
+    descs, prims, cp48, res1, th, tw = build_scene(records, quad_tiles, width, height, residual_maps,
+                                                   target_width, target_height)
+    return _launch(descs, prims, cp48, res1, th, tw)
+
+
+def render_tile(prims, tile_size: int, residual_rgb=None, source_size: int | None = None) -> np.ndarray:
+    """GPU render of one stack as a single tile (clipped, with optional RES0)."""
+    ts = int(tile_size)
+    src = int(source_size) if source_size is not None else ts
+    p, offs, cp48, counts = pack_records([list(prims)])
+    d = np.zeros(1, TILE_DECODE_DTYPE)
+    d["prim_count"] = counts[0]
+    d["target_w"] = d["target_h"] = ts
+    d["source_size"] = src
+    d["res1_index"] = -1
+    if residual_rgb is not None:
+        d["res0_r"], d["res0_g"], d["res0_b"] = res0_float(residual_rgb)
+    return _launch(d, p, cp48, None, ts, ts)

@@ -1,0 +1,107 @@
+/*
+ * weftk_fit.h — device-resident greedy candidate-scoring fit (C ABI of libweftk.so).
+ *
+ * Replaces the greedy loop of the reference's adaptive fit
+ * (src/weft/encoder.py:2668-2831, _fit_adaptive_state), whose every round was a
+ * host->device copy, a batch_tile_objective launch, a device->host copy and a
+ * host argmin.  Here all tiles' pixels, candidate pools, selections and
+ * objectives stay in device memory; one call runs one round for every tile.
+ *
+ * Memory is owned by the caller (all pointers below are device pointers) and
+ * laid out tile-major:
+ *   pixels     float4 (r, g, b, 0) per pixel, each tile's ts*ts pixels
+ *              row-major starting at px_off[t];
+ *   candidates tile t owns slots [pool_off[t], pool_off[t] + pool_cap[t]) of
+ *              every candidate array; the first pool_cnt[t] are filled
+ *              (original order = tie-break order, as in the reference).
+ *
+ * Round semantics (mode WEFTK_FIT_ROUND), per tile with flag COMPLEX, at least
+ * one live candidate and fewer than cap[t] selected primitives:
+ *   mse_k = mean over pixels and channels of (clip(cand_k over bg) - src)^2
+ *   obj_k = mse_k + f32(lambda) * f32(sel_bits + 8 * bytes[kind_k])  (float32)
+ *   k* = first argmin; accept if (double)obj_k* < cur_obj[t].
+ * An accepted candidate is composited into bg, appended to sel, its slot marked
+ * dead, sel_bits and cur_obj updated.  If any tile improved, COMPLEX becomes
+ * "improved this round"; otherwise COMPLEX is unchanged (the caller re-seeds).
+ * Mode WEFTK_FIT_INIT scores every live candidate alone over black, accepts
+ * each tile's argmin unconditionally, sets cur_obj = (double)mse + lambda*bits
+ * and COMPLEX = cur_obj > complex_threshold and a live candidate remains.
+ */
+#ifndef WEFTK_FIT_H
+#define WEFTK_FIT_H
+
+#include "weftk.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WEFTK_FIT_INIT 0
+#define WEFTK_FIT_ROUND 1
+
+#define WEFTK_TILE_COMPLEX 1
+#define WEFTK_TILE_EVAL 2
+#define WEFTK_TILE_IMPROVED 4
+
+/* Byte size of a candidate's kind on the wire; bits per primitive = 8 * this
+ * (src/weft/encoder.py:242-256: 7, 18, 17, 21, 19, everything else 20). */
+#define WEFTK_PRIM_BYTES {7, 18, 17, 21, 19, 20, 20, 20}
+
+typedef struct WeftFitState {
+    int32_t n_tiles;
+    int32_t cap_max;         /* row stride of sel[] */
+    int64_t n_slots;         /* candidate slots in total */
+    /* tiles */
+    const float* src;        /* float4 per pixel */
+    float* bg;               /* float4 per pixel: composite of the selected stack */
+    const int32_t* px_off;   /* [n_tiles] pixel offset of the tile */
+    const int32_t* size;     /* [n_tiles] tile side: 8, 16, 32 or 64 */
+    const int32_t* cap;      /* [n_tiles] primitive cap */
+    const int32_t* pool_off; /* [n_tiles] first slot */
+    const int32_t* pool_cnt; /* [n_tiles] filled slots */
+    int32_t* n_alive;        /* [n_tiles] live candidates */
+    int32_t* n_sel;          /* [n_tiles] selected primitives */
+    int32_t* sel_bits;       /* [n_tiles] 8 + sum of 8 * bytes[kind] over the selection */
+    int32_t* flags;          /* [n_tiles] WEFTK_TILE_* bits */
+    double* cur_obj;         /* [n_tiles] current objective */
+    int32_t* sel;            /* [n_tiles * cap_max] selected slot indices (pool-local) */
+    /* candidates (slot-indexed) */
+    const WeftPrim* cand;    /* [n_slots] candidate records */
+    float* prep;             /* [n_slots * 16] prepared per-candidate terms (64 B each) */
+    uint8_t* alive;          /* [n_slots] 1 = still in the pool */
+    float* partial;          /* [n_slots * 4] per-1024-pixel-block squared-error sums (scratch) */
+    int32_t* status;         /* [4] round counters: evaluated tiles, improved tiles */
+} WeftFitState;
+
+/* A unit of scoring work: tile, 1024-pixel block, and a run of candidate
+ * slots (pool-local, into perm). */
+typedef struct WeftFitItem {
+    int32_t tile;
+    int32_t block;
+    int32_t first;
+    int32_t count;
+} WeftFitItem;
+
+/* Prepare candidate slots [pool_off[t] + lo, pool_off[t] + pool_cnt[t]) of every
+ * tile whose slot range changed: compute the prepared terms and mark them live.
+ * first_new[t] = first pool-local slot to prepare (pass pool_cnt[t] to skip). */
+int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_new, void* stream);
+
+/*
+ * Run one fit round over all tiles.
+ *   d_perm     [n_slots] pool-local scoring order of each tile's slots (any
+ *              permutation; ties are broken by slot index, not by perm)
+ *   d_items_*  scoring work for tiles of side 8, 16, and >= 32 (block-split)
+ *   lambda     rate weight (_tile_lambda of the quality)
+ * Counters are written to st->status; read them after the stream syncs.
+ */
+int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double complex_threshold,
+                    const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
+                    const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32, int n_items32,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WEFTK_FIT_H */

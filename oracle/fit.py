@@ -48,7 +48,7 @@ def stack_mse(patch: np.ndarray, prims) -> np.float32:
     return np.float32(np.mean((patch - render.render_tile(prims, patch.shape[0])) ** 2))
 
 
-def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None):
+def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None, max_rounds=None):
     """Run the greedy; ``reseed(tile_index, patch, pred) -> list[Prim]``.
 
     Returns (selected index lists, current objectives (float64), stats dict).
@@ -76,7 +76,8 @@ def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None):
 
     thr = 0.00005 if quality >= 90 else 0.0005
     complex_tiles = [i for i in range(n) if cur[i] > thr and alive[i]]
-    max_rounds = 20 if quality >= 90 else 8 if quality >= 70 else 4
+    if max_rounds is None:
+        max_rounds = 20 if quality >= 90 else 8 if quality >= 70 else 4
     stalls = 0
     for _ in range(max_rounds):
         active = [i for i in complex_tiles if alive[i] and len(selected[i]) < caps[i]]

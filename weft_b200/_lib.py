@@ -37,6 +37,14 @@ class WeftTileDecodeDesc(ctypes.Structure):
                 ("res0_g", ctypes.c_float), ("res0_b", ctypes.c_float), ("_pad2", ctypes.c_float)]
 
 
+class WeftFitState(ctypes.Structure):
+    """Device pointers of a fit (include/weftk_fit.h)."""
+    _fields_ = [("n_tiles", ctypes.c_int32), ("cap_max", ctypes.c_int32), ("n_slots", ctypes.c_int64)] + [
+        (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "n_alive",
+                                       "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive",
+                                       "partial", "status")]
+
+
 # numpy mirrors of the C structs (same byte layout)
 PRIM_DTYPE = np.dtype([("kind", np.int32), ("geom", np.float32, 7), ("color0", np.float32, 3),
                        ("color1", np.float32, 3), ("alpha", np.float32)])
@@ -48,7 +56,9 @@ TILE_DECODE_DTYPE = np.dtype([("prim_offset", np.int32), ("prim_count", np.int32
                               ("res0_g", np.float32), ("res0_b", np.float32), ("_pad2", np.float32)])
 assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
 assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
+FIT_ITEM_DTYPE = np.dtype([("tile", np.int32), ("block", np.int32), ("first", np.int32), ("count", np.int32)])
 assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
+assert ctypes.sizeof(WeftFitState) == 16 + 18 * 8
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -64,6 +74,8 @@ SIGNATURES: dict[str, list] = {
     "weftk_score_evals_host": [_P, _I, _P, _I, _P, _I64, _P, _I],
     "weftk_render_tiles": [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _P],
     "weftk_render_tiles_host": [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I],
+    "weftk_fit_prepare": [_P, _P, _P],
+    "weftk_fit_round": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],
 }
 
 _lock = threading.Lock()

@@ -1,0 +1,306 @@
+// weftk_fit.cu — device-resident greedy candidate-scoring fit (see include/weftk_fit.h).
+//
+// Scoring exploits the greedy's structure: every eval of a round is "the tile's
+// selected stack + one candidate on top", and the over-composite is evaluated
+// back to front, so the selected stack's composite (bg) is kept per pixel in
+// HBM and each eval composites ONE primitive over it.  The float operations are
+// the same sequence a full re-render performs, so results are identical to
+// rendering the whole stack (blend() is shared with the decode walk).
+//
+// Work mapping (all CTAs are 128 threads = 4 warps; a warp works on one
+// candidate at a time, each lane owns PPL pixels held in registers):
+//   8-px tiles   PPL=2, one warp covers the tile, 4 independent warps per CTA
+//   16-px tiles  PPL=8, one warp covers the tile, 4 independent warps per CTA
+//   32/64-px     PPL=8, four warps cover a 1024-pixel block; a CTA scores a run
+//                of candidates on one block and combines the 4 warp sums in
+//                shared memory in a fixed order.
+// Per-candidate sums go to partial[slot*4 + block] (float32, fixed reduction
+// order, so results are deterministic run to run).
+#include <cuda_runtime.h>
+
+#include <climits>
+
+#include "../../include/weftk_fit.h"
+#include "weftk_common.cuh"
+#include "weftk_prim.cuh"
+
+namespace weftk {
+
+extern __device__ int g_device_status;
+__device__ __forceinline__ void fit_report(int code) { atomicCAS(&g_device_status, 0, code); }
+
+__constant__ int c_prim_bytes[8] = WEFTK_PRIM_BYTES;
+
+__device__ __forceinline__ int prim_bits(int kind) { return 8 * c_prim_bytes[(kind >= 0 && kind < 8) ? kind : 7]; }
+
+__device__ __forceinline__ Prep load_prep(const float* prep, long long slot) {
+    const float4* p = reinterpret_cast<const float4*>(prep) + slot * 4;
+    Prep r;
+    float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    r.kind = __float_as_int(a.x);
+    r.a = a.y;
+    r.cr = a.z;
+    r.cg = a.w;
+    r.cb = b.x;
+    r.q[0] = b.y; r.q[1] = b.z; r.q[2] = b.w;
+    r.q[3] = c.x; r.q[4] = c.y; r.q[5] = c.z; r.q[6] = c.w;
+    r.q[7] = d.x; r.q[8] = d.y; r.q[9] = d.z; r.q[10] = d.w;
+    return r;
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ prepare
+__global__ void fit_prepare_kernel(WeftFitState st, const int* __restrict__ first_new) {
+    const int t = blockIdx.x;
+    if (t >= st.n_tiles) return;
+    const int lo = first_new[t], hi = st.pool_cnt[t];
+    const long long off = st.pool_off[t];
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const long long slot = off + i;
+        const WeftPrim& P = st.cand[slot];
+        WeftPrim c;
+        c.kind = P.kind;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) c.geom[k] = P.geom[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            c.color0[k] = P.color0[k];
+            c.color1[k] = P.color1[k];
+        }
+        c.alpha = P.alpha;
+        Prep r = prep_prim(c);
+        if (r.kind == K_BICUBIC) r.kind = K_SKIP;  // bicubic grids are never fit candidates
+        float4* dst = reinterpret_cast<float4*>(st.prep) + slot * 4;
+        dst[0] = make_float4(__int_as_float(r.kind), r.a, r.cr, r.cg);
+        dst[1] = make_float4(r.cb, r.q[0], r.q[1], r.q[2]);
+        dst[2] = make_float4(r.q[3], r.q[4], r.q[5], r.q[6]);
+        dst[3] = make_float4(r.q[7], r.q[8], r.q[9], r.q[10]);
+        st.alive[slot] = 1;
+    }
+    if (threadIdx.x == 0 && hi > lo) st.n_alive[t] += hi - lo;
+}
+
+// ------------------------------------------------------------------ round begin / end
+__global__ void fit_begin_kernel(WeftFitState st, int mode) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= st.n_tiles) return;
+    int f = st.flags[t] & ~(WEFTK_TILE_EVAL | WEFTK_TILE_IMPROVED);
+    bool ev;
+    if (mode == WEFTK_FIT_INIT)
+        ev = st.n_alive[t] > 0;
+    else
+        ev = (f & WEFTK_TILE_COMPLEX) && st.n_alive[t] > 0 && st.n_sel[t] < st.cap[t];
+    if (ev) {
+        f |= WEFTK_TILE_EVAL;
+        atomicAdd(&st.status[0], 1);
+    }
+    st.flags[t] = f;
+}
+
+__global__ void fit_end_kernel(WeftFitState st, int mode, double complex_threshold) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= st.n_tiles) return;
+    int f = st.flags[t];
+    if (mode == WEFTK_FIT_INIT) {
+        bool cx = st.cur_obj[t] > complex_threshold && st.n_alive[t] > 0;
+        f = cx ? (f | WEFTK_TILE_COMPLEX) : (f & ~WEFTK_TILE_COMPLEX);
+    } else if (*(volatile int*)&st.status[1] > 0) {
+        f = (f & WEFTK_TILE_IMPROVED) ? (f | WEFTK_TILE_COMPLEX) : (f & ~WEFTK_TILE_COMPLEX);
+    }
+    st.flags[t] = f;
+}
+
+// ------------------------------------------------------------------ scoring
+template <int PPL, int WPC>
+__global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
+                                                        const WeftFitItem* __restrict__ items, int n_items,
+                                                        int expect_min, int expect_max) {
+    constexpr int GROUPS = 4 / WPC;
+    constexpr int MAX_RUN = 64;
+    __shared__ float red[MAX_RUN][WPC];
+    if ((int)blockIdx.x >= n_items) return;
+    const WeftFitItem w = items[blockIdx.x];
+    const int t = w.tile;
+    if (t < 0 || t >= st.n_tiles) {
+        if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
+        return;
+    }
+    if (!(st.flags[t] & WEFTK_TILE_EVAL)) return;
+    const int ts = st.size[t];
+    if (ts < expect_min || ts > expect_max || (WPC > 1 && w.count > MAX_RUN) || w.block * 1024 >= ts * ts ||
+        w.first < 0 || w.first + w.count > st.pool_cnt[t]) {
+        if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
+        return;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = warp / WPC, wig = warp % WPC;
+    const long long off = st.pool_off[t];
+    const float4* src = reinterpret_cast<const float4*>(st.src) + st.px_off[t];
+    const float4* bg = reinterpret_cast<const float4*>(st.bg) + st.px_off[t];
+    const int pbase = w.block * 1024 + wig * 32 * PPL;
+
+    float fx[PPL], fy[PPL];
+    float4 s[PPL], g[PPL];
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) {
+        const int p = pbase + j * 32 + lane;
+        fx[j] = (float)(p % ts) + 0.5f;
+        fy[j] = (float)(p / ts) + 0.5f;
+        s[j] = src[p];
+        g[j] = bg[p];
+    }
+    for (int c = group; c < w.count; c += GROUPS) {
+        const int local = perm[off + w.first + c];
+        const long long slot = off + local;
+        if (!st.alive[slot]) continue;
+        const Prep P = load_prep(st.prep, slot);
+        float a[PPL], sr[PPL], sg[PPL], sb[PPL];
+        prim_eval<PPL>(P, fx, fy, a, sr, sg, sb, lane);
+        float e = 0.0f;
+#pragma unroll
+        for (int j = 0; j < PPL; ++j) {
+            const float dr = clamp01(blend(sr[j], a[j], g[j].x)) - s[j].x;
+            const float dg = clamp01(blend(sg[j], a[j], g[j].y)) - s[j].y;
+            const float db = clamp01(blend(sb[j], a[j], g[j].z)) - s[j].z;
+            e = fmaf(dr, dr, fmaf(dg, dg, fmaf(db, db, e)));
+        }
+        e = warp_sum_f(e);
+        if (WPC == 1) {
+            if (lane == 0) st.partial[slot * 4] = e;
+        } else if (lane == 0) {
+            red[c][wig] = e;
+        }
+    }
+    if (WPC > 1) {
+        __syncthreads();
+        for (int c = threadIdx.x; c < w.count; c += blockDim.x) {
+            const long long slot = off + perm[off + w.first + c];
+            if (!st.alive[slot]) continue;
+            float e = red[c][0];
+#pragma unroll
+            for (int k = 1; k < WPC; ++k) e += red[c][k];
+            st.partial[slot * 4 + w.block] = e;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ select / accept
+__global__ void __launch_bounds__(128) fit_select_kernel(WeftFitState st, int mode, float lam_f, double lam_d) {
+    const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= st.n_tiles) return;
+    if (!(st.flags[t] & WEFTK_TILE_EVAL)) return;
+    const int ts = st.size[t], npix = ts * ts, nb = (npix + 1023) / 1024;
+    const long long off = st.pool_off[t];
+    const int cnt = st.pool_cnt[t];
+    const int base_bits = (mode == WEFTK_FIT_INIT) ? 8 : st.sel_bits[t];
+    const float denom = (float)(3 * npix);
+    float best = __int_as_float(0x7f800000);
+    int bi = INT_MAX;
+    for (int c = lane; c < cnt; c += 32) {
+        const long long slot = off + c;
+        if (!st.alive[slot]) continue;
+        float sse = st.partial[slot * 4];
+        for (int b = 1; b < nb; ++b) sse += st.partial[slot * 4 + b];
+        const float mse = __fdiv_rn(sse, denom);
+        const float obj = __fadd_rn(mse, __fmul_rn(lam_f, (float)(base_bits + prim_bits(st.cand[slot].kind))));
+        if (obj < best || (obj == best && c < bi)) {
+            best = obj;
+            bi = c;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(FULL, best, o);
+        const int oi = __shfl_xor_sync(FULL, bi, o);
+        if (ob < best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    if (bi == INT_MAX) return;
+    const bool accept = (mode == WEFTK_FIT_INIT) || ((double)best < st.cur_obj[t]);
+    if (!accept) return;
+    const long long slot = off + bi;
+    const int kind = st.cand[slot].kind;
+    if (lane == 0) {
+        const int k = st.n_sel[t];
+        if (k < st.cap_max) st.sel[(long long)t * st.cap_max + k] = bi;
+        else fit_report(WEFTK_E_RANGE);
+        st.n_sel[t] = k + 1;
+        st.n_alive[t] -= 1;
+        st.alive[slot] = 0;
+        const int bits = base_bits + prim_bits(kind);
+        st.sel_bits[t] = bits;
+        if (mode == WEFTK_FIT_INIT) {
+            float sse = st.partial[slot * 4];
+            for (int b = 1; b < nb; ++b) sse += st.partial[slot * 4 + b];
+            st.cur_obj[t] = (double)__fdiv_rn(sse, denom) + lam_d * (double)bits;
+        } else {
+            st.cur_obj[t] = (double)best;
+        }
+        st.flags[t] |= WEFTK_TILE_IMPROVED;
+        atomicAdd(&st.status[1], 1);
+    }
+    // Composite the accepted candidate into the tile's bg.
+    const Prep P = load_prep(st.prep, slot);
+    float4* bgp = reinterpret_cast<float4*>(st.bg) + st.px_off[t];
+    constexpr int U = 4;
+    for (int base = 0; base < npix; base += 32 * U) {
+        float fx[U], fy[U], a[U], sr[U], sg[U], sb[U];
+        float4 g[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int p = min(base + j * 32 + lane, npix - 1);
+            fx[j] = (float)(p % ts) + 0.5f;
+            fy[j] = (float)(p / ts) + 0.5f;
+            g[j] = bgp[p];
+        }
+        prim_eval<U>(P, fx, fy, a, sr, sg, sb, lane);
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int p = base + j * 32 + lane;
+            if (p < npix)
+                bgp[p] = make_float4(blend(sr[j], a[j], g[j].x), blend(sg[j], a[j], g[j].y),
+                                     blend(sb[j], a[j], g[j].z), 0.0f);
+        }
+    }
+}
+
+}  // namespace weftk
+
+using namespace weftk;
+
+extern "C" int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_new, void* stream) {
+    WEFTK_REQUIRE(st && d_first_new, "fit_prepare: null argument");
+    if (st->n_tiles == 0) return WEFTK_OK;
+    fit_prepare_kernel<<<st->n_tiles, 128, 0, (cudaStream_t)stream>>>(*st, d_first_new);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
+extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double complex_threshold,
+                               const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
+                               const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
+                               int n_items32, void* stream) {
+    WEFTK_REQUIRE(st && d_perm, "fit_round: null argument");
+    WEFTK_REQUIRE(mode == WEFTK_FIT_INIT || mode == WEFTK_FIT_ROUND, "fit_round: bad mode");
+    WEFTK_REQUIRE(n_items8 >= 0 && n_items16 >= 0 && n_items32 >= 0, "fit_round: negative item count");
+    if (st->n_tiles == 0) return WEFTK_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nt = st->n_tiles;
+    WEFTK_CUDA(cudaMemsetAsync(st->status, 0, 4 * sizeof(int32_t), s));
+    fit_begin_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(*st, mode);
+    if (n_items8) fit_score_kernel<2, 1><<<n_items8, 128, 0, s>>>(*st, d_perm, d_items8, n_items8, 8, 8);
+    if (n_items16) fit_score_kernel<8, 1><<<n_items16, 128, 0, s>>>(*st, d_perm, d_items16, n_items16, 16, 16);
+    if (n_items32) fit_score_kernel<8, 4><<<n_items32, 128, 0, s>>>(*st, d_perm, d_items32, n_items32, 32, 64);
+    fit_select_kernel<<<ceil_div(nt, 4), 128, 0, s>>>(*st, mode, (float)lambda, lambda);
+    fit_end_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(*st, mode, complex_threshold);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}

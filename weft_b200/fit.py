@@ -1,0 +1,303 @@
+"""Batched greedy candidate-scoring fit with all state resident on the GPU.
+
+Host side of ``include/weftk_fit.h``.  ``BatchedFit`` takes the tiles of one or
+many images and their candidate pools, uploads them once, and runs the
+reference's greedy (src/weft/encoder.py:2668-2831) with one
+``weftk_fit_round`` launch sequence per round for every tile at once:
+
+    init  : best single candidate per tile (accepted unconditionally)
+    rounds: score selected+candidate for every live candidate of every complex
+            tile, accept the argmin if it lowers the objective
+    stall : when no tile improved, re-seed the complex tiles that have room
+            with residual-targeted candidates (at most 3 times)
+
+Per round the host reads back 16 bytes of counters.  Candidate slots are
+sorted by kind for scoring (``perm``) so work items have uniform cost; the
+argmin still breaks ties by original pool order, as the reference's
+``np.argmin`` does.  Device memory comes from torch; the kernels come from
+libweftk.so (no fallback).
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib, rate
+from ._lib import FIT_ITEM_DTYPE, PRIM_DTYPE
+from .candidates import Cand, residual_candidates
+from .quadtree import MAX_PRIMS_BY_SIZE
+
+# FP32 operations per pixel to evaluate one primitive of each kind over a pixel
+# (the blend included); used to balance scoring work items.
+KIND_COST = np.array([10, 24, 28, 509, 26, 112, 10, 10], np.int64)
+RESEED_RESERVE = 3 * 128  # slots kept per tile for up to 3 re-seeds (<= 117 candidates each)
+CHUNK = {8: 128, 16: 64, 32: 32}
+FIT_INIT, FIT_ROUND = 0, 1
+TILE_COMPLEX, TILE_EVAL, TILE_IMPROVED = 1, 2, 4
+
+
+def pack_cands(cands) -> np.ndarray:
+    n = len(cands)
+    arr = np.zeros(n, PRIM_DTYPE)
+    if n == 0:
+        return arr
+    arr["kind"] = [c.kind for c in cands]
+    arr["alpha"] = [c.alpha for c in cands]
+    arr["color0"] = [tuple(c.color0) for c in cands]
+    arr["color1"] = [tuple(c.color1) if c.color1 is not None else (0.0, 0.0, 0.0) for c in cands]
+    arr["geom"] = [tuple(c.geom)[:7] + (0.0,) * (7 - min(7, len(c.geom))) for c in cands]
+    return arr
+
+
+def _dev(a: np.ndarray, device) -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device, non_blocking=False)
+
+
+@dataclass
+class FitStats:
+    rounds: int = 0
+    reseeds: int = 0
+    reseed_tiles: int = 0
+    evals: int = 0
+    launches: int = 0
+    t_reseed_s: float = 0.0
+    per_round: list = field(default_factory=list)
+
+
+class BatchedFit:
+    """All tiles of a fit, resident on one GPU."""
+
+    def __init__(self, patches, pools, quality: int = 75, caps=None, device: int = 0, reserve: int = RESEED_RESERVE):
+        self.device = torch.device("cuda", device)
+        self.lib = _lib.lib_for_device(device)
+        self.quality = int(quality)
+        self.lam = rate.tile_lambda(quality)
+        self.thr = rate.complexity_threshold(quality)
+        self.patches = [np.ascontiguousarray(p, np.float32) for p in patches]
+        n = len(self.patches)
+        self.n = n
+        self.sizes = np.array([p.shape[0] for p in self.patches], np.int32)
+        if np.any(~np.isin(self.sizes, (8, 16, 32, 64))):
+            raise ValueError("tile sizes must be 8, 16, 32 or 64")
+        self.caps = np.array(caps if caps is not None else [MAX_PRIMS_BY_SIZE.get(int(s), 48) for s in self.sizes],
+                             np.int32)
+        self.cap_max = int(self.caps.max()) if n else 1
+        self.pools: list[list] = [list(p) for p in pools]
+        cnt = np.array([len(p) for p in self.pools], np.int64)
+        self.pool_cap = cnt + reserve
+        self.pool_off = np.zeros(n, np.int64)
+        if n > 1:
+            np.cumsum(self.pool_cap[:-1], out=self.pool_off[1:])
+        self.n_slots = int(self.pool_cap.sum()) if n else 0
+        if self.n_slots >= 2 ** 31:
+            raise ValueError("too many candidate slots")
+        self.pool_cnt = cnt.astype(np.int32)
+        px = self.sizes.astype(np.int64) ** 2
+        self.px_off = np.zeros(n, np.int64)
+        if n > 1:
+            np.cumsum(px[:-1], out=self.px_off[1:])
+        n_px = int(px.sum())
+
+        d = self.device
+        src = np.zeros((n_px, 4), np.float32)
+        src[:, :3] = np.concatenate([p.reshape(-1, 3) for p in self.patches]) if n else np.zeros((0, 3))
+        self.t_src = _dev(src, d)
+        self.t_bg = torch.zeros((n_px, 4), dtype=torch.float32, device=d)
+        self.t_px_off = _dev(self.px_off.astype(np.int32), d)
+        self.t_size = _dev(self.sizes, d)
+        self.t_cap = _dev(self.caps, d)
+        self.t_pool_off = _dev(self.pool_off.astype(np.int32), d)
+        self.t_pool_cnt = _dev(self.pool_cnt, d)
+        self.t_n_alive = torch.zeros(n, dtype=torch.int32, device=d)
+        self.t_n_sel = torch.zeros(n, dtype=torch.int32, device=d)
+        self.t_sel_bits = torch.full((n,), 8, dtype=torch.int32, device=d)
+        self.t_flags = torch.zeros(n, dtype=torch.int32, device=d)
+        self.t_cur_obj = torch.zeros(n, dtype=torch.float64, device=d)
+        self.t_sel = torch.full((n * self.cap_max,), -1, dtype=torch.int32, device=d)
+        self.kinds = np.full(self.n_slots, 7, np.int8)
+        recs = np.zeros(self.n_slots, PRIM_DTYPE)
+        for t, pool in enumerate(self.pools):
+            if pool:
+                a = pool if isinstance(pool, np.ndarray) else pack_cands(pool)
+                recs[self.pool_off[t]:self.pool_off[t] + len(a)] = a
+        self.kinds[:] = np.where(recs["kind"] < 7, recs["kind"], 7)
+        self.t_cand = _dev(recs.view(np.uint8), d)
+        self.t_prep = torch.zeros(self.n_slots * 16, dtype=torch.float32, device=d)
+        self.t_alive = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
+        self.t_partial = torch.zeros(self.n_slots * 4, dtype=torch.float32, device=d)
+        self.t_status = torch.zeros(4, dtype=torch.int32, device=d)
+        self.h_status = torch.zeros(4, dtype=torch.int32).pin_memory()
+        self.st = _lib.WeftFitState(
+            n, self.cap_max, self.n_slots,
+            *[_lib.ptr(x) for x in (self.t_src, self.t_bg, self.t_px_off, self.t_size, self.t_cap, self.t_pool_off,
+                                    self.t_pool_cnt, self.t_n_alive, self.t_n_sel, self.t_sel_bits, self.t_flags,
+                                    self.t_cur_obj, self.t_sel, self.t_cand, self.t_prep, self.t_alive,
+                                    self.t_partial, self.t_status)])
+        self.stats = FitStats()
+        self._prepare(np.zeros(n, np.int32))
+        self._build_work()
+
+    # ------------------------------------------------------------------ plumbing
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _prepare(self, first_new: np.ndarray) -> None:
+        t_first = _dev(first_new.astype(np.int32), self.device)
+        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(t_first), self._stream()),
+                   "weftk_fit_prepare")
+        self._keep = t_first  # keep alive until the launch has consumed it
+
+    def _build_work(self) -> None:
+        """perm (kind-sorted, curves first) and cost-sorted work items per size class."""
+        n = self.n
+        cnt = self.pool_cnt.astype(np.int64)
+        tile_of = np.repeat(np.arange(n), cnt)
+        first_of_tile = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64)
+        local = np.arange(int(cnt.sum())) - np.repeat(first_of_tile, cnt)
+        slot = np.repeat(self.pool_off, cnt) + local
+        cost = KIND_COST[self.kinds[slot]]
+        order = np.lexsort((local, -cost, tile_of))
+        perm = np.zeros(self.n_slots, np.int32)
+        perm[np.repeat(self.pool_off, cnt) + local] = local[order]
+        self.t_perm = _dev(perm, self.device)
+        sorted_cost = cost[order]
+        csum = np.concatenate([[0], np.cumsum(sorted_cost)])
+        items = {}
+        for cls, sizes in ((8, (8,)), (16, (16,)), (32, (32, 64))):
+            chunk = CHUNK[cls]
+            rows = []
+            for s in sizes:
+                ts_idx = np.nonzero(self.sizes == s)[0]
+                if ts_idx.size == 0:
+                    continue
+                nch = (cnt[ts_idx] + chunk - 1) // chunk
+                t_rep = np.repeat(ts_idx, nch)
+                k = np.arange(int(nch.sum())) - np.repeat(np.concatenate([[0], np.cumsum(nch)[:-1]]), nch)
+                first = k * chunk
+                count = np.minimum(chunk, cnt[t_rep] - first)
+                g0 = first_of_tile[t_rep] + first
+                c = (csum[g0 + count] - csum[g0]) * (s * s)
+                blocks = max(1, (s * s) // 1024)
+                for b in range(blocks):
+                    rows.append(np.stack([t_rep, np.full_like(t_rep, b), first, count, c], axis=1))
+            if rows:
+                r = np.concatenate(rows)
+                r = r[np.argsort(-r[:, 4], kind="stable")]
+                arr = np.zeros(len(r), FIT_ITEM_DTYPE)
+                arr["tile"], arr["block"], arr["first"], arr["count"] = r[:, 0], r[:, 1], r[:, 2], r[:, 3]
+            else:
+                arr = np.zeros(0, FIT_ITEM_DTYPE)
+            items[cls] = arr
+        self.items = items
+        self.t_items = {k: _dev(v.view(np.uint8), self.device) if len(v) else None for k, v in items.items()}
+
+    def _round(self, mode: int) -> tuple[int, int]:
+        ti = self.t_items
+        n8, n16, n32 = (len(self.items[k]) for k in (8, 16, 32))
+        rc = self.lib.weftk_fit_round(ctypes_ref(self.st), mode, self.lam, self.thr, _lib.ptr(self.t_perm),
+                                      _lib.ptr(ti[8]), n8, _lib.ptr(ti[16]), n16, _lib.ptr(ti[32]), n32,
+                                      self._stream())
+        _lib.check(rc, "weftk_fit_round")
+        self.stats.launches += 1
+        self.h_status.copy_(self.t_status, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        ev, imp = int(self.h_status[0]), int(self.h_status[1])
+        self.stats.per_round.append((mode, ev, imp))
+        return ev, imp
+
+    # ------------------------------------------------------------------ re-seed
+    def _reseed(self, reseed) -> None:
+        t0 = time.perf_counter()
+        flags = self.t_flags.cpu().numpy()
+        n_sel = self.t_n_sel.cpu().numpy()
+        tiles = np.nonzero((flags & TILE_COMPLEX) & (n_sel < self.caps))[0]
+        if tiles.size == 0:
+            return
+        bg = self.t_bg.cpu().numpy()
+        first_new = self.pool_cnt.copy()
+        new_recs, new_slots = [], []
+        for t in tiles:
+            s = int(self.sizes[t])
+            a = int(self.px_off[t])
+            pred = np.clip(bg[a:a + s * s, :3].reshape(s, s, 3), 0.0, 1.0)
+            cands = reseed(int(t), self.patches[t], pred) if reseed is not None else \
+                residual_candidates(self.patches[t], pred, self.quality)
+            if not cands:
+                continue
+            k = len(cands)
+            c0 = int(self.pool_cnt[t])
+            if c0 + k > self.pool_cap[t]:
+                raise RuntimeError(f"tile {t}: re-seed overflows its {self.pool_cap[t]} candidate slots")
+            self.pools[t].extend(cands)
+            new_recs.append(pack_cands(cands))
+            new_slots.append(self.pool_off[t] + c0 + np.arange(k))
+            self.pool_cnt[t] = c0 + k
+        self.stats.reseeds += 1
+        self.stats.reseed_tiles += int(tiles.size)
+        if new_recs:
+            recs = np.concatenate(new_recs)
+            slots = np.concatenate(new_slots)
+            self.kinds[slots] = np.where(recs["kind"] < 7, recs["kind"], 7)
+            view = self.t_cand.view(-1, PRIM_DTYPE.itemsize)
+            view[_dev(slots.astype(np.int64), self.device)] = _dev(recs.view(np.uint8).reshape(-1, PRIM_DTYPE.itemsize),
+                                                                    self.device)
+            self.t_pool_cnt.copy_(torch.from_numpy(self.pool_cnt))
+            self._prepare(first_new)
+            self._build_work()
+        self.stats.t_reseed_s += time.perf_counter() - t0
+
+    # ------------------------------------------------------------------ driver
+    def run(self, reseed=None, max_rounds: int | None = None) -> "BatchedFit":
+        """Run init plus up to ``max_rounds`` greedy rounds (default: the quality's budget).
+
+        ``reseed(tile, patch, pred) -> list[Cand]`` supplies re-seed candidates;
+        default is ``candidates.residual_candidates``.
+        """
+        self._round(FIT_INIT)
+        rounds = rate.max_rounds(self.quality) if max_rounds is None else int(max_rounds)
+        stalls = 0
+        for _ in range(rounds):
+            ev, imp = self._round(FIT_ROUND)
+            if ev == 0:
+                break
+            self.stats.rounds += 1
+            if imp == 0:
+                stalls += 1
+                if stalls > 3:
+                    break
+                self._reseed(reseed)
+            else:
+                stalls = 0
+        return self
+
+    # ------------------------------------------------------------------ results
+    def selected_indices(self) -> list[list[int]]:
+        sel = self.t_sel.cpu().numpy().reshape(self.n, self.cap_max)
+        n_sel = self.t_n_sel.cpu().numpy()
+        return [sel[t, :n_sel[t]].tolist() for t in range(self.n)]
+
+    def selected(self) -> list[list]:
+        return [[self.pools[t][i] for i in idx] for t, idx in enumerate(self.selected_indices())]
+
+    def objectives(self) -> np.ndarray:
+        return self.t_cur_obj.cpu().numpy()
+
+    def recon_tiles(self) -> list[np.ndarray]:
+        """Per-tile clipped composite of the selected stacks (what the decoder renders before residuals)."""
+        bg = self.t_bg.clamp(0.0, 1.0).cpu().numpy()
+        out = []
+        for t in range(self.n):
+            s = int(self.sizes[t])
+            a = int(self.px_off[t])
+            out.append(bg[a:a + s * s, :3].reshape(s, s, 3))
+        return out
+
+
+def ctypes_ref(st) -> int:
+    import ctypes
+
+    return ctypes.addressof(st)

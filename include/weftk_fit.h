@@ -71,6 +71,8 @@ typedef struct WeftFitState {
     uint8_t* alive;          /* [n_slots] 1 = still in the pool */
     float* partial;          /* [n_slots * 4] per-1024-pixel-block squared-error sums (scratch) */
     int32_t* status;         /* [4] round counters: evaluated tiles, improved tiles */
+    unsigned long long* work; /* [2] running totals: candidate-pixels scored, algorithmic FP32 ops
+                                 (per candidate-pixel: per-kind op count + 9 for the error); may be NULL */
 } WeftFitState;
 
 /* A unit of scoring work: tile, 1024-pixel block, and a run of candidate
@@ -99,6 +101,16 @@ int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double comp
                     const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
                     const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32, int n_items32,
                     void* stream);
+
+/* Kernel timing for measurement: while enabled, weftk_fit_round brackets its
+ * scoring launches with CUDA events.  *score_ms receives the summed device time
+ * of the scoring launches since the previous query and *n_rounds how many
+ * rounds that covers; both reset on read.  Call after the stream has synced. */
+int weftk_fit_timing(int enable, double* score_ms, int* n_rounds);
+
+/* Measured FP32 FMA throughput of the current GPU in GFLOP/s (2 ops per FMA):
+ * a register-resident FMA loop on every SM, timed with CUDA events. */
+int weftk_measure_fp32_peak(double* gflops);
 
 #ifdef __cplusplus
 }

@@ -33,6 +33,11 @@ __constant__ int c_prim_bytes[8] = WEFTK_PRIM_BYTES;
 
 __device__ __forceinline__ int prim_bits(int kind) { return 8 * c_prim_bytes[(kind >= 0 && kind < 8) ? kind : 7]; }
 
+// FP32 operations to evaluate and blend one primitive at one pixel (FMA = 2): const 10,
+// linear 24, line 28, curve 31 segments x 16 + 13 = 509, triangle 26.
+__constant__ int c_kind_ops[8] = {10, 24, 28, 509, 26, 0, 0, 0};
+__device__ __forceinline__ int kind_ops(int kind) { return c_kind_ops[(kind >= 0 && kind < 8) ? kind : 7]; }
+
 __device__ __forceinline__ Prep load_prep(const float* prep, long long slot) {
     const float4* p = reinterpret_cast<const float4*>(prep) + slot * 4;
     Prep r;
@@ -154,11 +159,14 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
         s[j] = src[p];
         g[j] = bg[p];
     }
+    unsigned long long ops = 0, cpx = 0;
     for (int c = group; c < w.count; c += GROUPS) {
         const int local = perm[off + w.first + c];
         const long long slot = off + local;
         if (!st.alive[slot]) continue;
         const Prep P = load_prep(st.prep, slot);
+        cpx += 32 * PPL;
+        ops += (unsigned long long)(32 * PPL) * (unsigned long long)(kind_ops(st.cand[slot].kind) + 9);
         float a[PPL], sr[PPL], sg[PPL], sb[PPL];
         prim_eval<PPL>(P, fx, fy, a, sr, sg, sb, lane);
         float e = 0.0f;
@@ -175,6 +183,10 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
         } else if (lane == 0) {
             red[c][wig] = e;
         }
+    }
+    if (st.work != nullptr && lane == 0 && cpx) {
+        atomicAdd(&st.work[0], cpx);
+        atomicAdd(&st.work[1], ops);
     }
     if (WPC > 1) {
         __syncthreads();
@@ -272,9 +284,89 @@ __global__ void __launch_bounds__(128) fit_select_kernel(WeftFitState st, int mo
     }
 }
 
+// Register-resident FMA loop for measuring the FP32 pipe: 8 independent chains per thread.
+__global__ void __launch_bounds__(256) fp32_peak_kernel(float* out, int iters, float a, float b) {
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = (float)(threadIdx.x + k);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = fmaf(v[k], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += v[k];
+    if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the loop live; practically never taken
+}
+
+struct FitTiming {
+    bool enabled = false;
+    bool pending = false;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    double ms = 0.0;
+    int rounds = 0;
+};
+static FitTiming g_timing;
+
+static int timing_collect() {
+    if (!g_timing.pending) return WEFTK_OK;
+    WEFTK_CUDA(cudaEventSynchronize(g_timing.stop));
+    float ms = 0.0f;
+    WEFTK_CUDA(cudaEventElapsedTime(&ms, g_timing.start, g_timing.stop));
+    g_timing.ms += ms;
+    g_timing.rounds += 1;
+    g_timing.pending = false;
+    return WEFTK_OK;
+}
+
 }  // namespace weftk
 
 using namespace weftk;
+
+extern "C" int weftk_fit_timing(int enable, double* score_ms, int* n_rounds) {
+    int rc = timing_collect();
+    if (rc) return rc;
+    if (enable && !g_timing.start) {
+        WEFTK_CUDA(cudaEventCreate(&g_timing.start));
+        WEFTK_CUDA(cudaEventCreate(&g_timing.stop));
+    }
+    g_timing.enabled = enable != 0;
+    if (score_ms) *score_ms = g_timing.ms;
+    if (n_rounds) *n_rounds = g_timing.rounds;
+    g_timing.ms = 0.0;
+    g_timing.rounds = 0;
+    return WEFTK_OK;
+}
+
+extern "C" int weftk_measure_fp32_peak(double* gflops) {
+    WEFTK_REQUIRE(gflops, "measure_fp32_peak: null pointer");
+    int dev = 0, sms = 0;
+    WEFTK_CUDA(cudaGetDevice(&dev));
+    WEFTK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    float* out = nullptr;
+    WEFTK_CUDA(cudaMalloc(&out, 256 * sizeof(float)));
+    cudaEvent_t a, b;
+    WEFTK_CUDA(cudaEventCreate(&a));
+    WEFTK_CUDA(cudaEventCreate(&b));
+    const int blocks = sms * 8, iters = 1 << 15;
+    fp32_peak_kernel<<<blocks, 256>>>(out, 256, 1.0000001f, 1e-7f);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 5; ++r) {
+        WEFTK_CUDA(cudaEventRecord(a));
+        fp32_peak_kernel<<<blocks, 256>>>(out, iters, 1.0000001f, 1e-7f);
+        WEFTK_CUDA(cudaEventRecord(b));
+        WEFTK_CUDA(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        WEFTK_CUDA(cudaEventElapsedTime(&ms, a, b));
+        best = ms < best ? ms : best;
+    }
+    WEFTK_CUDA(cudaGetLastError());
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    *gflops = 2.0 * 8.0 * (double)iters * 256.0 * (double)blocks / (best * 1e-3) / 1e9;
+    return WEFTK_OK;
+}
 
 extern "C" int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_new, void* stream) {
     WEFTK_REQUIRE(st && d_first_new, "fit_prepare: null argument");
@@ -296,9 +388,18 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
     const int nt = st->n_tiles;
     WEFTK_CUDA(cudaMemsetAsync(st->status, 0, 4 * sizeof(int32_t), s));
     fit_begin_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(*st, mode);
+    if (g_timing.enabled) {
+        int rc = timing_collect();
+        if (rc) return rc;
+        WEFTK_CUDA(cudaEventRecord(g_timing.start, s));
+    }
     if (n_items8) fit_score_kernel<2, 1><<<n_items8, 128, 0, s>>>(*st, d_perm, d_items8, n_items8, 8, 8);
     if (n_items16) fit_score_kernel<8, 1><<<n_items16, 128, 0, s>>>(*st, d_perm, d_items16, n_items16, 16, 16);
     if (n_items32) fit_score_kernel<8, 4><<<n_items32, 128, 0, s>>>(*st, d_perm, d_items32, n_items32, 32, 64);
+    if (g_timing.enabled) {
+        WEFTK_CUDA(cudaEventRecord(g_timing.stop, s));
+        g_timing.pending = true;
+    }
     fit_select_kernel<<<ceil_div(nt, 4), 128, 0, s>>>(*st, mode, (float)lambda, lambda);
     fit_end_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(*st, mode, complex_threshold);
     WEFTK_CUDA(cudaGetLastError());

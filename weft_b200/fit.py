@@ -53,6 +53,16 @@ def pack_cands(cands) -> np.ndarray:
     return arr
 
 
+def unpack_cands(arr: np.ndarray) -> list:
+    glen = {0: 0, 1: 4, 2: 5, 3: 7, 4: 6}
+    out = []
+    for r in arr:
+        k = int(r["kind"])
+        out.append(Cand(k, tuple(float(v) for v in r["geom"][:glen.get(k, 7)]), tuple(float(v) for v in r["color0"]),
+                        tuple(float(v) for v in r["color1"]) if k == 1 else None, float(r["alpha"])))
+    return out
+
+
 def _dev(a: np.ndarray, device) -> torch.Tensor:
     return torch.from_numpy(np.ascontiguousarray(a)).to(device, non_blocking=False)
 
@@ -86,7 +96,7 @@ class BatchedFit:
         self.caps = np.array(caps if caps is not None else [MAX_PRIMS_BY_SIZE.get(int(s), 48) for s in self.sizes],
                              np.int32)
         self.cap_max = int(self.caps.max()) if n else 1
-        self.pools: list[list] = [list(p) for p in pools]
+        self.pools: list = [p if isinstance(p, np.ndarray) else list(p) for p in pools]
         cnt = np.array([len(p) for p in self.pools], np.int64)
         self.pool_cap = cnt + reserve
         self.pool_off = np.zeros(n, np.int64)
@@ -125,18 +135,21 @@ class BatchedFit:
                 a = pool if isinstance(pool, np.ndarray) else pack_cands(pool)
                 recs[self.pool_off[t]:self.pool_off[t] + len(a)] = a
         self.kinds[:] = np.where(recs["kind"] < 7, recs["kind"], 7)
+        self._init_kinds = self.kinds.copy()
         self.t_cand = _dev(recs.view(np.uint8), d)
         self.t_prep = torch.zeros(self.n_slots * 16, dtype=torch.float32, device=d)
         self.t_alive = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
         self.t_partial = torch.zeros(self.n_slots * 4, dtype=torch.float32, device=d)
         self.t_status = torch.zeros(4, dtype=torch.int32, device=d)
+        self.t_work = torch.zeros(2, dtype=torch.int64, device=d)
         self.h_status = torch.zeros(4, dtype=torch.int32).pin_memory()
+        self.init_cnt = self.pool_cnt.copy()
         self.st = _lib.WeftFitState(
             n, self.cap_max, self.n_slots,
             *[_lib.ptr(x) for x in (self.t_src, self.t_bg, self.t_px_off, self.t_size, self.t_cap, self.t_pool_off,
                                     self.t_pool_cnt, self.t_n_alive, self.t_n_sel, self.t_sel_bits, self.t_flags,
                                     self.t_cur_obj, self.t_sel, self.t_cand, self.t_prep, self.t_alive,
-                                    self.t_partial, self.t_status)])
+                                    self.t_partial, self.t_status, self.t_work)])
         self.stats = FitStats()
         self._prepare(np.zeros(n, np.int32))
         self._build_work()
@@ -210,7 +223,7 @@ class BatchedFit:
         return ev, imp
 
     # ------------------------------------------------------------------ re-seed
-    def _reseed(self, reseed) -> None:
+    def _reseed(self, reseed, reseed_batch=None) -> None:
         t0 = time.perf_counter()
         flags = self.t_flags.cpu().numpy()
         n_sel = self.t_n_sel.cpu().numpy()
@@ -220,18 +233,26 @@ class BatchedFit:
         bg = self.t_bg.cpu().numpy()
         first_new = self.pool_cnt.copy()
         new_recs, new_slots = [], []
+        preds = []
         for t in tiles:
             s = int(self.sizes[t])
             a = int(self.px_off[t])
-            pred = np.clip(bg[a:a + s * s, :3].reshape(s, s, 3), 0.0, 1.0)
-            cands = reseed(int(t), self.patches[t], pred) if reseed is not None else \
-                residual_candidates(self.patches[t], pred, self.quality)
+            preds.append(np.clip(bg[a:a + s * s, :3].reshape(s, s, 3), 0.0, 1.0))
+        if reseed_batch is not None:
+            batch = reseed_batch([int(t) for t in tiles], [self.patches[t] for t in tiles], preds)
+        else:
+            fn = reseed if reseed is not None else \
+                (lambda t, patch, pred: residual_candidates(patch, pred, self.quality))
+            batch = [fn(int(t), self.patches[t], p) for t, p in zip(tiles, preds)]
+        for t, cands in zip(tiles, batch):
             if not cands:
                 continue
             k = len(cands)
             c0 = int(self.pool_cnt[t])
             if c0 + k > self.pool_cap[t]:
                 raise RuntimeError(f"tile {t}: re-seed overflows its {self.pool_cap[t]} candidate slots")
+            if isinstance(self.pools[t], np.ndarray):
+                self.pools[t] = unpack_cands(self.pools[t])
             self.pools[t].extend(cands)
             new_recs.append(pack_cands(cands))
             new_slots.append(self.pool_off[t] + c0 + np.arange(k))
@@ -250,12 +271,41 @@ class BatchedFit:
             self._build_work()
         self.stats.t_reseed_s += time.perf_counter() - t0
 
+    def reset(self) -> None:
+        """Forget the fit (selections, re-seeds) but keep pixels and initial pools resident."""
+        self.pool_cnt[:] = self.init_cnt
+        for t in range(self.n):
+            p = self.pools[t]
+            if not isinstance(p, np.ndarray) and len(p) > self.init_cnt[t]:
+                del p[self.init_cnt[t]:]
+        self.kinds[:] = 7
+        self.t_pool_cnt.copy_(torch.from_numpy(self.pool_cnt))
+        self.t_bg.zero_()
+        self.t_n_alive.zero_()
+        self.t_n_sel.zero_()
+        self.t_sel_bits.fill_(8)
+        self.t_flags.zero_()
+        self.t_cur_obj.zero_()
+        self.t_sel.fill_(-1)
+        self.t_alive.zero_()
+        self.t_work.zero_()
+        self.kinds[:] = self._init_kinds
+        self._prepare(np.zeros(self.n, np.int32))
+        self._build_work()
+        self.stats = FitStats()
+
+    def work_counters(self) -> tuple[int, int]:
+        """(candidate-pixels scored, algorithmic FP32 ops) since the last reset."""
+        w = self.t_work.cpu().numpy()
+        return int(w[0]), int(w[1])
+
     # ------------------------------------------------------------------ driver
-    def run(self, reseed=None, max_rounds: int | None = None) -> "BatchedFit":
+    def run(self, reseed=None, max_rounds: int | None = None, reseed_batch=None) -> "BatchedFit":
         """Run init plus up to ``max_rounds`` greedy rounds (default: the quality's budget).
 
-        ``reseed(tile, patch, pred) -> list[Cand]`` supplies re-seed candidates;
-        default is ``candidates.residual_candidates``.
+        ``reseed(tile, patch, pred) -> list[Cand]`` supplies re-seed candidates
+        (default ``candidates.residual_candidates``); ``reseed_batch(tiles,
+        patches, preds) -> list[list[Cand]]`` does all stalled tiles at once.
         """
         self._round(FIT_INIT)
         rounds = rate.max_rounds(self.quality) if max_rounds is None else int(max_rounds)
@@ -269,7 +319,7 @@ class BatchedFit:
                 stalls += 1
                 if stalls > 3:
                     break
-                self._reseed(reseed)
+                self._reseed(reseed, reseed_batch)
             else:
                 stalls = 0
         return self
@@ -281,7 +331,11 @@ class BatchedFit:
         return [sel[t, :n_sel[t]].tolist() for t in range(self.n)]
 
     def selected(self) -> list[list]:
-        return [[self.pools[t][i] for i in idx] for t, idx in enumerate(self.selected_indices())]
+        out = []
+        for t, idx in enumerate(self.selected_indices()):
+            p = self.pools[t]
+            out.append(unpack_cands(p[idx]) if isinstance(p, np.ndarray) else [p[i] for i in idx])
+        return out
 
     def objectives(self) -> np.ndarray:
         return self.t_cur_obj.cpu().numpy()

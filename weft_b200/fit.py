@@ -131,7 +131,7 @@ class BatchedFit:
         self.kinds = np.full(self.n_slots, 7, np.int8)
         recs = np.zeros(self.n_slots, PRIM_DTYPE)
         for t, pool in enumerate(self.pools):
-            if pool:
+            if len(pool):
                 a = pool if isinstance(pool, np.ndarray) else pack_cands(pool)
                 recs[self.pool_off[t]:self.pool_off[t] + len(a)] = a
         self.kinds[:] = np.where(recs["kind"] < 7, recs["kind"], 7)

@@ -58,7 +58,8 @@ typedef struct WeftFitState {
     const int32_t* size;     /* [n_tiles] tile side: 8, 16, 32 or 64 */
     const int32_t* cap;      /* [n_tiles] primitive cap */
     const int32_t* pool_off; /* [n_tiles] first slot */
-    const int32_t* pool_cnt; /* [n_tiles] filled slots */
+    int32_t* pool_cnt;       /* [n_tiles] filled slots (grows with re-seeds) */
+    const int32_t* pool_cap; /* [n_tiles] slots reserved for the tile */
     int32_t* n_alive;        /* [n_tiles] live candidates */
     int32_t* n_sel;          /* [n_tiles] selected primitives */
     int32_t* sel_bits;       /* [n_tiles] 8 + sum of 8 * bytes[kind] over the selection */
@@ -101,6 +102,16 @@ int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double comp
                     const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
                     const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32, int n_items32,
                     void* stream);
+
+/*
+ * Re-seed every tile that has flag COMPLEX and room under its cap with
+ * residual-targeted candidates, generated on the device from src and the
+ * clipped composite bg (the reference's _generate_residual_candidates,
+ * src/weft/encoder.py:1255-1366), de-duplicated, appended to the tile's pool,
+ * prepared and marked live.  At most 117 candidates per tile per call; a tile
+ * whose reserved slots would overflow is skipped and reported.
+ */
+int weftk_fit_reseed(const WeftFitState* st, int quality, void* stream);
 
 /* Kernel timing for measurement: while enabled, weftk_fit_round brackets its
  * scoring launches with CUDA events.  *score_ms receives the summed device time

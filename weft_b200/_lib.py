@@ -40,7 +40,7 @@ class WeftTileDecodeDesc(ctypes.Structure):
 class WeftFitState(ctypes.Structure):
     """Device pointers of a fit (include/weftk_fit.h)."""
     _fields_ = [("n_tiles", ctypes.c_int32), ("cap_max", ctypes.c_int32), ("n_slots", ctypes.c_int64)] + [
-        (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "n_alive",
+        (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "pool_cap", "n_alive",
                                        "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive",
                                        "partial", "status", "work")]
 
@@ -58,7 +58,7 @@ assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
 assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
 FIT_ITEM_DTYPE = np.dtype([("tile", np.int32), ("block", np.int32), ("first", np.int32), ("count", np.int32)])
 assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
-assert ctypes.sizeof(WeftFitState) == 16 + 19 * 8
+assert ctypes.sizeof(WeftFitState) == 16 + 20 * 8
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -77,6 +77,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_fit_prepare": [_P, _P, _P],
     "weftk_fit_round": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],
     "weftk_fit_timing": [_I, _P, _P],
+    "weftk_fit_reseed": [_P, _I, _P],
     "weftk_measure_fp32_peak": [_P],
 }
 

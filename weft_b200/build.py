@@ -47,7 +47,7 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
-    cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
+    cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-rdc=true", "--shared", "-Xcompiler", "-fPIC",
            "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *_sources()]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

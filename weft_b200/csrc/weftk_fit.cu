@@ -138,10 +138,13 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
     if (!(st.flags[t] & WEFTK_TILE_EVAL)) return;
     const int ts = st.size[t];
     if (ts < expect_min || ts > expect_max || (WPC > 1 && w.count > MAX_RUN) || w.block * 1024 >= ts * ts ||
-        w.first < 0 || w.first + w.count > st.pool_cnt[t]) {
+        w.first < 0 || w.first + w.count > st.pool_cap[t]) {
         if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
         return;
     }
+    // items cover the tile's reserved slots; only the filled ones are scored
+    const int count = min(w.count, st.pool_cnt[t] - w.first);
+    if (count <= 0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int group = warp / WPC, wig = warp % WPC;
     const long long off = st.pool_off[t];
@@ -160,7 +163,7 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
         g[j] = bg[p];
     }
     unsigned long long ops = 0, cpx = 0;
-    for (int c = group; c < w.count; c += GROUPS) {
+    for (int c = group; c < count; c += GROUPS) {
         const int local = perm[off + w.first + c];
         const long long slot = off + local;
         if (!st.alive[slot]) continue;
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
     }
     if (WPC > 1) {
         __syncthreads();
-        for (int c = threadIdx.x; c < w.count; c += blockDim.x) {
+        for (int c = threadIdx.x; c < count; c += blockDim.x) {
             const long long slot = off + perm[off + w.first + c];
             if (!st.alive[slot]) continue;
             float e = red[c][0];

@@ -122,6 +122,7 @@ class BatchedFit:
         self.t_cap = _dev(self.caps, d)
         self.t_pool_off = _dev(self.pool_off.astype(np.int32), d)
         self.t_pool_cnt = _dev(self.pool_cnt, d)
+        self.t_pool_cap = _dev(self.pool_cap.astype(np.int32), d)
         self.t_n_alive = torch.zeros(n, dtype=torch.int32, device=d)
         self.t_n_sel = torch.zeros(n, dtype=torch.int32, device=d)
         self.t_sel_bits = torch.full((n,), 8, dtype=torch.int32, device=d)
@@ -147,10 +148,11 @@ class BatchedFit:
         self.st = _lib.WeftFitState(
             n, self.cap_max, self.n_slots,
             *[_lib.ptr(x) for x in (self.t_src, self.t_bg, self.t_px_off, self.t_size, self.t_cap, self.t_pool_off,
-                                    self.t_pool_cnt, self.t_n_alive, self.t_n_sel, self.t_sel_bits, self.t_flags,
+                                    self.t_pool_cnt, self.t_pool_cap, self.t_n_alive, self.t_n_sel, self.t_sel_bits, self.t_flags,
                                     self.t_cur_obj, self.t_sel, self.t_cand, self.t_prep, self.t_alive,
                                     self.t_partial, self.t_status, self.t_work)])
         self.stats = FitStats()
+        self.device_reseeded = False
         self._prepare(np.zeros(n, np.int32))
         self._build_work()
 
@@ -165,20 +167,30 @@ class BatchedFit:
         self._keep = t_first  # keep alive until the launch has consumed it
 
     def _build_work(self) -> None:
-        """perm (kind-sorted, curves first) and cost-sorted work items per size class."""
+        """perm and cost-sorted work items per size class, covering every reserved slot.
+
+        The initial pool is scored in kind order (curves first) so a work item
+        holds candidates of similar cost; re-seeded slots are scored in slot
+        order.  Items cover the reserved slots too; the kernel only scores the
+        filled ones, so re-seeding needs no new items.
+        """
         n = self.n
-        cnt = self.pool_cnt.astype(np.int64)
+        cnt = self.init_cnt.astype(np.int64)
+        cap = self.pool_cap.astype(np.int64)
         tile_of = np.repeat(np.arange(n), cnt)
         first_of_tile = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64)
         local = np.arange(int(cnt.sum())) - np.repeat(first_of_tile, cnt)
         slot = np.repeat(self.pool_off, cnt) + local
         cost = KIND_COST[self.kinds[slot]]
         order = np.lexsort((local, -cost, tile_of))
-        perm = np.zeros(self.n_slots, np.int32)
-        perm[np.repeat(self.pool_off, cnt) + local] = local[order]
+        cap_first = np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.int64)
+        perm = (np.arange(self.n_slots, dtype=np.int64) - np.repeat(cap_first, cap)).astype(np.int32)
+        perm[slot] = local[order]
         self.t_perm = _dev(perm, self.device)
-        sorted_cost = cost[order]
-        csum = np.concatenate([[0], np.cumsum(sorted_cost)])
+        # cost of a run of slots in scoring order (reserved slots: a typical re-seed mix)
+        slot_cost = np.full(self.n_slots, 60, np.int64)
+        slot_cost[slot] = cost[order]
+        csum = np.concatenate([[0], np.cumsum(slot_cost)])
         items = {}
         for cls, sizes in ((8, (8,)), (16, (16,)), (32, (32, 64))):
             chunk = CHUNK[cls]
@@ -187,13 +199,15 @@ class BatchedFit:
                 ts_idx = np.nonzero(self.sizes == s)[0]
                 if ts_idx.size == 0:
                     continue
-                nch = (cnt[ts_idx] + chunk - 1) // chunk
+                nch = (cap[ts_idx] + chunk - 1) // chunk
                 t_rep = np.repeat(ts_idx, nch)
                 k = np.arange(int(nch.sum())) - np.repeat(np.concatenate([[0], np.cumsum(nch)[:-1]]), nch)
                 first = k * chunk
-                count = np.minimum(chunk, cnt[t_rep] - first)
-                g0 = first_of_tile[t_rep] + first
+                count = np.minimum(chunk, cap[t_rep] - first)
+                g0 = self.pool_off[t_rep] + first
                 c = (csum[g0 + count] - csum[g0]) * (s * s)
+                # runs that start in the reserved region only cost once re-seeded
+                c = np.where(first >= cnt[t_rep], 0, c)
                 blocks = max(1, (s * s) // 1024)
                 for b in range(blocks):
                     rows.append(np.stack([t_rep, np.full_like(t_rep, b), first, count, c], axis=1))
@@ -268,12 +282,17 @@ class BatchedFit:
                                                                     self.device)
             self.t_pool_cnt.copy_(torch.from_numpy(self.pool_cnt))
             self._prepare(first_new)
-            self._build_work()
         self.stats.t_reseed_s += time.perf_counter() - t0
+
+    def _reseed_device(self) -> None:
+        _lib.check(self.lib.weftk_fit_reseed(ctypes_ref(self.st), self.quality, self._stream()), "weftk_fit_reseed")
+        self.stats.reseeds += 1
+        self.device_reseeded = True
 
     def reset(self) -> None:
         """Forget the fit (selections, re-seeds) but keep pixels and initial pools resident."""
         self.pool_cnt[:] = self.init_cnt
+        self.device_reseeded = False
         for t in range(self.n):
             p = self.pools[t]
             if not isinstance(p, np.ndarray) and len(p) > self.init_cnt[t]:
@@ -291,8 +310,8 @@ class BatchedFit:
         self.t_work.zero_()
         self.kinds[:] = self._init_kinds
         self._prepare(np.zeros(self.n, np.int32))
-        self._build_work()
         self.stats = FitStats()
+        self.device_reseeded = False
 
     def work_counters(self) -> tuple[int, int]:
         """(candidate-pixels scored, algorithmic FP32 ops) since the last reset."""
@@ -319,7 +338,10 @@ class BatchedFit:
                 stalls += 1
                 if stalls > 3:
                     break
-                self._reseed(reseed, reseed_batch)
+                if reseed is None and reseed_batch is None:
+                    self._reseed_device()
+                else:
+                    self._reseed(reseed, reseed_batch)
             else:
                 stalls = 0
         return self
@@ -330,12 +352,22 @@ class BatchedFit:
         n_sel = self.t_n_sel.cpu().numpy()
         return [sel[t, :n_sel[t]].tolist() for t in range(self.n)]
 
-    def selected(self) -> list[list]:
-        out = []
-        for t, idx in enumerate(self.selected_indices()):
-            p = self.pools[t]
-            out.append(unpack_cands(p[idx]) if isinstance(p, np.ndarray) else [p[i] for i in idx])
+    def selected_records(self) -> list[np.ndarray]:
+        """The selected primitives of every tile as 60-byte records, read from the device."""
+        idx = self.selected_indices()
+        flat = np.concatenate([self.pool_off[t] + np.asarray(i, np.int64) for t, i in enumerate(idx)]) \
+            if self.n else np.zeros(0, np.int64)
+        recs = self.t_cand.view(-1, PRIM_DTYPE.itemsize)[_dev(flat, self.device)].cpu().numpy()
+        recs = recs.reshape(-1).view(PRIM_DTYPE)
+        out, k = [], 0
+        for i in idx:
+            out.append(recs[k:k + len(i)])
+            k += len(i)
         return out
+
+    def selected(self) -> list[list]:
+        """The selected primitives of every tile as ``Cand`` objects (float32-rounded values)."""
+        return [unpack_cands(r) for r in self.selected_records()]
 
     def objectives(self) -> np.ndarray:
         return self.t_cur_obj.cpu().numpy()

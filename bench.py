@@ -52,11 +52,6 @@ def _pool_cands(args):
     return pack_cands(candidates.tile_candidates(patch, q))
 
 
-def _pool_resid(args):
-    patch, pred, q = args
-    return candidates.residual_candidates(patch, pred, q)
-
-
 def _oracle_shard(args):
     """CPU baseline worker: the oracle greedy over a shard of tiles."""
     patches, pools, q = args
@@ -223,6 +218,7 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=8.0)
     ap.add_argument("--ref-step-s", type=float, default=8.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     args = ap.parse_args()
 
     # Process pools first: spawned before any CUDA initialisation.
@@ -247,21 +243,24 @@ def run_weft(args, world, rank, local, executor, cores):
 
     img, tiles, patches, pools, cand_s = build_workload(args.size, args.prims, rank, executor)
 
-    def reseed_batch(ts, ps, preds):
-        return list(executor.map(_pool_resid, [(p, q, QUALITY) for p, q in zip(ps, preds)], chunksize=16))
-
     torch.cuda.set_device(local)
     from weft_b200 import _lib
     from weft_b200.fit import BatchedFit
 
     lib = _lib.lib_for_device(local)
-    fit = BatchedFit(patches, pools, QUALITY, caps=[CAP] * len(patches), device=local)
+    # flat host inputs of the public API (what a caller hands over)
+    pixels = np.concatenate([p.reshape(-1, 3) for p in patches])
+    sizes = np.array([p.shape[0] for p in patches], np.int32)
+    records = np.concatenate(pools)
+    counts = np.array([len(p) for p in pools], np.int64)
+    caps = [CAP] * len(patches)
+    fit = BatchedFit.from_arrays(pixels, sizes, records, counts, QUALITY, caps=caps, device=local)
     n_px = int(sum(p.shape[0] ** 2 for p in patches))
     stream = torch.cuda.current_stream()
 
     def step():
         fit.reset()
-        fit.run(reseed_batch=reseed_batch)
+        fit.run()
 
     for _ in range(args.warmup):
         step()
@@ -329,19 +328,19 @@ def run_weft(args, world, rank, local, executor, cores):
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        f2 = BatchedFit(patches, pools, QUALITY, caps=[CAP] * len(patches), device=local)
-        f2.run(reseed_batch=reseed_batch)
+        f2 = BatchedFit.from_arrays(pixels, sizes, records, counts, QUALITY, caps=caps, device=local)
+        f2.run()
         idx = f2.selected_indices()
         b.record(stream)
         torch.cuda.synchronize()
         e2e_ms.append(a.elapsed_time(b))
-        h2d = int(f2.t_src.numel() * 4 + f2.t_cand.numel() + 4 * 6 * f2.n)
+        h2d = int(pixels.nbytes + records.nbytes + 4 * 6 * f2.n)
         d2h = int(f2.t_sel.numel() * 4 + f2.t_n_sel.numel() * 4 + 16 * len(f2.stats.per_round))
         del f2
-    e2e_val = world * n_px / (statistics.mean(e2e_ms) * 1e-3) / 1e6
+    e2e_val = world * n_px / (statistics.mean(e2e_ms) * 1e-3) / 1e6 if e2e_ms else None
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         pick = cpu_sample(patches, pools, args.cpu_budget_s, executor)
         v, wall, px = run_cpu(patches, pools, pick, executor, cores)
         cpu = {"value": v, "unit": "MPix/s", "cores": cores, "kind": "port",

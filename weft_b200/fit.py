@@ -82,22 +82,46 @@ class BatchedFit:
     """All tiles of a fit, resident on one GPU."""
 
     def __init__(self, patches, pools, quality: int = 75, caps=None, device: int = 0, reserve: int = RESEED_RESERVE):
+        """``patches``: per-tile (ts, ts, 3) float32 arrays; ``pools``: per-tile candidate
+        lists (``Cand``-like objects) or packed record arrays."""
+        patches = [np.ascontiguousarray(p, np.float32) for p in patches]
+        sizes = np.array([p.shape[0] for p in patches], np.int32)
+        pixels = np.concatenate([p.reshape(-1, 3) for p in patches]) if patches else np.zeros((0, 3), np.float32)
+        packed = [p if isinstance(p, np.ndarray) else pack_cands(p) for p in pools]
+        counts = np.array([len(p) for p in packed], np.int64)
+        records = np.concatenate(packed) if packed else np.zeros(0, PRIM_DTYPE)
+        self._setup(pixels, sizes, records, counts, quality, caps, device, reserve)
+        self.pools = [p if isinstance(p, np.ndarray) else list(p) for p in pools]
+        self.patches = patches
+
+    @classmethod
+    def from_arrays(cls, pixels: np.ndarray, sizes, records: np.ndarray, counts, quality: int = 75, caps=None,
+                    device: int = 0, reserve: int = RESEED_RESERVE) -> "BatchedFit":
+        """Flat inputs: ``pixels`` (sum ts^2, 3) float32 tile-major (row-major inside a
+        tile), ``sizes`` per tile, ``records`` all pools' 60-byte records back to back,
+        ``counts`` pool length per tile."""
+        self = cls.__new__(cls)
+        self._setup(np.asarray(pixels, np.float32), np.asarray(sizes, np.int32), np.asarray(records, PRIM_DTYPE),
+                    np.asarray(counts, np.int64), quality, caps, device, reserve)
+        self.pools = None
+        self.patches = None
+        return self
+
+    def _setup(self, pixels, sizes, records, counts, quality, caps, device, reserve) -> None:
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
         self.quality = int(quality)
         self.lam = rate.tile_lambda(quality)
         self.thr = rate.complexity_threshold(quality)
-        self.patches = [np.ascontiguousarray(p, np.float32) for p in patches]
-        n = len(self.patches)
+        n = len(sizes)
         self.n = n
-        self.sizes = np.array([p.shape[0] for p in self.patches], np.int32)
+        self.sizes = sizes
         if np.any(~np.isin(self.sizes, (8, 16, 32, 64))):
             raise ValueError("tile sizes must be 8, 16, 32 or 64")
         self.caps = np.array(caps if caps is not None else [MAX_PRIMS_BY_SIZE.get(int(s), 48) for s in self.sizes],
                              np.int32)
         self.cap_max = int(self.caps.max()) if n else 1
-        self.pools: list = [p if isinstance(p, np.ndarray) else list(p) for p in pools]
-        cnt = np.array([len(p) for p in self.pools], np.int64)
+        cnt = counts.astype(np.int64)
         self.pool_cap = cnt + reserve
         self.pool_off = np.zeros(n, np.int64)
         if n > 1:
@@ -106,16 +130,20 @@ class BatchedFit:
         if self.n_slots >= 2 ** 31:
             raise ValueError("too many candidate slots")
         self.pool_cnt = cnt.astype(np.int32)
+        self.init_cnt = self.pool_cnt.copy()
         px = self.sizes.astype(np.int64) ** 2
         self.px_off = np.zeros(n, np.int64)
         if n > 1:
             np.cumsum(px[:-1], out=self.px_off[1:])
         n_px = int(px.sum())
+        if pixels.shape != (n_px, 3):
+            raise ValueError(f"pixels must be ({n_px}, 3)")
+        if len(records) != int(cnt.sum()):
+            raise ValueError("records and counts disagree")
 
         d = self.device
-        src = np.zeros((n_px, 4), np.float32)
-        src[:, :3] = np.concatenate([p.reshape(-1, 3) for p in self.patches]) if n else np.zeros((0, 3))
-        self.t_src = _dev(src, d)
+        self.t_src = torch.zeros((n_px, 4), dtype=torch.float32, device=d)
+        self.t_src[:, :3] = _dev(pixels, d)
         self.t_bg = torch.zeros((n_px, 4), dtype=torch.float32, device=d)
         self.t_px_off = _dev(self.px_off.astype(np.int32), d)
         self.t_size = _dev(self.sizes, d)
@@ -129,27 +157,27 @@ class BatchedFit:
         self.t_flags = torch.zeros(n, dtype=torch.int32, device=d)
         self.t_cur_obj = torch.zeros(n, dtype=torch.float64, device=d)
         self.t_sel = torch.full((n * self.cap_max,), -1, dtype=torch.int32, device=d)
+        # slot of every packed record: pool_off of its tile + its index in the pool
+        first = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+        slots = np.repeat(self.pool_off - first, cnt) + np.arange(int(cnt.sum()))
         self.kinds = np.full(self.n_slots, 7, np.int8)
-        recs = np.zeros(self.n_slots, PRIM_DTYPE)
-        for t, pool in enumerate(self.pools):
-            if len(pool):
-                a = pool if isinstance(pool, np.ndarray) else pack_cands(pool)
-                recs[self.pool_off[t]:self.pool_off[t] + len(a)] = a
-        self.kinds[:] = np.where(recs["kind"] < 7, recs["kind"], 7)
+        self.kinds[slots] = np.where(records["kind"] < 7, records["kind"], 7)
         self._init_kinds = self.kinds.copy()
-        self.t_cand = _dev(recs.view(np.uint8), d)
-        self.t_prep = torch.zeros(self.n_slots * 16, dtype=torch.float32, device=d)
+        self.t_cand = torch.zeros((self.n_slots, PRIM_DTYPE.itemsize), dtype=torch.uint8, device=d)
+        if len(records):
+            self.t_cand[_dev(slots, d)] = _dev(np.ascontiguousarray(records).view(np.uint8).reshape(-1, PRIM_DTYPE.itemsize), d)
+        self.t_cand = self.t_cand.view(-1)
+        self.t_prep = torch.empty(self.n_slots * 16, dtype=torch.float32, device=d)
         self.t_alive = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
-        self.t_partial = torch.zeros(self.n_slots * 4, dtype=torch.float32, device=d)
+        self.t_partial = torch.empty(self.n_slots * 4, dtype=torch.float32, device=d)
         self.t_status = torch.zeros(4, dtype=torch.int32, device=d)
         self.t_work = torch.zeros(2, dtype=torch.int64, device=d)
         self.h_status = torch.zeros(4, dtype=torch.int32).pin_memory()
-        self.init_cnt = self.pool_cnt.copy()
         self.st = _lib.WeftFitState(
             n, self.cap_max, self.n_slots,
             *[_lib.ptr(x) for x in (self.t_src, self.t_bg, self.t_px_off, self.t_size, self.t_cap, self.t_pool_off,
-                                    self.t_pool_cnt, self.t_pool_cap, self.t_n_alive, self.t_n_sel, self.t_sel_bits, self.t_flags,
-                                    self.t_cur_obj, self.t_sel, self.t_cand, self.t_prep, self.t_alive,
+                                    self.t_pool_cnt, self.t_pool_cap, self.t_n_alive, self.t_n_sel, self.t_sel_bits,
+                                    self.t_flags, self.t_cur_obj, self.t_sel, self.t_cand, self.t_prep, self.t_alive,
                                     self.t_partial, self.t_status, self.t_work)])
         self.stats = FitStats()
         self.device_reseeded = False
@@ -252,6 +280,8 @@ class BatchedFit:
             s = int(self.sizes[t])
             a = int(self.px_off[t])
             preds.append(np.clip(bg[a:a + s * s, :3].reshape(s, s, 3), 0.0, 1.0))
+        if self.patches is None:
+            raise ValueError("host re-seeding needs the per-tile patches; use the device re-seed")
         if reseed_batch is not None:
             batch = reseed_batch([int(t) for t in tiles], [self.patches[t] for t in tiles], preds)
         else:
@@ -265,9 +295,10 @@ class BatchedFit:
             c0 = int(self.pool_cnt[t])
             if c0 + k > self.pool_cap[t]:
                 raise RuntimeError(f"tile {t}: re-seed overflows its {self.pool_cap[t]} candidate slots")
-            if isinstance(self.pools[t], np.ndarray):
-                self.pools[t] = unpack_cands(self.pools[t])
-            self.pools[t].extend(cands)
+            if self.pools is not None:
+                if isinstance(self.pools[t], np.ndarray):
+                    self.pools[t] = unpack_cands(self.pools[t])
+                self.pools[t].extend(cands)
             new_recs.append(pack_cands(cands))
             new_slots.append(self.pool_off[t] + c0 + np.arange(k))
             self.pool_cnt[t] = c0 + k
@@ -293,7 +324,7 @@ class BatchedFit:
         """Forget the fit (selections, re-seeds) but keep pixels and initial pools resident."""
         self.pool_cnt[:] = self.init_cnt
         self.device_reseeded = False
-        for t in range(self.n):
+        for t in range(self.n if self.pools is not None else 0):
             p = self.pools[t]
             if not isinstance(p, np.ndarray) and len(p) > self.init_cnt[t]:
                 del p[self.init_cnt[t]:]

@@ -275,7 +275,7 @@ def run_weft(args, world, rank, local, executor, cores):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     work = []
     rounds = []
-    n_classes = sum(1 for k in (8, 16, 32) if len(fit.items[k]))
+    n_classes = sum(1 for k in (8, 16, 32) if fit.n_items[k])
     torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(args.steps):

@@ -70,6 +70,7 @@ typedef struct WeftFitState {
     const WeftPrim* cand;    /* [n_slots] candidate records */
     float* prep;             /* [n_slots * 16] prepared per-candidate terms (64 B each) */
     uint8_t* alive;          /* [n_slots] 1 = still in the pool */
+    uint8_t* kind;           /* [n_slots] primitive kind of the slot (filled by prepare / re-seed) */
     float* partial;          /* [n_slots * 4] per-1024-pixel-block squared-error sums (scratch) */
     int32_t* status;         /* [4] round counters: evaluated tiles, improved tiles */
     unsigned long long* work; /* [2] running totals: candidate-pixels scored, algorithmic FP32 ops

@@ -41,7 +41,7 @@ class WeftFitState(ctypes.Structure):
     """Device pointers of a fit (include/weftk_fit.h)."""
     _fields_ = [("n_tiles", ctypes.c_int32), ("cap_max", ctypes.c_int32), ("n_slots", ctypes.c_int64)] + [
         (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "pool_cap", "n_alive",
-                                       "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive",
+                                       "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive", "kind",
                                        "partial", "status", "work")]
 
 
@@ -58,7 +58,7 @@ assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
 assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
 FIT_ITEM_DTYPE = np.dtype([("tile", np.int32), ("block", np.int32), ("first", np.int32), ("count", np.int32)])
 assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
-assert ctypes.sizeof(WeftFitState) == 16 + 20 * 8
+assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int

@@ -86,6 +86,7 @@ __global__ void fit_prepare_kernel(WeftFitState st, const int* __restrict__ firs
         dst[2] = make_float4(r.q[3], r.q[4], r.q[5], r.q[6]);
         dst[3] = make_float4(r.q[7], r.q[8], r.q[9], r.q[10]);
         st.alive[slot] = 1;
+        st.kind[slot] = (uint8_t)(c.kind >= 0 && c.kind < 8 ? c.kind : 7);
     }
     if (threadIdx.x == 0 && hi > lo) st.n_alive[t] += hi - lo;
 }
@@ -121,13 +122,22 @@ __global__ void fit_end_kernel(WeftFitState st, int mode, double complex_thresho
 }
 
 // ------------------------------------------------------------------ scoring
+// A CTA first gathers the live candidates of its run into shared memory (prepared
+// terms + slot), compacting out dead slots; warps then read their candidate's terms
+// as warp-uniform shared-memory broadcasts.  A curve's 31 polyline segments are
+// computed one per lane into the warp's segment table and read back the same way.
+constexpr int MAX_ITEM = 128;
+
 template <int PPL, int WPC>
 __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
                                                         const WeftFitItem* __restrict__ items, int n_items,
                                                         int expect_min, int expect_max) {
     constexpr int GROUPS = 4 / WPC;
-    constexpr int MAX_RUN = 64;
-    __shared__ float red[MAX_RUN][WPC];
+    __shared__ float4 s_prep[MAX_ITEM][4];
+    __shared__ int s_slot[MAX_ITEM];
+    __shared__ int s_wcount[4];
+    __shared__ float4 s_seg[4][32][2];
+    __shared__ float red[WPC > 1 ? MAX_ITEM : 1][WPC];
     if ((int)blockIdx.x >= n_items) return;
     const WeftFitItem w = items[blockIdx.x];
     const int t = w.tile;
@@ -137,8 +147,8 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
     }
     if (!(st.flags[t] & WEFTK_TILE_EVAL)) return;
     const int ts = st.size[t];
-    if (ts < expect_min || ts > expect_max || (WPC > 1 && w.count > MAX_RUN) || w.block * 1024 >= ts * ts ||
-        w.first < 0 || w.first + w.count > st.pool_cap[t]) {
+    if (ts < expect_min || ts > expect_max || w.count > MAX_ITEM || w.block * 1024 >= ts * ts || w.first < 0 ||
+        w.first + w.count > st.pool_cap[t]) {
         if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
         return;
     }
@@ -146,32 +156,77 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
     const int count = min(w.count, st.pool_cnt[t] - w.first);
     if (count <= 0) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int group = warp / WPC, wig = warp % WPC;
     const long long off = st.pool_off[t];
+
+    // stage live candidates (order-preserving compaction with warp ballots)
+    long long my_slot = -1;
+    bool live = false;
+    if ((int)threadIdx.x < count) {
+        my_slot = off + perm[off + w.first + threadIdx.x];
+        live = st.alive[my_slot] != 0;
+    }
+    const unsigned bal = __ballot_sync(FULL, live);
+    if (lane == 0) s_wcount[warp] = __popc(bal);
+    __syncthreads();
+    int base = 0;
+    for (int k = 0; k < warp; ++k) base += s_wcount[k];
+    const int m = s_wcount[0] + s_wcount[1] + s_wcount[2] + s_wcount[3];
+    if (live) {
+        const int pos = base + __popc(bal & ((1u << lane) - 1u));
+        const float4* src4 = reinterpret_cast<const float4*>(st.prep) + my_slot * 4;
+        s_prep[pos][0] = __ldg(src4);
+        s_prep[pos][1] = __ldg(src4 + 1);
+        s_prep[pos][2] = __ldg(src4 + 2);
+        s_prep[pos][3] = __ldg(src4 + 3);
+        s_slot[pos] = (int)(my_slot - off);
+    }
+    __syncthreads();
+    if (m == 0) return;
+
+    const int group = warp / WPC, wig = warp % WPC;
     const float4* src = reinterpret_cast<const float4*>(st.src) + st.px_off[t];
     const float4* bg = reinterpret_cast<const float4*>(st.bg) + st.px_off[t];
     const int pbase = w.block * 1024 + wig * 32 * PPL;
-
     float fx[PPL], fy[PPL];
-    float4 s[PPL], g[PPL];
+    float3 s[PPL], g[PPL];
 #pragma unroll
     for (int j = 0; j < PPL; ++j) {
         const int p = pbase + j * 32 + lane;
         fx[j] = (float)(p % ts) + 0.5f;
         fy[j] = (float)(p / ts) + 0.5f;
-        s[j] = src[p];
-        g[j] = bg[p];
+        const float4 a = src[p], b = bg[p];
+        s[j] = make_float3(a.x, a.y, a.z);
+        g[j] = make_float3(b.x, b.y, b.z);
     }
-    unsigned long long ops = 0, cpx = 0;
-    for (int c = group; c < count; c += GROUPS) {
-        const int local = perm[off + w.first + c];
-        const long long slot = off + local;
-        if (!st.alive[slot]) continue;
-        const Prep P = load_prep(st.prep, slot);
-        cpx += 32 * PPL;
-        ops += (unsigned long long)(32 * PPL) * (unsigned long long)(kind_ops(st.cand[slot].kind) + 9);
+    unsigned long long ops = 0;
+    for (int c = group; c < m; c += GROUPS) {
+        Prep P;
+        {
+            const float4 a = s_prep[c][0], b = s_prep[c][1], cc = s_prep[c][2], d = s_prep[c][3];
+            P.kind = __float_as_int(a.x);
+            P.a = a.y; P.cr = a.z; P.cg = a.w; P.cb = b.x;
+            P.q[0] = b.y; P.q[1] = b.z; P.q[2] = b.w;
+            P.q[3] = cc.x; P.q[4] = cc.y; P.q[5] = cc.z; P.q[6] = cc.w;
+            P.q[7] = d.x; P.q[8] = d.y; P.q[9] = d.z; P.q[10] = d.w;
+        }
+        ops += (unsigned long long)(32 * PPL) * (unsigned long long)(kind_ops(P.kind) + 9);
         float a[PPL], sr[PPL], sg[PPL], sb[PPL];
-        prim_eval<PPL>(P, fx, fy, a, sr, sg, sb, lane);
+        if (P.kind == K_CURVE) {
+            const Seg sg1 = lane_segment(P, lane);
+            s_seg[warp][lane][0] = make_float4(sg1.ax, sg1.ay, sg1.vx, sg1.vy);
+            s_seg[warp][lane][1] = make_float4(sg1.ux, sg1.uy, 0.0f, 0.0f);
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < PPL; ++j) {
+                sr[j] = P.cr;
+                sg[j] = P.cg;
+                sb[j] = P.cb;
+            }
+            curve_alpha_smem<PPL>(P, s_seg[warp], fx, fy, a);
+            __syncwarp();
+        } else {
+            prim_eval<PPL>(P, fx, fy, a, sr, sg, sb, lane);
+        }
         float e = 0.0f;
 #pragma unroll
         for (int j = 0; j < PPL; ++j) {
@@ -182,26 +237,24 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
         }
         e = warp_sum_f(e);
         if (WPC == 1) {
-            if (lane == 0) st.partial[slot * 4] = e;
+            if (lane == 0) st.partial[(off + s_slot[c]) * 4] = e;
         } else if (lane == 0) {
             red[c][wig] = e;
         }
     }
-    if (st.work != nullptr && lane == 0 && cpx) {
-        atomicAdd(&st.work[0], cpx);
-        atomicAdd(&st.work[1], ops);
-    }
+    if (st.work != nullptr && lane == 0 && ops) atomicAdd(&st.work[1], ops);
     if (WPC > 1) {
         __syncthreads();
-        for (int c = threadIdx.x; c < count; c += blockDim.x) {
-            const long long slot = off + perm[off + w.first + c];
-            if (!st.alive[slot]) continue;
+        for (int c = threadIdx.x; c < m; c += blockDim.x) {
             float e = red[c][0];
 #pragma unroll
             for (int k = 1; k < WPC; ++k) e += red[c][k];
-            st.partial[slot * 4 + w.block] = e;
+            st.partial[(off + s_slot[c]) * 4 + w.block] = e;
         }
     }
+    // candidate-pixels of this CTA: every live candidate over its 1024-pixel block or whole tile
+    if (st.work != nullptr && threadIdx.x == 0)
+        atomicAdd(&st.work[0], (unsigned long long)m * (unsigned long long)(WPC * 32 * PPL));
 }
 
 // ------------------------------------------------------------------ select / accept
@@ -223,7 +276,7 @@ __global__ void __launch_bounds__(128) fit_select_kernel(WeftFitState st, int mo
         float sse = st.partial[slot * 4];
         for (int b = 1; b < nb; ++b) sse += st.partial[slot * 4 + b];
         const float mse = __fdiv_rn(sse, denom);
-        const float obj = __fadd_rn(mse, __fmul_rn(lam_f, (float)(base_bits + prim_bits(st.cand[slot].kind))));
+        const float obj = __fadd_rn(mse, __fmul_rn(lam_f, (float)(base_bits + prim_bits(st.kind[slot]))));
         if (obj < best || (obj == best && c < bi)) {
             best = obj;
             bi = c;
@@ -242,7 +295,7 @@ __global__ void __launch_bounds__(128) fit_select_kernel(WeftFitState st, int mo
     const bool accept = (mode == WEFTK_FIT_INIT) || ((double)best < st.cur_obj[t]);
     if (!accept) return;
     const long long slot = off + bi;
-    const int kind = st.cand[slot].kind;
+    const int kind = st.kind[slot];
     if (lane == 0) {
         const int k = st.n_sel[t];
         if (k < st.cap_max) st.sel[(long long)t * st.cap_max + k] = bi;

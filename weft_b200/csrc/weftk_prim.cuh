@@ -25,9 +25,10 @@ constexpr unsigned FULL = 0xffffffffu;
 
 enum Kind : int { K_CONST = 0, K_LINEAR = 1, K_LINE = 2, K_CURVE = 3, K_TRI = 4, K_BICUBIC = 5, K_SKIP = -1 };
 
-// Per-primitive hoisted terms.  q[] meaning by kind:
-//   linear:   X0 Y0 VX VY IDEN c1r c1g c1b
-//   line:     X0 Y0 VX VY IDEN K          (alpha = exp(K * d^2) * a)
+// Per-primitive hoisted terms.  q[] meaning by kind (U = V / (|V|^2 + 1e-8), the
+// projection vector, so the clamped segment parameter is t = clamp(D . U)):
+//   linear:   X0 Y0 UX UY c1r c1g c1b
+//   line:     X0 Y0 VX VY UX UY K         (alpha = exp(K * d^2) * a)
 //   curve:    K p0x p0y cx cy p1x p1y
 //   triangle: X2 Y2 A B C D DEN           (a = (A dx + B dy)/DEN, b = (C dx + D dy)/DEN)
 //   bicubic:  index of the 48-value control grid (as float)
@@ -68,15 +69,18 @@ __device__ __forceinline__ Prep prep_prim(const WeftPrim& P) {
             double den = vx * vx + vy * vy + 1e-8;
             r.q[0] = g[0];
             r.q[1] = g[1];
-            r.q[2] = (float)vx;
-            r.q[3] = (float)vy;
-            r.q[4] = 1.0f / (float)den;
             if (P.kind == K_LINEAR) {
-                r.q[5] = P.color1[0];
-                r.q[6] = P.color1[1];
-                r.q[7] = P.color1[2];
+                r.q[2] = (float)(vx / den);
+                r.q[3] = (float)(vy / den);
+                r.q[4] = P.color1[0];
+                r.q[5] = P.color1[1];
+                r.q[6] = P.color1[2];
             } else {
-                r.q[5] = gauss_k(g[4]);
+                r.q[2] = (float)vx;
+                r.q[3] = (float)vy;
+                r.q[4] = (float)(vx / den);
+                r.q[5] = (float)(vy / den);
+                r.q[6] = gauss_k(g[4]);
             }
             break;
         }
@@ -123,8 +127,9 @@ __device__ __forceinline__ float2 bezier_point(const Prep& P, int i) {
 }
 
 // Segment owned by this lane (lane s: point s -> point s+1); lane 31's is unused.
+// (ax, ay) start, (vx, vy) direction, (ux, uy) = v / (|v|^2 + 1e-8).
 struct Seg {
-    float ax, ay, vx, vy, iden;
+    float ax, ay, vx, vy, ux, uy;
 };
 
 __device__ __forceinline__ Seg lane_segment(const Prep& P, int lane) {
@@ -136,14 +141,17 @@ __device__ __forceinline__ Seg lane_segment(const Prep& P, int lane) {
     s.vx = __fsub_rn(n.x, p.x);
     s.vy = __fsub_rn(n.y, p.y);
     float den = __fadd_rn(__fadd_rn(__fmul_rn(s.vx, s.vx), __fmul_rn(s.vy, s.vy)), 1e-8f);
-    s.iden = 1.0f / den;
+    s.ux = __fdiv_rn(s.vx, den);
+    s.uy = __fdiv_rn(s.vy, den);
     return s;
 }
 
-// Squared distance from (px,py) to the segment (ax,ay)+t(vx,vy), t clamped to [0,1].
-__device__ __forceinline__ float seg_d2(float px, float py, float ax, float ay, float vx, float vy, float iden) {
+// Squared distance from (px,py) to the segment (ax,ay)+t(vx,vy), t = clamp((p-a).u) in [0,1].
+// Every kernel uses this one formula, so cached composites equal full re-renders bit for bit.
+__device__ __forceinline__ float seg_d2(float px, float py, float ax, float ay, float vx, float vy, float ux,
+                                        float uy) {
     float dx = px - ax, dy = py - ay;
-    float t = clamp01(fmaf(dx, vx, dy * vy) * iden);
+    float t = clamp01(fmaf(dx, ux, dy * uy));
     float ex = fmaf(-t, vx, dx), ey = fmaf(-t, vy, dy);
     return fmaf(ex, ex, ey * ey);
 }
@@ -179,19 +187,19 @@ __device__ __forceinline__ void prim_eval(const Prep& P, const float (&fx)[PPL],
         case K_LINEAR:
 #pragma unroll
             for (int j = 0; j < PPL; ++j) {
-                float t = clamp01(fmaf(fx[j] - P.q[0], P.q[2], (fy[j] - P.q[1]) * P.q[3]) * P.q[4]);
+                float t = clamp01(fmaf(fx[j] - P.q[0], P.q[2], (fy[j] - P.q[1]) * P.q[3]));
                 float u = 1.0f - t;
-                sr[j] = fmaf(P.q[5], t, P.cr * u);
-                sg[j] = fmaf(P.q[6], t, P.cg * u);
-                sb[j] = fmaf(P.q[7], t, P.cb * u);
+                sr[j] = fmaf(P.q[4], t, P.cr * u);
+                sg[j] = fmaf(P.q[5], t, P.cg * u);
+                sb[j] = fmaf(P.q[6], t, P.cb * u);
                 a[j] = P.a;
             }
             break;
         case K_LINE:
 #pragma unroll
             for (int j = 0; j < PPL; ++j) {
-                float d2 = seg_d2(fx[j], fy[j], P.q[0], P.q[1], P.q[2], P.q[3], P.q[4]);
-                a[j] = expf(d2 * P.q[5]) * P.a;
+                float d2 = seg_d2(fx[j], fy[j], P.q[0], P.q[1], P.q[2], P.q[3], P.q[4], P.q[5]);
+                a[j] = expf(d2 * P.q[6]) * P.a;
             }
             break;
         case K_CURVE: {
@@ -203,9 +211,9 @@ __device__ __forceinline__ void prim_eval(const Prep& P, const float (&fx)[PPL],
             for (int k = 0; k < 31; ++k) {
                 float ax = __shfl_sync(FULL, s.ax, k), ay = __shfl_sync(FULL, s.ay, k);
                 float vx = __shfl_sync(FULL, s.vx, k), vy = __shfl_sync(FULL, s.vy, k);
-                float iden = __shfl_sync(FULL, s.iden, k);
+                float ux = __shfl_sync(FULL, s.ux, k), uy = __shfl_sync(FULL, s.uy, k);
 #pragma unroll
-                for (int j = 0; j < PPL; ++j) best[j] = fminf(best[j], seg_d2(fx[j], fy[j], ax, ay, vx, vy, iden));
+                for (int j = 0; j < PPL; ++j) best[j] = fminf(best[j], seg_d2(fx[j], fy[j], ax, ay, vx, vy, ux, uy));
             }
 #pragma unroll
             for (int j = 0; j < PPL; ++j) a[j] = expf(best[j] * P.q[0]) * P.a;
@@ -218,6 +226,26 @@ __device__ __forceinline__ void prim_eval(const Prep& P, const float (&fx)[PPL],
         default:
             break;  // skipped primitive: a = 0, blend is the identity
     }
+}
+
+// Same as prim_eval for kind K_CURVE, with the warp's 31 segments already in shared
+// memory (seg[k] = {ax, ay, vx, vy}, {ux, uy, -, -}); reads are warp-uniform broadcasts.
+template <int PPL>
+__device__ __forceinline__ void curve_alpha_smem(const Prep& P, const float4 (*seg)[2], const float (&fx)[PPL],
+                                                 const float (&fy)[PPL], float (&a)[PPL]) {
+    float best[PPL];
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) best[j] = 1e18f;
+#pragma unroll 2
+    for (int k = 0; k < 31; ++k) {
+        const float4 s0 = seg[k][0];
+        const float4 s1 = seg[k][1];
+#pragma unroll
+        for (int j = 0; j < PPL; ++j)
+            best[j] = fminf(best[j], seg_d2(fx[j], fy[j], s0.x, s0.y, s0.z, s0.w, s1.x, s1.y));
+    }
+#pragma unroll
+    for (int j = 0; j < PPL; ++j) a[j] = expf(best[j] * P.q[0]) * P.a;
 }
 
 // "over" blend, identical sequence in every kernel so incremental and full renders agree bit for bit.

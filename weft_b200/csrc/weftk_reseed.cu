@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(RS_THREADS) fit_reseed_kernel(WeftFitState st)
         pp[2] = make_float4(r.q[3], r.q[4], r.q[5], r.q[6]);
         pp[3] = make_float4(r.q[7], r.q[8], r.q[9], r.q[10]);
         st.alive[slot] = 1;
+        st.kind[slot] = (uint8_t)s.cand[tid].kind;
     }
     if (tid == 0) {
         st.pool_cnt[t] = base_cnt + n_new;

@@ -169,6 +169,7 @@ class BatchedFit:
         self.t_cand = self.t_cand.view(-1)
         self.t_prep = torch.empty(self.n_slots * 16, dtype=torch.float32, device=d)
         self.t_alive = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
+        self.t_kind = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
         self.t_partial = torch.empty(self.n_slots * 4, dtype=torch.float32, device=d)
         self.t_status = torch.zeros(4, dtype=torch.int32, device=d)
         self.t_work = torch.zeros(2, dtype=torch.int64, device=d)
@@ -178,9 +179,10 @@ class BatchedFit:
             *[_lib.ptr(x) for x in (self.t_src, self.t_bg, self.t_px_off, self.t_size, self.t_cap, self.t_pool_off,
                                     self.t_pool_cnt, self.t_pool_cap, self.t_n_alive, self.t_n_sel, self.t_sel_bits,
                                     self.t_flags, self.t_cur_obj, self.t_sel, self.t_cand, self.t_prep, self.t_alive,
-                                    self.t_partial, self.t_status, self.t_work)])
+                                    self.t_kind, self.t_partial, self.t_status, self.t_work)])
         self.stats = FitStats()
         self.device_reseeded = False
+        self.n_items = {}
         self._prepare(np.zeros(n, np.int32))
         self._build_work()
 
@@ -200,59 +202,57 @@ class BatchedFit:
         The initial pool is scored in kind order (curves first) so a work item
         holds candidates of similar cost; re-seeded slots are scored in slot
         order.  Items cover the reserved slots too; the kernel only scores the
-        filled ones, so re-seeding needs no new items.
+        filled ones, so re-seeding needs no new items.  Sorting runs on the GPU.
         """
+        d = self.device
         n = self.n
-        cnt = self.init_cnt.astype(np.int64)
-        cap = self.pool_cap.astype(np.int64)
-        tile_of = np.repeat(np.arange(n), cnt)
-        first_of_tile = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64)
-        local = np.arange(int(cnt.sum())) - np.repeat(first_of_tile, cnt)
-        slot = np.repeat(self.pool_off, cnt) + local
-        cost = KIND_COST[self.kinds[slot]]
-        order = np.lexsort((local, -cost, tile_of))
-        cap_first = np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.int64)
-        perm = (np.arange(self.n_slots, dtype=np.int64) - np.repeat(cap_first, cap)).astype(np.int32)
-        perm[slot] = local[order]
-        self.t_perm = _dev(perm, self.device)
-        # cost of a run of slots in scoring order (reserved slots: a typical re-seed mix)
-        slot_cost = np.full(self.n_slots, 60, np.int64)
-        slot_cost[slot] = cost[order]
-        csum = np.concatenate([[0], np.cumsum(slot_cost)])
+        cap = torch.from_numpy(self.pool_cap).to(d)
+        cnt = torch.from_numpy(self.init_cnt.astype(np.int64)).to(d)
+        off = torch.from_numpy(self.pool_off).to(d)
+        kinds = torch.from_numpy(self._init_kinds.astype(np.int64)).to(d)
+        tile_of = torch.repeat_interleave(torch.arange(n, device=d), cap)
+        local = torch.arange(self.n_slots, device=d) - torch.repeat_interleave(off, cap)
+        filled = local < cnt[tile_of]
+        cost = torch.from_numpy(KIND_COST).to(d)[kinds]
+        # order inside each tile: filled slots by descending cost (stable), then the reserve
+        key = tile_of * (1 << 20) + torch.where(filled, 1023 - cost, torch.full_like(cost, 1 << 12))
+        order = torch.sort(key, stable=True).indices
+        perm = local[order].to(torch.int32)
+        self.t_perm = perm.contiguous()
+        slot_cost = torch.where(filled, cost, torch.zeros_like(cost))[order]
+        csum = torch.cat([torch.zeros(1, dtype=torch.int64, device=d), torch.cumsum(slot_cost, 0)])
+        sizes = torch.from_numpy(self.sizes.astype(np.int64)).to(d)
         items = {}
-        for cls, sizes in ((8, (8,)), (16, (16,)), (32, (32, 64))):
+        for cls, members in ((8, (8,)), (16, (16,)), (32, (32, 64))):
             chunk = CHUNK[cls]
-            rows = []
-            for s in sizes:
-                ts_idx = np.nonzero(self.sizes == s)[0]
-                if ts_idx.size == 0:
-                    continue
-                nch = (cap[ts_idx] + chunk - 1) // chunk
-                t_rep = np.repeat(ts_idx, nch)
-                k = np.arange(int(nch.sum())) - np.repeat(np.concatenate([[0], np.cumsum(nch)[:-1]]), nch)
-                first = k * chunk
-                count = np.minimum(chunk, cap[t_rep] - first)
-                g0 = self.pool_off[t_rep] + first
-                c = (csum[g0 + count] - csum[g0]) * (s * s)
-                # runs that start in the reserved region only cost once re-seeded
-                c = np.where(first >= cnt[t_rep], 0, c)
-                blocks = max(1, (s * s) // 1024)
-                for b in range(blocks):
-                    rows.append(np.stack([t_rep, np.full_like(t_rep, b), first, count, c], axis=1))
-            if rows:
-                r = np.concatenate(rows)
-                r = r[np.argsort(-r[:, 4], kind="stable")]
-                arr = np.zeros(len(r), FIT_ITEM_DTYPE)
-                arr["tile"], arr["block"], arr["first"], arr["count"] = r[:, 0], r[:, 1], r[:, 2], r[:, 3]
-            else:
-                arr = np.zeros(0, FIT_ITEM_DTYPE)
-            items[cls] = arr
-        self.items = items
-        self.t_items = {k: _dev(v.view(np.uint8), self.device) if len(v) else None for k, v in items.items()}
+            sel = torch.zeros(n, dtype=torch.bool, device=d)
+            for m in members:
+                sel |= sizes == m
+            ts_idx = torch.nonzero(sel).flatten()
+            if ts_idx.numel() == 0:
+                items[cls] = None
+                self.n_items[cls] = 0
+                continue
+            nch = (cap[ts_idx] + chunk - 1) // chunk
+            t_rep = torch.repeat_interleave(ts_idx, nch)
+            k = torch.arange(int(nch.sum()), device=d) - torch.repeat_interleave(torch.cumsum(nch, 0) - nch, nch)
+            first = k * chunk
+            count = torch.minimum(torch.full_like(first, chunk), cap[t_rep] - first)
+            g0 = off[t_rep] + first
+            px = sizes[t_rep] ** 2
+            c = (csum[g0 + count] - csum[g0]) * px
+            blocks = torch.clamp(px // 1024, min=1)
+            b_rep = torch.repeat_interleave(torch.arange(t_rep.numel(), device=d), blocks)
+            blk = torch.arange(b_rep.numel(), device=d) - torch.repeat_interleave(torch.cumsum(blocks, 0) - blocks, blocks)
+            rows = torch.stack([t_rep[b_rep], blk, first[b_rep], count[b_rep]], 1).to(torch.int32)
+            o = torch.sort(-c[b_rep], stable=True).indices
+            items[cls] = rows[o].contiguous()
+            self.n_items[cls] = int(rows.shape[0])
+        self.t_items = items
 
     def _round(self, mode: int) -> tuple[int, int]:
         ti = self.t_items
-        n8, n16, n32 = (len(self.items[k]) for k in (8, 16, 32))
+        n8, n16, n32 = (self.n_items[k] for k in (8, 16, 32))
         rc = self.lib.weftk_fit_round(ctypes_ref(self.st), mode, self.lam, self.thr, _lib.ptr(self.t_perm),
                                       _lib.ptr(ti[8]), n8, _lib.ptr(ti[16]), n16, _lib.ptr(ti[32]), n32,
                                       self._stream())

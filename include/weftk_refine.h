@@ -1,0 +1,56 @@
+/*
+ * weftk_refine.h — per-tile stack loss and its hand-written backward (C ABI of libweftk.so).
+ *
+ * No counterpart in the reference renderer's interface: the reference has no
+ * differentiable path (its refinement is discrete perturbation).  The forward is
+ * the reference's objective without the rate term (src/weft/encoder.py:271-285):
+ * loss[t] = mean over pixels and channels of (clip(render(stack_t)) - src)^2, with
+ * render = the reference CPU renderer's over-composite at pixel centres
+ * (src/weft/render.py:127-234).  The backward recomputes coverage per pixel (no
+ * per-pixel state is stored in HBM) and returns d(sum_t g[t] * loss[t]) / d params.
+ *
+ * Parameter rows: float[16] per primitive
+ *   [0..6]  geom (kind-specific, as WeftPrim.geom)   [7..9]  color0
+ *   [10..12] color1 (linear patch)                   [13]    alpha     [14..15] unused
+ * Gradients exist for geometry (positions, thickness), colours and opacity.
+ * Triangle coverage is a step function; its geometry gradient uses a soft-edge
+ * surrogate (product of logistic functions of the signed edge distances,
+ * width 0.5 px) in the backward only.  WEFTK_SOFT_TRIANGLES makes the forward use
+ * the same surrogate, which is what a finite-difference check of the surrogate
+ * differentiates.  Bicubic (kind 5) rows are inert.
+ */
+#ifndef WEFTK_REFINE_H
+#define WEFTK_REFINE_H
+
+#include "weftk.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WEFTK_SOFT_TRIANGLES 2
+#define WEFTK_REFINE_MAX_PRIMS 32 /* longest stack the refine kernels accept */
+
+typedef struct WeftStackSet {
+    int32_t n_tiles;
+    int32_t max_prims;        /* longest stack (<= WEFTK_REFINE_MAX_PRIMS) */
+    const float* src;         /* float4 (r, g, b, 0) per pixel, tile-major */
+    const int32_t* px_off;    /* [n_tiles] first pixel of the tile */
+    const int32_t* size;      /* [n_tiles] tile side (1..64) */
+    const int32_t* prim_off;  /* [n_tiles + 1] tile t owns parameter rows [prim_off[t], prim_off[t+1]) */
+    const int32_t* kind;      /* [n_prims] primitive kind of each row */
+} WeftStackSet;
+
+/* loss[t] for every tile (float32). */
+int weftk_stack_loss(const WeftStackSet* set, const float* d_params, float* d_loss, int flags, void* stream);
+
+/* grad_params = sum_t grad_loss[t] * d loss[t] / d params (rows of untouched
+ * tiles are written with zeros; rows are owned by one tile, so no atomics). */
+int weftk_stack_loss_backward(const WeftStackSet* set, const float* d_params, const float* d_grad_loss,
+                              float* d_grad_params, int flags, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WEFTK_REFINE_H */

@@ -45,6 +45,12 @@ class WeftFitState(ctypes.Structure):
                                        "partial", "status", "work")]
 
 
+class WeftStackSet(ctypes.Structure):
+    """Device pointers of a set of per-tile stacks (include/weftk_refine.h)."""
+    _fields_ = [("n_tiles", ctypes.c_int32), ("max_prims", ctypes.c_int32)] + [
+        (n, ctypes.c_void_p) for n in ("src", "px_off", "size", "prim_off", "kind")]
+
+
 # numpy mirrors of the C structs (same byte layout)
 PRIM_DTYPE = np.dtype([("kind", np.int32), ("geom", np.float32, 7), ("color0", np.float32, 3),
                        ("color1", np.float32, 3), ("alpha", np.float32)])
@@ -78,6 +84,8 @@ SIGNATURES: dict[str, list] = {
     "weftk_fit_round": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],
     "weftk_fit_timing": [_I, _P, _P],
     "weftk_fit_reseed": [_P, _I, _P],
+    "weftk_stack_loss": [_P, _P, _P, _I, _P],
+    "weftk_stack_loss_backward": [_P, _P, _P, _P, _I, _P],
     "weftk_measure_fp32_peak": [_P],
 }
 

@@ -1,0 +1,192 @@
+"""Gradient refinement of fitted primitive stacks (host side of include/weftk_refine.h).
+
+``StackSet`` holds per-tile stacks on the GPU (parameter rows float32[16]:
+geom[0..6], color0[7..9], color1[10..12], alpha[13]); ``StackLoss`` is the
+``torch.autograd.Function`` whose forward is ``weftk_stack_loss`` (per-tile MSE
+of the rendered stack) and whose backward is the hand-written
+``weftk_stack_loss_backward``.  ``refine`` runs a fixed number of Adam steps on
+the parameters, projecting them after every step onto what the bitstream can
+carry (src/weft/primitives.py:102-177: colours and alpha in [0, 1], coordinates
+in [0, 15], thickness in [0, 4]); ``quantize_params`` snaps them to the wire grid
+exactly as the reference's ``_quantize_primitive`` (src/weft/encoder.py:211-237).
+
+This path has no reference counterpart (the reference's refinement is discrete
+perturbation); its correctness is pinned by central finite differences and a
+float64 PyTorch autograd restatement in the tests.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import PRIM_DTYPE
+
+SOFT_TRIANGLES = 2
+MAX_PRIMS = 32
+GEOM_LEN = {0: 0, 1: 4, 2: 5, 3: 7, 4: 6, 5: 0}
+
+
+def records_to_rows(recs: np.ndarray) -> np.ndarray:
+    """60-byte primitive records -> float32[n, 16] parameter rows."""
+    rows = np.zeros((len(recs), 16), np.float32)
+    rows[:, 0:7] = recs["geom"]
+    rows[:, 7:10] = recs["color0"]
+    rows[:, 10:13] = recs["color1"]
+    rows[:, 13] = recs["alpha"]
+    return rows
+
+
+def rows_to_records(rows: np.ndarray, kinds: np.ndarray) -> np.ndarray:
+    recs = np.zeros(len(rows), PRIM_DTYPE)
+    recs["kind"] = kinds
+    recs["geom"] = rows[:, 0:7]
+    recs["color0"] = rows[:, 7:10]
+    recs["color1"] = rows[:, 10:13]
+    recs["alpha"] = rows[:, 13]
+    return recs
+
+
+class StackSet:
+    """Per-tile stacks over tile pixels resident on the GPU."""
+
+    def __init__(self, src: torch.Tensor, px_off: torch.Tensor, sizes: torch.Tensor, prim_off: np.ndarray,
+                 kinds: np.ndarray, device: int = 0):
+        self.device = torch.device("cuda", device)
+        self.lib = _lib.lib_for_device(device)
+        self.n = int(sizes.numel())
+        counts = np.diff(prim_off)
+        self.max_prims = int(counts.max()) if counts.size else 0
+        if self.max_prims > MAX_PRIMS:
+            raise ValueError(f"stacks longer than {MAX_PRIMS} primitives are not supported")
+        self.src, self.px_off, self.sizes = src, px_off, sizes
+        self.prim_off_np = np.asarray(prim_off, np.int64)
+        self.kinds_np = np.asarray(kinds, np.int32)
+        self.t_prim_off = torch.from_numpy(self.prim_off_np.astype(np.int32)).to(self.device)
+        self.t_kind = torch.from_numpy(self.kinds_np).to(self.device)
+        self.st = _lib.WeftStackSet(self.n, self.max_prims, _lib.ptr(src), _lib.ptr(px_off), _lib.ptr(sizes),
+                                    _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind))
+        n_px = (sizes.to(torch.int64) ** 2)
+        self.weights = (n_px.to(torch.float32) / float(n_px.sum().item())) if self.n else n_px.float()
+
+    @classmethod
+    def from_fit(cls, fit) -> tuple["StackSet", torch.Tensor]:
+        """The selected stacks of a ``BatchedFit`` (tiles stay where the fit put them)."""
+        recs = fit.selected_records()
+        counts = np.array([len(r) for r in recs], np.int64)
+        prim_off = np.concatenate([[0], np.cumsum(counts)])
+        flat = np.concatenate(recs) if recs else np.zeros(0, PRIM_DTYPE)
+        set_ = cls(fit.t_src, fit.t_px_off, fit.t_size, prim_off, flat["kind"], fit.device.index or 0)
+        return set_, torch.from_numpy(records_to_rows(flat)).to(set_.device)
+
+    @classmethod
+    def from_stacks(cls, patches, stacks, device: int = 0) -> tuple["StackSet", torch.Tensor]:
+        """Tiles (ts, ts, 3) and per-tile primitive lists (objects with kind/geom/color0/color1/alpha)."""
+        d = torch.device("cuda", device)
+        sizes = np.array([p.shape[0] for p in patches], np.int32)
+        px = sizes.astype(np.int64) ** 2
+        px_off = np.concatenate([[0], np.cumsum(px)[:-1]]).astype(np.int32)
+        src = np.zeros((int(px.sum()), 4), np.float32)
+        src[:, :3] = np.concatenate([np.asarray(p, np.float32).reshape(-1, 3) for p in patches])
+        from .fit import pack_cands
+
+        recs = [pack_cands(s) for s in stacks]
+        counts = np.array([len(r) for r in recs], np.int64)
+        flat = np.concatenate(recs) if recs else np.zeros(0, PRIM_DTYPE)
+        t_src = torch.from_numpy(src).to(d)
+        set_ = cls(t_src, torch.from_numpy(px_off).to(d), torch.from_numpy(sizes).to(d),
+                   np.concatenate([[0], np.cumsum(counts)]), flat["kind"], device)
+        set_._keep = t_src
+        return set_, torch.from_numpy(records_to_rows(flat)).to(d)
+
+    def _stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def loss(self, params: torch.Tensor, soft: bool = False) -> torch.Tensor:
+        params = params.detach().contiguous()
+        out = torch.empty(self.n, dtype=torch.float32, device=self.device)
+        _lib.check(self.lib.weftk_stack_loss(ctypes_addr(self.st), _lib.ptr(params), _lib.ptr(out),
+                                             SOFT_TRIANGLES if soft else 0, self._stream()), "weftk_stack_loss")
+        return out
+
+    def loss_backward(self, params: torch.Tensor, grad_loss: torch.Tensor, soft: bool = False) -> torch.Tensor:
+        params = params.detach().contiguous()
+        g = grad_loss.detach().to(torch.float32).contiguous()
+        out = torch.zeros_like(params)
+        _lib.check(self.lib.weftk_stack_loss_backward(ctypes_addr(self.st), _lib.ptr(params), _lib.ptr(g),
+                                                      _lib.ptr(out), SOFT_TRIANGLES if soft else 0, self._stream()),
+                   "weftk_stack_loss_backward")
+        return out
+
+    # --------------------------------------------------------------- parameter space
+    def project_(self, params: torch.Tensor) -> None:
+        """Clamp rows onto what the wire format can represent (in place)."""
+        with torch.no_grad():
+            params[:, 7:14].clamp_(0.0, 1.0)
+            k = self.t_kind
+            geo = params[:, 0:7]
+            geo.clamp_(0.0, 15.0)
+            thick = torch.where(k == 2, 4, torch.where(k == 3, 6, -1))
+            rows = torch.nonzero(thick >= 0).flatten()
+            if rows.numel():
+                cols = thick[rows].long()
+                params[rows, cols] = params[rows, cols].clamp(0.0, 4.0)
+
+    def quantize(self, params: torch.Tensor) -> torch.Tensor:
+        """Snap to the wire grid: coordinates u16 over [0, 15], thickness u16 over [0, 4],
+        colours u8, alpha u16 (half-to-even rounding, as Python's round)."""
+        p = params.detach().to(torch.float64).clone()
+        k = self.t_kind
+        p[:, 7:13] = torch.round(p[:, 7:13].clamp(0, 1) * 255.0) / 255.0
+        p[:, 13] = torch.round(p[:, 13].clamp(0, 1) * 65535.0) / 65535.0
+        g = torch.round((p[:, 0:7] / 15.0).clamp(0, 1) * 65535.0) / 65535.0 * 15.0
+        th = torch.where(k == 2, 4, torch.where(k == 3, 6, -1))
+        gt = torch.round((p[:, 0:7] / 4.0).clamp(0, 1) * 65535.0) / 65535.0 * 4.0
+        col = torch.arange(7, device=p.device)[None, :]
+        g = torch.where(col == th[:, None], gt, g)
+        ng = torch.tensor([GEOM_LEN.get(i, 0) for i in range(8)], device=p.device)[k.clamp(0, 7).long()]
+        p[:, 0:7] = torch.where((col < ng[:, None]) & (k[:, None] != 0), g, p[:, 0:7])
+        return p.to(torch.float32)
+
+
+def ctypes_addr(st) -> int:
+    import ctypes
+
+    return ctypes.addressof(st)
+
+
+class StackLoss(torch.autograd.Function):
+    """Per-tile losses of the stacks; backward is the hand-written kernel."""
+
+    @staticmethod
+    def forward(ctx, params: torch.Tensor, stack_set: StackSet, soft: bool = False):
+        ctx.stack_set = stack_set
+        ctx.soft = soft
+        ctx.save_for_backward(params)
+        return stack_set.loss(params, soft)
+
+    @staticmethod
+    def backward(ctx, grad_loss):
+        (params,) = ctx.saved_tensors
+        return ctx.stack_set.loss_backward(params, grad_loss, ctx.soft), None, None
+
+
+def refine(stack_set: StackSet, params: torch.Tensor, steps: int = 200, lr: float = 1e-2
+           ) -> tuple[torch.Tensor, list[float]]:
+    """Adam (FP32 parameters and moments) on the pixel-weighted total loss, projecting
+    onto the wire-representable box after every step; returns (params, loss history)."""
+    p = params.detach().clone().contiguous()
+    stack_set.project_(p)
+    p.requires_grad_(True)
+    opt = torch.optim.Adam([p], lr=lr, fused=True)
+    w = stack_set.weights
+    hist = []
+    for _ in range(int(steps)):
+        opt.zero_grad(set_to_none=False)
+        loss = (StackLoss.apply(p, stack_set, False) * w).sum()
+        loss.backward()
+        opt.step()
+        stack_set.project_(p.data)
+        hist.append(loss.detach())
+    return p.detach(), [float(h) for h in torch.stack(hist).cpu()] if hist else []

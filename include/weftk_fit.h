@@ -114,6 +114,33 @@ int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double comp
  */
 int weftk_fit_reseed(const WeftFitState* st, int quality, void* stream);
 
+/*
+ * weftk_fit_round_static — weftk_fit_round for callers that cannot allocate device
+ * memory.  No counterpart in the reference.  Some callers must not call
+ * cudaMalloc while they run: hosts that hand the library a fixed device budget
+ * up front (plugin and FFI hosts with their own pool), latency-sensitive
+ * services for which cudaMalloc's implicit device synchronisation would stall
+ * other streams, and callers in the middle of stream-ordered work that an
+ * allocation would serialise.  This entry point takes the same state but
+ * ignores st->partial: the per-candidate scoring scratch lives in a file-scope
+ * __device__ array of WEFTK_FIT_STATIC_SCRATCH_FLOATS floats (16 MiB) that every
+ * GPU loading the library holds until the process exits.  It calls no
+ * cudaMalloc/cudaFree and no allocating library routine.
+ *   - needs 4 * st->n_slots <= WEFTK_FIT_STATIC_SCRATCH_FLOATS, else WEFTK_E_RANGE;
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture;
+ *   - all calls share the one array and it keeps the last call's contents; a
+ *     round writes every scratch entry before it reads it, so nothing needs
+ *     clearing, but calls whose work overlaps on the GPU (other streams, other
+ *     threads) race on the array and must be serialised by the caller.
+ */
+#define WEFTK_FIT_STATIC_SCRATCH_FLOATS (4 * 1024 * 1024)
+int weftk_fit_round_static(const WeftFitState* st, int mode, double lambda, double complex_threshold,
+                           const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
+                           const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
+                           int n_items32, void* stream);
+
 /* Kernel timing for measurement: while enabled, weftk_fit_round brackets its
  * scoring launches with CUDA events.  *score_ms receives the summed device time
  * of the scoring launches since the previous query and *n_rounds how many

@@ -83,6 +83,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_fit_prepare": [_P, _P, _P],
     "weftk_fit_round": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],
     "weftk_fit_timing": [_I, _P, _P],
+    "weftk_fit_round_static": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],
     "weftk_fit_reseed": [_P, _I, _P],
     "weftk_stack_loss": [_P, _P, _P, _I, _P],
     "weftk_stack_loss_backward": [_P, _P, _P, _P, _I, _P],

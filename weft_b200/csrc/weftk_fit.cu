@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <mutex>
+#include <string>
 
 #include "../../include/weftk_fit.h"
 #include "weftk_common.cuh"
@@ -379,6 +381,30 @@ static int timing_collect() {
 
 using namespace weftk;
 
+// ---------------------------------------------------------------- allocation-free round
+// Scoring scratch for weftk_fit_round_static: a fixed array in device memory, so
+// that entry point never allocates.  Host code must not use the symbol as a
+// pointer (it is a host-side stand-in); the device address comes from
+// cudaGetSymbolAddress, looked up once per device.
+static __device__ __align__(256) float g_fit_static_scratch[WEFTK_FIT_STATIC_SCRATCH_FLOATS];
+static std::mutex g_static_mu;
+static float* g_static_ptr[64] = {nullptr};
+
+static int static_scratch_for_current_device(float** out) {
+    int dev = 0;
+    WEFTK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(WEFTK_E_RANGE, "fit_round_static: device index beyond 63");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_fit_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_fit_static_scratch)");
+        g_static_ptr[dev] = static_cast<float*>(p);
+    }
+    *out = g_static_ptr[dev];
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_fit_timing(int enable, double* score_ms, int* n_rounds) {
     int rc = timing_collect();
     if (rc) return rc;
@@ -430,6 +456,26 @@ extern "C" int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_
     fit_prepare_kernel<<<st->n_tiles, 128, 0, (cudaStream_t)stream>>>(*st, d_first_new);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
+}
+
+extern "C" int weftk_fit_round_static(const WeftFitState* st, int mode, double lambda, double complex_threshold,
+                                      const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
+                                      const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
+                                      int n_items32, void* stream) {
+    WEFTK_REQUIRE(st, "fit_round_static: null state");
+    if (st->n_slots < 0 || st->n_slots > (long long)WEFTK_FIT_STATIC_SCRATCH_FLOATS / 4)
+        return fail(WEFTK_E_RANGE, "fit_round_static: " + std::to_string((long long)st->n_slots) +
+                                       " candidate slots need more than the " +
+                                       std::to_string(WEFTK_FIT_STATIC_SCRATCH_FLOATS) +
+                                       "-float static scratch (at most " +
+                                       std::to_string(WEFTK_FIT_STATIC_SCRATCH_FLOATS / 4) + " slots)");
+    float* scratch = nullptr;
+    int rc = static_scratch_for_current_device(&scratch);
+    if (rc) return rc;
+    WeftFitState local = *st;
+    local.partial = scratch;
+    return weftk_fit_round(&local, mode, lambda, complex_threshold, d_perm, d_items8, n_items8, d_items16, n_items16,
+                           d_items32, n_items32, stream);
 }
 
 extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double complex_threshold,

@@ -164,6 +164,74 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
+    """Decoder primitive walk of the fitted stacks at out_w x out_h (one launch renders the image).
+
+    Each launch is timed alone with CUDA events; a 256 MiB buffer is written between launches so the
+    99.5 MB output is not served from L2.
+    """
+    import ctypes
+
+    import torch
+
+    from weft_b200 import _lib
+    from weft_b200.render import build_scene
+
+    class _Rec:
+        __slots__ = ("primitives", "residual_rgb")
+
+        def __init__(self, p):
+            self.primitives = p
+            self.residual_rgb = (0, 0, 0)
+
+    recs = [_Rec(s) for s in fit.selected()]
+    descs, prims, cp48, _, th, tw = build_scene(recs, tiles, width, height, None, out_w, out_h)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t_d = torch.from_numpy(descs.view(np.uint8)).to(dev)
+    t_p = torch.from_numpy(prims.view(np.uint8)).to(dev)
+    t_c = torch.from_numpy(np.ascontiguousarray(cp48)).to(dev)
+    out = torch.empty((th, tw, 3), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    lib = _lib.lib_for_device(dev.index)
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_p), _lib.ptr(t_c), len(cp48), 0, 0,
+                                          _lib.ptr(out), th, tw, 0, stream.cuda_stream), "weftk_render_tiles")
+
+    for _ in range(3):
+        launch()
+    times = []
+    for _ in range(iters):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        launch()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    st = ctypes.c_int(0)
+    _lib.check(lib.weftk_device_status(ctypes.addressof(st)), "weftk_device_status")
+    if st.value:
+        raise RuntimeError("decode walk reported a bad descriptor")
+    ms = statistics.median(times)
+    nbytes = 12 * tw * th + 48 * len(descs) + 60 * len(prims)
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    peak_gbs, peak_source = peak
+    return {"target": f"{tw}x{th}", "ms": ms, "mpix_per_s": tw * th / (ms * 1e-3) / 1e6, "bytes": nbytes,
+            "achieved_gbs": gbs, "peak_gbs": peak_gbs, "frac": gbs / peak_gbs,
+            "peak_source": peak_source,
+            "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims))}
+
+
+def _hbm_peak() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
+
+
 def dist_setup(n_gpus: int):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -219,6 +287,7 @@ def main():
     ap.add_argument("--ref-step-s", type=float, default=8.0)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--decode-iters", type=int, default=10)
     args = ap.parse_args()
 
     # Process pools first: spawned before any CUDA initialisation.
@@ -321,6 +390,9 @@ def run_weft(args, world, rank, local, executor, cores):
     prims_total = sum(len(s) for s in sel)
     prim_bytes = sum(1 + sum(2 + rate.PRIM_BYTES.get(c.kind, 48) for c in s) for s in sel)
 
+    decode = decode_bench(fit, tiles, args.size, args.size, 3840, 2160, args.decode_iters, _hbm_peak()) \
+        if args.decode_iters > 0 else None
+
     # e2e through the public API from host buffers
     e2e_ms = []
     h2d = d2h = 0
@@ -370,6 +442,7 @@ def run_weft(args, world, rank, local, executor, cores):
         "fit": {"rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds, "reseed_host_s": fit.stats.t_reseed_s,
                 "cand_gen_s": cand_s, "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
                 "prim_payload_bytes": prim_bytes},
+        "decode": decode,
     }
     print(json.dumps(line), flush=True)
 

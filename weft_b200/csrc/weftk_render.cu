@@ -104,7 +104,27 @@ constexpr int DEC_PPL = 4;
 constexpr int DEC_THREADS = 256;
 constexpr int MAX_TILE_PRIMS = 48;
 
-__global__ void __launch_bounds__(DEC_THREADS) render_tiles_kernel(
+// Sole-bicubic tile: float64 Bernstein evaluation of the 4x4x3 control grid at sample
+// (lx, ly) of a side x side grid (src/weft/bicubic.py:106-115), clipped.  Kept out of
+// line so the common path's register budget is not set by this rare one.
+__device__ __noinline__ void bicubic_pixel(const float* ctrl, int lx, int ly, int side, float* rgb) {
+    double by[4], bx[4];
+    bernstein4(ly, side, by);
+    bernstein4(lx, side, bx);
+    double o[3] = {0.0, 0.0, 0.0};
+    for (int r = 0; r < 4; ++r) {
+        for (int ch = 0; ch < 3; ++ch) {
+            double m = 0.0;
+            for (int c = 0; c < 4; ++c) m = fma((double)ctrl[(r * 4 + c) * 3 + ch], bx[c], m);
+            o[ch] = fma(by[r], m, o[ch]);
+        }
+    }
+    rgb[0] = clamp01((float)o[0]);
+    rgb[1] = clamp01((float)o[1]);
+    rgb[2] = clamp01((float)o[2]);
+}
+
+__global__ void __launch_bounds__(DEC_THREADS, 2) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, const WeftPrim* __restrict__ prims,
     const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1, int n_res1, float* __restrict__ out,
     int H, int W) {
@@ -153,25 +173,12 @@ __global__ void __launch_bounds__(DEC_THREADS) render_tiles_kernel(
             cr[j] = cg[j] = cb[j] = 0.0f;
         }
         if (bic) {
-#pragma unroll
             for (int j = 0; j < DEC_PPL; ++j) {
-                double by[4], bx[4];
-                bernstein4(ly[j] < side ? ly[j] : side - 1, side, by);
-                bernstein4(lx[j] < side ? lx[j] : side - 1, side, bx);
-                double o[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-#pragma unroll
-                    for (int ch = 0; ch < 3; ++ch) {
-                        double m = 0.0;
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) m = fma((double)ctrl[(r * 4 + c) * 3 + ch], bx[c], m);
-                        o[ch] = fma(by[r], m, o[ch]);
-                    }
-                }
-                cr[j] = clamp01((float)o[0]);
-                cg[j] = clamp01((float)o[1]);
-                cb[j] = clamp01((float)o[2]);
+                float rgb[3];
+                bicubic_pixel(ctrl, min(lx[j], side - 1), min(ly[j], side - 1), side, rgb);
+                cr[j] = rgb[0];
+                cg[j] = rgb[1];
+                cb[j] = rgb[2];
             }
         } else {
             for (int k = 0; k < n; ++k) {

@@ -2,6 +2,7 @@
 // used by the synchronous host-buffer entry points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -17,7 +18,7 @@ namespace weftk {
 
 int launch_score_evals(const WeftEval*, int, const WeftPrim*, const float*, float*, int, cudaStream_t);
 int launch_render_tiles(const WeftTileDecodeDesc*, int, const WeftPrim*, const float*, int, const float*, int, float*,
-                        int, int, cudaStream_t);
+                        int, int, int, cudaStream_t);
 int read_device_status(int* status, bool clear);
 
 static thread_local std::string t_last_error;
@@ -153,11 +154,11 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
 }
 
 int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const WeftPrim* d_prims, const float* d_cp48,
-                       int n_cp48, const float* d_res1, int n_res1, float* d_out, int out_h, int out_w, int flags,
-                       void* stream) {
+                       int n_cp48, const float* d_res1, int n_res1, float* d_out, int out_h, int out_w,
+                       int max_tile_pixels, int flags, void* stream) {
     (void)flags;
     return launch_render_tiles(d_descs, n_tiles, d_prims, d_cp48, n_cp48, d_res1, n_res1, d_out, out_h, out_w,
-                               (cudaStream_t)stream);
+                               max_tile_pixels, (cudaStream_t)stream);
 }
 
 int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, const WeftPrim* h_prims, int n_prims,
@@ -166,8 +167,10 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     (void)flags;
     WEFTK_REQUIRE(n_tiles >= 0 && out_h > 0 && out_w > 0 && h_out && n_prims >= 0 && n_cp48 >= 0 && n_res1 >= 0,
                   "render_tiles_host: bad arguments");
+    int max_px = 0;
     for (int i = 0; i < n_tiles; ++i) {
         const WeftTileDecodeDesc& d = h_descs[i];
+        if ((long long)d.target_w * d.target_h > max_px) max_px = (int)std::min<long long>((long long)d.target_w * d.target_h, 1 << 30);
         if (d.prim_count < 0 || d.prim_count > 48 || d.prim_offset < 0 || (int64_t)d.prim_offset + d.prim_count > n_prims ||
             d.target_w <= 0 || d.target_h <= 0 || d.source_size <= 0 || (n_res1 > 0 && d.res1_index >= n_res1))
             return fail(WEFTK_E_ARG, "render_tiles_host: tile " + std::to_string(i) + " is out of range");
@@ -196,7 +199,7 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     WEFTK_CUDA(cudaMemsetAsync(dout, 0, out_bytes, s));
     if ((rc = launch_render_tiles((const WeftTileDecodeDesc*)dd, n_tiles, (const WeftPrim*)dp,
                                   n_cp48 ? (const float*)dc : nullptr, n_cp48, n_res1 ? (const float*)dr : nullptr,
-                                  n_res1, (float*)dout, out_h, out_w, s)))
+                                  n_res1, (float*)dout, out_h, out_w, max_px, s)))
         return rc;
     WEFTK_CUDA(cudaMemcpyAsync(h_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
     WEFTK_CUDA(cudaStreamSynchronize(s));

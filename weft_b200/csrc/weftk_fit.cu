@@ -130,8 +130,8 @@ __global__ void fit_end_kernel(WeftFitState st, int mode, double complex_thresho
 // computed one per lane into the warp's segment table and read back the same way.
 constexpr int MAX_ITEM = 128;
 
-template <int PPL, int WPC>
-__global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
+template <int PPL, int WPC, int MINB>
+__global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
                                                         const WeftFitItem* __restrict__ items, int n_items,
                                                         int expect_min, int expect_max) {
     constexpr int GROUPS = 4 / WPC;
@@ -173,10 +173,13 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
     int base = 0;
     for (int k = 0; k < warp; ++k) base += s_wcount[k];
     const int m = s_wcount[0] + s_wcount[1] + s_wcount[2] + s_wcount[3];
+    unsigned long long ops = 0;
     if (live) {
         const int pos = base + __popc(bal & ((1u << lane) - 1u));
         const float4* src4 = reinterpret_cast<const float4*>(st.prep) + my_slot * 4;
-        s_prep[pos][0] = __ldg(src4);
+        const float4 head = __ldg(src4);
+        ops = (unsigned long long)(WPC * 32 * PPL) * (unsigned long long)(kind_ops(__float_as_int(head.x)) + 9);
+        s_prep[pos][0] = head;
         s_prep[pos][1] = __ldg(src4 + 1);
         s_prep[pos][2] = __ldg(src4 + 2);
         s_prep[pos][3] = __ldg(src4 + 3);
@@ -200,7 +203,6 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
         s[j] = make_float3(a.x, a.y, a.z);
         g[j] = make_float3(b.x, b.y, b.z);
     }
-    unsigned long long ops = 0;
     for (int c = group; c < m; c += GROUPS) {
         Prep P;
         {
@@ -211,7 +213,6 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
             P.q[3] = cc.x; P.q[4] = cc.y; P.q[5] = cc.z; P.q[6] = cc.w;
             P.q[7] = d.x; P.q[8] = d.y; P.q[9] = d.z; P.q[10] = d.w;
         }
-        ops += (unsigned long long)(32 * PPL) * (unsigned long long)(kind_ops(P.kind) + 9);
         float a[PPL], sr[PPL], sg[PPL], sb[PPL];
         if (P.kind == K_CURVE) {
             const Seg sg1 = lane_segment(P, lane);
@@ -244,7 +245,12 @@ __global__ void __launch_bounds__(128) fit_score_kernel(WeftFitState st, const i
             red[c][wig] = e;
         }
     }
-    if (st.work != nullptr && lane == 0 && ops) atomicAdd(&st.work[1], ops);
+    if (st.work != nullptr) {
+        // algorithmic ops of this CTA: every live candidate over the pixels it covers
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ops += __shfl_xor_sync(FULL, ops, o);
+        if (lane == 0 && ops) atomicAdd(&st.work[1], ops);
+    }
     if (WPC > 1) {
         __syncthreads();
         for (int c = threadIdx.x; c < m; c += blockDim.x) {
@@ -495,9 +501,9 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
         if (rc) return rc;
         WEFTK_CUDA(cudaEventRecord(g_timing.start, s));
     }
-    if (n_items8) fit_score_kernel<2, 1><<<n_items8, 128, 0, s>>>(*st, d_perm, d_items8, n_items8, 8, 8);
-    if (n_items16) fit_score_kernel<8, 1><<<n_items16, 128, 0, s>>>(*st, d_perm, d_items16, n_items16, 16, 16);
-    if (n_items32) fit_score_kernel<8, 4><<<n_items32, 128, 0, s>>>(*st, d_perm, d_items32, n_items32, 32, 64);
+    if (n_items8) fit_score_kernel<2, 1, 7><<<n_items8, 128, 0, s>>>(*st, d_perm, d_items8, n_items8, 8, 8);
+    if (n_items16) fit_score_kernel<8, 1, 4><<<n_items16, 128, 0, s>>>(*st, d_perm, d_items16, n_items16, 16, 16);
+    if (n_items32) fit_score_kernel<8, 4, 4><<<n_items32, 128, 0, s>>>(*st, d_perm, d_items32, n_items32, 32, 64);
     if (g_timing.enabled) {
         WEFTK_CUDA(cudaEventRecord(g_timing.stop, s));
         g_timing.pending = true;

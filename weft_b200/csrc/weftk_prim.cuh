@@ -30,7 +30,7 @@ enum Kind : int { K_CONST = 0, K_LINEAR = 1, K_LINE = 2, K_CURVE = 3, K_TRI = 4,
 //   linear:   X0 Y0 UX UY c1r c1g c1b
 //   line:     X0 Y0 VX VY UX UY K         (alpha = exp(K * d^2) * a)
 //   curve:    K p0x p0y cx cy p1x p1y
-//   triangle: X2 Y2 A B C D DEN           (a = (A dx + B dy)/DEN, b = (C dx + D dy)/DEN)
+//   triangle: X2 Y2 A B C D DEN 1/DEN     (a = (A dx + B dy)/DEN, b = (C dx + D dy)/DEN)
 //   bicubic:  index of the 48-value control grid (as float)
 struct __align__(16) Prep {
     int kind;
@@ -40,7 +40,9 @@ struct __align__(16) Prep {
 };
 static_assert(sizeof(Prep) == 64, "Prep must be 64 bytes");
 
-__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.0f), 1.0f); }
+// Clamp to [0, 1] (NaN -> 0).  The saturate modifier folds into the producing FADD/FMUL/FFMA,
+// so the clamp costs no instruction; same results as fminf(fmaxf(v, 0), 1).
+__device__ __forceinline__ float clamp01(float v) { return __saturatef(v); }
 
 // Gaussian falloff coefficient: -f32(1 / (2 sigma^2)), sigma = max(0.5, thickness),
 // evaluated in float64 like the reference's Python scalars.
@@ -103,6 +105,7 @@ __device__ __forceinline__ Prep prep_prim(const WeftPrim& P) {
             r.q[4] = (float)(y2 - y0);
             r.q[5] = (float)(x0 - x2);
             r.q[6] = (float)den;
+            r.q[7] = __frcp_rn((float)den);
             break;
         }
         case K_BICUBIC:
@@ -156,12 +159,21 @@ __device__ __forceinline__ float seg_d2(float px, float py, float ax, float ay, 
     return fmaf(ex, ex, ey * ey);
 }
 
-// Exact reproduction of the reference's float32 barycentric inside test.
+// Exact reproduction of the reference's float32 barycentric inside test:
+// a = fl(num_a / den), b = fl(num_b / den), c = fl(fl(1 - a) - b), inside iff all >= 0.
+// The signs of a and b are the signs of num * (1/den), so they are tested without a
+// division; c is first estimated from the reciprocal products and the IEEE divisions
+// are only done when the estimate is within its error bound of zero.
 __device__ __forceinline__ float tri_inside(const Prep& P, float px, float py) {
-    float dx = __fsub_rn(px, P.q[0]), dy = __fsub_rn(py, P.q[1]);
-    float a = __fdiv_rn(__fadd_rn(__fmul_rn(P.q[2], dx), __fmul_rn(P.q[3], dy)), P.q[6]);
-    float b = __fdiv_rn(__fadd_rn(__fmul_rn(P.q[4], dx), __fmul_rn(P.q[5], dy)), P.q[6]);
-    float c = __fsub_rn(__fsub_rn(1.0f, a), b);
+    const float dx = __fsub_rn(px, P.q[0]), dy = __fsub_rn(py, P.q[1]);
+    const float na = __fadd_rn(__fmul_rn(P.q[2], dx), __fmul_rn(P.q[3], dy));
+    const float nb = __fadd_rn(__fmul_rn(P.q[4], dx), __fmul_rn(P.q[5], dy));
+    const float ea = __fmul_rn(na, P.q[7]), eb = __fmul_rn(nb, P.q[7]);
+    if (ea < 0.0f || eb < 0.0f) return 0.0f;
+    const float ec = __fsub_rn(__fsub_rn(1.0f, ea), eb);
+    if (fabsf(ec) > 1e-6f * (1.0f + ea + eb)) return ec >= 0.0f ? 1.0f : 0.0f;
+    const float a = __fdiv_rn(na, P.q[6]), b = __fdiv_rn(nb, P.q[6]);
+    const float c = __fsub_rn(__fsub_rn(1.0f, a), b);
     return (a >= 0.0f && b >= 0.0f && c >= 0.0f) ? 1.0f : 0.0f;
 }
 

@@ -175,7 +175,7 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
     import torch
 
     from weft_b200 import _lib
-    from weft_b200.render import build_scene
+    from weft_b200.render import build_scene, decode_items
 
     class _Rec:
         __slots__ = ("primitives", "residual_rgb")
@@ -191,14 +191,16 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
     t_p = torch.from_numpy(prims.view(np.uint8)).to(dev)
     t_c = torch.from_numpy(np.ascontiguousarray(cp48)).to(dev)
     out = torch.empty((th, tw, 3), dtype=torch.float32, device=dev)
-    max_px = int((descs["target_w"].astype(np.int64) * descs["target_h"]).max())
+    items = decode_items(descs)
+    t_i = torch.from_numpy(items).to(dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     lib = _lib.lib_for_device(dev.index)
     stream = torch.cuda.current_stream()
 
     def launch():
-        _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_p), _lib.ptr(t_c), len(cp48), 0, 0,
-                                          _lib.ptr(out), th, tw, max_px, 0, stream.cuda_stream), "weftk_render_tiles")
+        _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_i), len(items), _lib.ptr(t_p),
+                                          _lib.ptr(t_c), len(cp48), 0, 0, _lib.ptr(out), th, tw, 0,
+                                          stream.cuda_stream), "weftk_render_tiles")
 
     for _ in range(3):
         launch()

@@ -116,16 +116,22 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
  * are left untouched.  Replaces decode_tile_pixels (src/weft/gpu_render.py:179-237)
  * behind gpu_render_tiles_to_image (:594-690) with the semantics of
  * render_scene_adaptive (src/weft/render.py:270-358).
+ *   d_items [n_items] work items (tile index, first chunk): a tile's target rect,
+ *                     row-major, is cut into chunks of WEFTK_DECODE_CHUNK pixels
+ *                     and every item covers WEFTK_DECODE_ITEM_CHUNKS consecutive
+ *                     chunks, i.e. tile t contributes items (t, 0), (t, 2), ...
+ *                     below ceil(w * h / WEFTK_DECODE_CHUNK)
  *   d_cp48  [n_cp48 * 48]  control grids for kind-5 tiles (may be NULL)
  *   d_res1  [n_res1 * 48]  RES1 grids, (4, 4, 3) row-major, float (may be NULL;
  *                          res1_index is ignored when n_res1 == 0)
- * max_tile_pixels: largest target_w * target_h of any tile (0 = unknown); it sets
- * how many CTAs share a tile.  Tiles with more than 48 primitives, a bad rect or
- * an out-of-range grid index are skipped and reported through weftk_device_status.
+ * Tiles with more than 48 primitives, a bad rect or an out-of-range grid index
+ * are skipped and reported through weftk_device_status.
  */
-int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const WeftPrim* d_prims,
-                       const float* d_cp48, int n_cp48, const float* d_res1, int n_res1, float* d_out,
-                       int out_h, int out_w, int max_tile_pixels, int flags, void* stream);
+#define WEFTK_DECODE_CHUNK 512
+#define WEFTK_DECODE_ITEM_CHUNKS 2
+int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const int32_t* d_items, int n_items,
+                       const WeftPrim* d_prims, const float* d_cp48, int n_cp48, const float* d_res1, int n_res1,
+                       float* d_out, int out_h, int out_w, int flags, void* stream);
 
 /* Synchronous host-buffer form of weftk_render_tiles (gpu_render_tiles_to_image). */
 int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, const WeftPrim* h_prims,

@@ -78,7 +78,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_device_status": [_P],
     "weftk_score_evals": [_P, _I, _P, _P, _P, _I, _P],
     "weftk_score_evals_host": [_P, _I, _P, _I, _P, _I64, _P, _I],
-    "weftk_render_tiles": [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I, _P],
+    "weftk_render_tiles": [_P, _I, _P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _P],
     "weftk_render_tiles_host": [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I],
     "weftk_fit_prepare": [_P, _P, _P],
     "weftk_fit_round": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],

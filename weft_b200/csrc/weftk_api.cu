@@ -17,8 +17,8 @@ static_assert(sizeof(WeftTileDecodeDesc) == 48, "WeftTileDecodeDesc must match T
 namespace weftk {
 
 int launch_score_evals(const WeftEval*, int, const WeftPrim*, const float*, float*, int, cudaStream_t);
-int launch_render_tiles(const WeftTileDecodeDesc*, int, const WeftPrim*, const float*, int, const float*, int, float*,
-                        int, int, int, cudaStream_t);
+int launch_render_tiles(const WeftTileDecodeDesc*, int, const int2*, int, const WeftPrim*, const float*, int,
+                        const float*, int, float*, int, int, cudaStream_t);
 int read_device_status(int* status, bool clear);
 
 static thread_local std::string t_last_error;
@@ -153,12 +153,12 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
     return check_status_after_sync();
 }
 
-int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const WeftPrim* d_prims, const float* d_cp48,
-                       int n_cp48, const float* d_res1, int n_res1, float* d_out, int out_h, int out_w,
-                       int max_tile_pixels, int flags, void* stream) {
+int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const int32_t* d_items, int n_items,
+                       const WeftPrim* d_prims, const float* d_cp48, int n_cp48, const float* d_res1, int n_res1,
+                       float* d_out, int out_h, int out_w, int flags, void* stream) {
     (void)flags;
-    return launch_render_tiles(d_descs, n_tiles, d_prims, d_cp48, n_cp48, d_res1, n_res1, d_out, out_h, out_w,
-                               max_tile_pixels, (cudaStream_t)stream);
+    return launch_render_tiles(d_descs, n_tiles, reinterpret_cast<const int2*>(d_items), n_items, d_prims, d_cp48,
+                               n_cp48, d_res1, n_res1, d_out, out_h, out_w, (cudaStream_t)stream);
 }
 
 int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, const WeftPrim* h_prims, int n_prims,
@@ -167,10 +167,13 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     (void)flags;
     WEFTK_REQUIRE(n_tiles >= 0 && out_h > 0 && out_w > 0 && h_out && n_prims >= 0 && n_cp48 >= 0 && n_res1 >= 0,
                   "render_tiles_host: bad arguments");
-    int max_px = 0;
+    std::vector<int2> items;
     for (int i = 0; i < n_tiles; ++i) {
         const WeftTileDecodeDesc& d = h_descs[i];
-        if ((long long)d.target_w * d.target_h > max_px) max_px = (int)std::min<long long>((long long)d.target_w * d.target_h, 1 << 30);
+        if (d.target_w > 0 && d.target_h > 0) {
+            const long long chunks = ((long long)d.target_w * d.target_h + WEFTK_DECODE_CHUNK - 1) / WEFTK_DECODE_CHUNK;
+            for (long long c = 0; c < chunks; c += WEFTK_DECODE_ITEM_CHUNKS) items.push_back(make_int2(i, (int)c));
+        }
         if (d.prim_count < 0 || d.prim_count > 48 || d.prim_offset < 0 || (int64_t)d.prim_offset + d.prim_count > n_prims ||
             d.target_w <= 0 || d.target_h <= 0 || d.source_size <= 0 || (n_res1 > 0 && d.res1_index >= n_res1))
             return fail(WEFTK_E_ARG, "render_tiles_host: tile " + std::to_string(i) + " is out of range");
@@ -184,7 +187,8 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     int rc = arena_for_current(&a);
     if (rc) return rc;
     size_t out_bytes = sizeof(float) * 3 * (size_t)out_h * (size_t)out_w;
-    void *dd, *dp, *dc, *dr, *dout;
+    void *dd, *dp, *dc, *dr, *dout, *di;
+    if ((rc = arena_get(9, sizeof(int2) * (items.empty() ? 1 : items.size()), &di, *a))) return rc;
     if ((rc = arena_get(4, sizeof(WeftTileDecodeDesc) * (size_t)(n_tiles > 0 ? n_tiles : 1), &dd, *a))) return rc;
     if ((rc = arena_get(5, sizeof(WeftPrim) * (size_t)(n_prims > 0 ? n_prims : 1), &dp, *a))) return rc;
     if ((rc = arena_get(6, sizeof(float) * 48 * (size_t)(n_cp48 > 0 ? n_cp48 : 1), &dc, *a))) return rc;
@@ -196,10 +200,12 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     if (n_prims > 0) WEFTK_CUDA(cudaMemcpyAsync(dp, h_prims, sizeof(WeftPrim) * (size_t)n_prims, cudaMemcpyHostToDevice, s));
     if (n_cp48 > 0) WEFTK_CUDA(cudaMemcpyAsync(dc, h_cp48, sizeof(float) * 48 * (size_t)n_cp48, cudaMemcpyHostToDevice, s));
     if (n_res1 > 0) WEFTK_CUDA(cudaMemcpyAsync(dr, h_res1, sizeof(float) * 48 * (size_t)n_res1, cudaMemcpyHostToDevice, s));
+    if (!items.empty())
+        WEFTK_CUDA(cudaMemcpyAsync(di, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
     WEFTK_CUDA(cudaMemsetAsync(dout, 0, out_bytes, s));
-    if ((rc = launch_render_tiles((const WeftTileDecodeDesc*)dd, n_tiles, (const WeftPrim*)dp,
-                                  n_cp48 ? (const float*)dc : nullptr, n_cp48, n_res1 ? (const float*)dr : nullptr,
-                                  n_res1, (float*)dout, out_h, out_w, max_px, s)))
+    if ((rc = launch_render_tiles((const WeftTileDecodeDesc*)dd, n_tiles, (const int2*)di, (int)items.size(),
+                                  (const WeftPrim*)dp, n_cp48 ? (const float*)dc : nullptr, n_cp48,
+                                  n_res1 ? (const float*)dr : nullptr, n_res1, (float*)dout, out_h, out_w, s)))
         return rc;
     WEFTK_CUDA(cudaMemcpyAsync(h_out, dout, out_bytes, cudaMemcpyDeviceToHost, s));
     WEFTK_CUDA(cudaStreamSynchronize(s));

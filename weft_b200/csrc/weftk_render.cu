@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) score_evals_kernel(const WeftEval* __rest
 constexpr int DEC_PPL = 4;
 constexpr int DEC_THREADS = 128;
 constexpr int DEC_CHUNK = DEC_THREADS * DEC_PPL;  // pixels one CTA renders per pass
-constexpr int DEC_MAX_SPLIT = 64;                 // CTAs sharing one tile (grid y)
+static_assert(DEC_CHUNK == WEFTK_DECODE_CHUNK, "chunk size is part of the C ABI");
 constexpr int MAX_TILE_PRIMS = 48;
 
 // Sole-bicubic tile: float64 Bernstein evaluation of the 4x4x3 control grid at sample
@@ -128,24 +128,33 @@ __device__ __noinline__ void bicubic_pixel(const float* ctrl, int lx, int ly, in
     rgb[2] = clamp01((float)o[2]);
 }
 
-// grid = (tiles, split): CTA (t, y) renders chunks y, y + split, ... of tile t's target
-// rect, so a large (upscaled) tile is spread over several SMs while a small one
-// occupies only the CTAs it needs (the others return before touching memory).
+// Work items: (tile, first chunk) pairs, each at most DEC_ITEM_CHUNKS chunks of DEC_CHUNK
+// pixels of the tile's target rect (row-major).  A persistent grid walks the item list,
+// so large upscaled tiles are spread over many SMs and no CTA is launched idle.
+constexpr int DEC_ITEM_CHUNKS = WEFTK_DECODE_ITEM_CHUNKS;
+
 __global__ void __launch_bounds__(DEC_THREADS, 8) render_tiles_kernel(
-    const WeftTileDecodeDesc* __restrict__ descs, const WeftPrim* __restrict__ prims,
-    const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1, int n_res1, float* __restrict__ out,
-    int H, int W) {
+    const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
+    const WeftPrim* __restrict__ prims, const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1,
+    int n_res1, float* __restrict__ out, int H, int W) {
     __shared__ Prep sp[MAX_TILE_PRIMS];
     __shared__ float grid[48];
     __shared__ float ctrl[48];
-    const WeftTileDecodeDesc d = descs[blockIdx.x];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int2 item = items[it];
+    __syncthreads();  // the previous item's readers of sp/grid/ctrl are done
+    if (item.x < 0 || item.x >= n_tiles) {
+        if (threadIdx.x == 0) report(WEFTK_E_ARG);
+        continue;
+    }
+    const WeftTileDecodeDesc d = descs[item.x];
     const int n = d.prim_count, w = d.target_w, h = d.target_h;
     if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || d.source_size <= 0) {
-        if (threadIdx.x == 0 && blockIdx.y == 0) report(WEFTK_E_ARG);
-        return;
+        if (threadIdx.x == 0) report(WEFTK_E_ARG);
+        continue;
     }
     const int n_chunks = (int)(((long long)w * h + DEC_CHUNK - 1) / DEC_CHUNK);
-    if ((int)blockIdx.y >= n_chunks) return;
+    const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
     for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
     const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
     if (has_res1 && d.res1_index >= n_res1) {
@@ -158,8 +167,8 @@ __global__ void __launch_bounds__(DEC_THREADS, 8) render_tiles_kernel(
     if (bic) {
         const int gi = (int)sp[0].q[0];
         if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
-            if (threadIdx.x == 0 && blockIdx.y == 0) report(WEFTK_E_ARG);
-            return;
+            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            continue;
         }
         if (threadIdx.x < 48) ctrl[threadIdx.x] = cp48[(size_t)gi * 48 + threadIdx.x];
         __syncthreads();
@@ -169,7 +178,7 @@ __global__ void __launch_bounds__(DEC_THREADS, 8) render_tiles_kernel(
     const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int npix = w * h;
-    for (int chunk = blockIdx.y; chunk < n_chunks; chunk += gridDim.y) {
+    for (int chunk = item.y; chunk < c_end; ++chunk) {
         const int base = chunk * DEC_CHUNK + warp * 32 * DEC_PPL;
         float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
         int lx[DEC_PPL], ly[DEC_PPL];
@@ -238,6 +247,7 @@ __global__ void __launch_bounds__(DEC_THREADS, 8) render_tiles_kernel(
             }
         }
     }
+    }
 }
 
 int launch_score_evals(const WeftEval* d_evals, int n_evals, const WeftPrim* d_prims, const float* d_tiles,
@@ -252,21 +262,20 @@ int launch_score_evals(const WeftEval* d_evals, int n_evals, const WeftPrim* d_p
     return WEFTK_OK;
 }
 
-int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const WeftPrim* d_prims,
-                        const float* d_cp48, int n_cp48, const float* d_res1, int n_res1, float* d_out, int out_h,
-                        int out_w, int max_tile_pixels, cudaStream_t stream) {
+int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const int2* d_items, int n_items,
+                        const WeftPrim* d_prims, const float* d_cp48, int n_cp48, const float* d_res1, int n_res1,
+                        float* d_out, int out_h, int out_w, cudaStream_t stream) {
     if (n_tiles == 0) return WEFTK_OK;
     WEFTK_REQUIRE(n_tiles > 0 && d_descs && d_out && out_h > 0 && out_w > 0, "render_tiles: bad arguments");
     WEFTK_REQUIRE(n_cp48 >= 0 && n_res1 >= 0, "render_tiles: negative table size");
-    // split: enough CTAs per tile for the largest tile's chunks, at least 2 chunks per CTA
-    int split = 4;
-    if (max_tile_pixels > 0) {
-        const int chunks = (max_tile_pixels + DEC_CHUNK - 1) / DEC_CHUNK;
-        split = std::max(1, std::min(DEC_MAX_SPLIT, (chunks + 1) / 2));
-    }
-    dim3 grid((unsigned)n_tiles, (unsigned)split);
-    render_tiles_kernel<<<grid, DEC_THREADS, 0, stream>>>(d_descs, d_prims, d_cp48, n_cp48, d_res1, n_res1, d_out,
-                                                          out_h, out_w);
+    WEFTK_REQUIRE(d_items != nullptr && n_items >= 0, "render_tiles: missing work items");
+    if (n_items == 0) return WEFTK_OK;
+    int dev = 0, sms = 148;
+    WEFTK_CUDA(cudaGetDevice(&dev));
+    WEFTK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = std::min(n_items, sms * 8 * 2);
+    render_tiles_kernel<<<blocks, DEC_THREADS, 0, stream>>>(d_descs, n_tiles, d_items, n_items, d_prims, d_cp48,
+                                                            n_cp48, d_res1, n_res1, d_out, out_h, out_w);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }

@@ -21,6 +21,18 @@ from . import _lib
 from ._lib import PRIM_DTYPE, TILE_DECODE_DTYPE
 
 MAX_TILE_PRIMS = 48
+DECODE_CHUNK = 512       # WEFTK_DECODE_CHUNK
+DECODE_ITEM_CHUNKS = 2   # WEFTK_DECODE_ITEM_CHUNKS
+
+
+def decode_items(descs: np.ndarray) -> np.ndarray:
+    """Work items (tile, first chunk) of weftk_render_tiles, int32 (n, 2)."""
+    px = descs["target_w"].astype(np.int64) * descs["target_h"].astype(np.int64)
+    chunks = (px + DECODE_CHUNK - 1) // DECODE_CHUNK
+    per = (chunks + DECODE_ITEM_CHUNKS - 1) // DECODE_ITEM_CHUNKS
+    tile = np.repeat(np.arange(len(descs)), per)
+    k = np.arange(int(per.sum())) - np.repeat(np.concatenate([[0], np.cumsum(per)[:-1]]), per)
+    return np.stack([tile, k * DECODE_ITEM_CHUNKS], axis=1).astype(np.int32)
 
 
 def pack_records(stacks) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:

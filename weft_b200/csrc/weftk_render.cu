@@ -104,8 +104,7 @@ __global__ void __launch_bounds__(256) score_evals_kernel(const WeftEval* __rest
 
 constexpr int DEC_PPL = 4;
 constexpr int DEC_THREADS = 128;
-constexpr int DEC_CHUNK = DEC_THREADS * DEC_PPL;  // pixels one CTA renders per pass
-static_assert(DEC_CHUNK == WEFTK_DECODE_CHUNK, "chunk size is part of the C ABI");
+static_assert(DEC_THREADS == WEFTK_DECODE_CHUNK_GROUPS && DEC_PPL == 4, "chunk layout is part of the C ABI");
 constexpr int MAX_TILE_PRIMS = 48;
 
 // Sole-bicubic tile: float64 Bernstein evaluation of the 4x4x3 control grid at sample
@@ -128,125 +127,151 @@ __device__ __noinline__ void bicubic_pixel(const float* ctrl, int lx, int ly, in
     rgb[2] = clamp01((float)o[2]);
 }
 
-// Work items: (tile, first chunk) pairs, each at most DEC_ITEM_CHUNKS chunks of DEC_CHUNK
-// pixels of the tile's target rect (row-major).  A persistent grid walks the item list,
-// so large upscaled tiles are spread over many SMs and no CTA is launched idle.
+// Work items: (tile, first chunk) pairs.  A tile's target rect is covered by 4-pixel
+// groups aligned to output x multiples of 4 (row by row); a chunk is DEC_THREADS such
+// groups (one per thread) and an item is up to DEC_ITEM_CHUNKS chunks.  Aligned groups
+// let a thread write its 4 pixels (48 bytes) as three 16-byte stores.  A persistent
+// grid walks the item list, so large upscaled tiles are spread over many SMs.
 constexpr int DEC_ITEM_CHUNKS = WEFTK_DECODE_ITEM_CHUNKS;
 
-__global__ void __launch_bounds__(DEC_THREADS, 8) render_tiles_kernel(
+__device__ __forceinline__ int floor_div4(int v) { return v >= 0 ? (v >> 2) : -((-v + 3) >> 2); }
+
+__global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
     const WeftPrim* __restrict__ prims, const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1,
     int n_res1, float* __restrict__ out, int H, int W) {
     __shared__ Prep sp[MAX_TILE_PRIMS];
     __shared__ float grid[48];
     __shared__ float ctrl[48];
+    const int lane = threadIdx.x & 31;
+    const bool w_aligned = (W & 3) == 0;
     for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-    const int2 item = items[it];
-    __syncthreads();  // the previous item's readers of sp/grid/ctrl are done
-    if (item.x < 0 || item.x >= n_tiles) {
-        if (threadIdx.x == 0) report(WEFTK_E_ARG);
-        continue;
-    }
-    const WeftTileDecodeDesc d = descs[item.x];
-    const int n = d.prim_count, w = d.target_w, h = d.target_h;
-    if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || d.source_size <= 0) {
-        if (threadIdx.x == 0) report(WEFTK_E_ARG);
-        continue;
-    }
-    const int n_chunks = (int)(((long long)w * h + DEC_CHUNK - 1) / DEC_CHUNK);
-    const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
-    const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
-    if (has_res1 && d.res1_index >= n_res1) {
-        if (threadIdx.x == 0) report(WEFTK_E_ARG);
-        return;
-    }
-    if (has_res1 && threadIdx.x < 48) grid[threadIdx.x] = res1[(size_t)d.res1_index * 48 + threadIdx.x];
-    __syncthreads();
-    const bool bic = (n == 1 && sp[0].kind == K_BICUBIC);
-    if (bic) {
-        const int gi = (int)sp[0].q[0];
-        if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
+        const int2 item = items[it];
+        __syncthreads();  // the previous item's readers of sp/grid/ctrl are done
+        if (item.x < 0 || item.x >= n_tiles) {
             if (threadIdx.x == 0) report(WEFTK_E_ARG);
             continue;
         }
-        if (threadIdx.x < 48) ctrl[threadIdx.x] = cp48[(size_t)gi * 48 + threadIdx.x];
-        __syncthreads();
-    }
-    const int side = max(w, h);
-    const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
-    const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int npix = w * h;
-    for (int chunk = item.y; chunk < c_end; ++chunk) {
-        const int base = chunk * DEC_CHUNK + warp * 32 * DEC_PPL;
-        float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
-        int lx[DEC_PPL], ly[DEC_PPL];
-#pragma unroll
-        for (int j = 0; j < DEC_PPL; ++j) {
-            int p = base + j * 32 + lane;
-            lx[j] = p % w;
-            ly[j] = p / w;
-            fx[j] = __fmul_rn((float)lx[j] + 0.5f, step);
-            fy[j] = __fmul_rn((float)ly[j] + 0.5f, step);
-            cr[j] = cg[j] = cb[j] = 0.0f;
+        const WeftTileDecodeDesc d = descs[item.x];
+        const int n = d.prim_count, w = d.target_w, h = d.target_h;
+        if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || d.source_size <= 0) {
+            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            continue;
         }
+        const int a0 = floor_div4(d.target_x0);
+        const int G = floor_div4(d.target_x0 + w + 3) - a0;  // aligned groups per row
+        const long long n_groups = (long long)G * h;
+        const int n_chunks = (int)((n_groups + DEC_THREADS - 1) / DEC_THREADS);
+        const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
+        const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
+        if (has_res1 && d.res1_index >= n_res1) {
+            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            continue;
+        }
+        if (has_res1 && threadIdx.x < 48) grid[threadIdx.x] = res1[(size_t)d.res1_index * 48 + threadIdx.x];
+        __syncthreads();
+        const bool bic = (n == 1 && sp[0].kind == K_BICUBIC);
         if (bic) {
-            for (int j = 0; j < DEC_PPL; ++j) {
-                float rgb[3];
-                bicubic_pixel(ctrl, min(lx[j], side - 1), min(ly[j], side - 1), side, rgb);
-                cr[j] = rgb[0];
-                cg[j] = rgb[1];
-                cb[j] = rgb[2];
+            const int gi = (int)sp[0].q[0];
+            if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
+                if (threadIdx.x == 0) report(WEFTK_E_ARG);
+                continue;
             }
-        } else {
-            for (int k = 0; k < n; ++k) {
-                Prep pr = sp[k];
-                if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
-                float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
-                prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
+            if (threadIdx.x < 48) ctrl[threadIdx.x] = cp48[(size_t)gi * 48 + threadIdx.x];
+            __syncthreads();
+        }
+        const int side = max(w, h);
+        const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
+        const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
+        for (int chunk = item.y; chunk < c_end; ++chunk) {
+            const long long g = (long long)chunk * DEC_THREADS + threadIdx.x;
+            const bool g_ok = g < n_groups;
+            const int row = g_ok ? (int)(g / G) : 0;
+            const int gxs = (a0 + (g_ok ? (int)(g % G) : 0)) * 4;
+            float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
+            int lx[DEC_PPL];
+            bool valid[DEC_PPL];
+#pragma unroll
+            for (int j = 0; j < DEC_PPL; ++j) {
+                lx[j] = gxs + j - d.target_x0;
+                valid[j] = g_ok && lx[j] >= 0 && lx[j] < w;
+                const int lxc = min(max(lx[j], 0), w - 1);
+                fx[j] = __fmul_rn((float)lxc + 0.5f, step);
+                fy[j] = __fmul_rn((float)row + 0.5f, step);
+                cr[j] = cg[j] = cb[j] = 0.0f;
+                lx[j] = lxc;
+            }
+            if (bic) {
+                for (int j = 0; j < DEC_PPL; ++j) {
+                    float rgb[3];
+                    bicubic_pixel(ctrl, lx[j], min(row, side - 1), side, rgb);
+                    cr[j] = rgb[0];
+                    cg[j] = rgb[1];
+                    cb[j] = rgb[2];
+                }
+            } else {
+                for (int k = 0; k < n; ++k) {
+                    Prep pr = sp[k];
+                    if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
+                    float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
+                    prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
+#pragma unroll
+                    for (int j = 0; j < DEC_PPL; ++j) {
+                        cr[j] = blend(sr[j], a[j], cr[j]);
+                        cg[j] = blend(sg[j], a[j], cg[j]);
+                        cb[j] = blend(sb[j], a[j], cb[j]);
+                    }
+                }
+            }
+            float o[DEC_PPL][3];
+#pragma unroll
+            for (int j = 0; j < DEC_PPL; ++j) {
+                float r = clamp01(cr[j] + d.res0_r), gg = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
+                if (has_res1) {
+                    // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
+                    float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                    float gy = fminf(fmaxf(__fsub_rn(__fmul_rn((float)row + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                    int x0 = (int)floorf(gx), y0 = (int)floorf(gy);
+                    float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
+                    int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
+                    float v[3];
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) {
+                        float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
+                        float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
+                        float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
+                        float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
+                        v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
+                    }
+                    r = clamp01(r + v[0]);
+                    gg = clamp01(gg + v[1]);
+                    b = clamp01(b + v[2]);
+                }
+                o[j][0] = r;
+                o[j][1] = gg;
+                o[j][2] = b;
+            }
+            const int gy = d.target_y0 + row;
+            if (!g_ok || gy < 0 || gy >= H) continue;
+            float* dst = out + ((size_t)gy * W + gxs) * 3;
+            if (w_aligned && valid[0] && valid[DEC_PPL - 1] && gxs >= 0 && gxs + DEC_PPL <= W) {
+                float4* d4 = reinterpret_cast<float4*>(dst);
+                d4[0] = make_float4(o[0][0], o[0][1], o[0][2], o[1][0]);
+                d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
+                d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
+            } else {
 #pragma unroll
                 for (int j = 0; j < DEC_PPL; ++j) {
-                    cr[j] = blend(sr[j], a[j], cr[j]);
-                    cg[j] = blend(sg[j], a[j], cg[j]);
-                    cb[j] = blend(sb[j], a[j], cb[j]);
+                    const int gxp = gxs + j;
+                    if (valid[j] && gxp >= 0 && gxp < W) {
+                        dst[3 * j] = o[j][0];
+                        dst[3 * j + 1] = o[j][1];
+                        dst[3 * j + 2] = o[j][2];
+                    }
                 }
             }
         }
-#pragma unroll
-        for (int j = 0; j < DEC_PPL; ++j) {
-            int p = base + j * 32 + lane;
-            if (p >= npix) continue;
-            float r = clamp01(cr[j] + d.res0_r), g = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
-            if (has_res1) {
-                // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
-                float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
-                float gy = fminf(fmaxf(__fsub_rn(__fmul_rn((float)ly[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
-                int x0 = (int)floorf(gx), y0 = (int)floorf(gy);
-                float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
-                int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
-                float v[3];
-#pragma unroll
-                for (int ch = 0; ch < 3; ++ch) {
-                    float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
-                    float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
-                    float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
-                    float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
-                    v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
-                }
-                r = clamp01(r + v[0]);
-                g = clamp01(g + v[1]);
-                b = clamp01(b + v[2]);
-            }
-            int gxp = d.target_x0 + lx[j], gyp = d.target_y0 + ly[j];
-            if (gxp >= 0 && gxp < W && gyp >= 0 && gyp < H) {
-                float* o = out + ((size_t)gyp * W + gxp) * 3;
-                o[0] = r;
-                o[1] = g;
-                o[2] = b;
-            }
-        }
-    }
     }
 }
 

@@ -21,14 +21,18 @@ from . import _lib
 from ._lib import PRIM_DTYPE, TILE_DECODE_DTYPE
 
 MAX_TILE_PRIMS = 48
-DECODE_CHUNK = 512       # WEFTK_DECODE_CHUNK
-DECODE_ITEM_CHUNKS = 2   # WEFTK_DECODE_ITEM_CHUNKS
+DECODE_CHUNK_GROUPS = 128  # WEFTK_DECODE_CHUNK_GROUPS
+DECODE_ITEM_CHUNKS = 2     # WEFTK_DECODE_ITEM_CHUNKS
 
 
 def decode_items(descs: np.ndarray) -> np.ndarray:
-    """Work items (tile, first chunk) of weftk_render_tiles, int32 (n, 2)."""
-    px = descs["target_w"].astype(np.int64) * descs["target_h"].astype(np.int64)
-    chunks = (px + DECODE_CHUNK - 1) // DECODE_CHUNK
+    """Work items (tile, first chunk) of weftk_render_tiles, int32 (n, 2).
+
+    A tile's rect rows are covered by 4-pixel groups aligned to output x multiples of 4.
+    """
+    x0 = descs["target_x0"].astype(np.int64)
+    groups = (np.floor_divide(x0 + descs["target_w"] + 3, 4) - np.floor_divide(x0, 4)) * descs["target_h"]
+    chunks = (groups + DECODE_CHUNK_GROUPS - 1) // DECODE_CHUNK_GROUPS
     per = (chunks + DECODE_ITEM_CHUNKS - 1) // DECODE_ITEM_CHUNKS
     tile = np.repeat(np.arange(len(descs)), per)
     k = np.arange(int(per.sum())) - np.repeat(np.concatenate([[0], np.cumsum(per)[:-1]]), per)

@@ -122,7 +122,7 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
  *                     groups per row, G * h per tile, row-major; a chunk is
  *                     WEFTK_DECODE_CHUNK_GROUPS groups and an item covers
  *                     WEFTK_DECODE_ITEM_CHUNKS consecutive chunks, i.e. tile t
- *                     contributes items (t, 0), (t, 2), ... below
+ *                     contributes items (t, 0), (t, 8), ... below
  *                     ceil(G * h / WEFTK_DECODE_CHUNK_GROUPS)
  *   d_cp48  [n_cp48 * 48]  control grids for kind-5 tiles (may be NULL)
  *   d_res1  [n_res1 * 48]  RES1 grids, (4, 4, 3) row-major, float (may be NULL;
@@ -130,8 +130,8 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
  * Tiles with more than 48 primitives, a bad rect or an out-of-range grid index
  * are skipped and reported through weftk_device_status.
  */
-#define WEFTK_DECODE_CHUNK_GROUPS 128
-#define WEFTK_DECODE_ITEM_CHUNKS 2
+#define WEFTK_DECODE_CHUNK_GROUPS 32
+#define WEFTK_DECODE_ITEM_CHUNKS 8
 int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const int32_t* d_items, int n_items,
                        const WeftPrim* d_prims, const float* d_cp48, int n_cp48, const float* d_res1, int n_res1,
                        float* d_out, int out_h, int out_w, int flags, void* stream);

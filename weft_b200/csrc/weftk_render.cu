@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) score_evals_kernel(const WeftEval* __rest
 
 constexpr int DEC_PPL = 4;
 constexpr int DEC_THREADS = 128;
-static_assert(DEC_THREADS == WEFTK_DECODE_CHUNK_GROUPS && DEC_PPL == 4, "chunk layout is part of the C ABI");
+static_assert(WEFTK_DECODE_CHUNK_GROUPS == 32 && DEC_PPL == 4, "chunk layout is part of the C ABI");
 constexpr int MAX_TILE_PRIMS = 48;
 
 // Sole-bicubic tile: float64 Bernstein evaluation of the 4x4x3 control grid at sample
@@ -127,12 +127,14 @@ __device__ __noinline__ void bicubic_pixel(const float* ctrl, int lx, int ly, in
     rgb[2] = clamp01((float)o[2]);
 }
 
-// Work items: (tile, first chunk) pairs.  A tile's target rect is covered by 4-pixel
-// groups aligned to output x multiples of 4 (row by row); a chunk is DEC_THREADS such
-// groups (one per thread) and an item is up to DEC_ITEM_CHUNKS chunks.  Aligned groups
-// let a thread write its 4 pixels (48 bytes) as three 16-byte stores.  A persistent
-// grid walks the item list, so large upscaled tiles are spread over many SMs.
+// Work items: (tile, first chunk) pairs.  Each row of a tile's target rect is covered by
+// 4-pixel groups aligned to output x multiples of 4, so a thread writes its 4 pixels
+// (48 bytes) as three 16-byte stores.  A chunk is 32 groups (one per lane) and an item is
+// up to DEC_ITEM_CHUNKS chunks, rendered by ONE warp: the warp stages its tile's
+// primitives in its own slice of shared memory and never waits on the rest of the CTA,
+// so every resident warp works on a different item.  A persistent grid walks the list.
 constexpr int DEC_ITEM_CHUNKS = WEFTK_DECODE_ITEM_CHUNKS;
+constexpr int DEC_WARPS = DEC_THREADS / 32;
 
 __device__ __forceinline__ int floor_div4(int v) { return v >= 0 ? (v >> 2) : -((-v + 3) >> 2); }
 
@@ -140,52 +142,57 @@ __global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
     const WeftPrim* __restrict__ prims, const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1,
     int n_res1, float* __restrict__ out, int H, int W) {
-    __shared__ Prep sp[MAX_TILE_PRIMS];
-    __shared__ float grid[48];
-    __shared__ float ctrl[48];
-    const int lane = threadIdx.x & 31;
+    __shared__ Prep sp_all[DEC_WARPS][MAX_TILE_PRIMS];
+    __shared__ float grid_all[DEC_WARPS][48];
+    __shared__ float ctrl_all[DEC_WARPS][48];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    Prep* sp = sp_all[wid];
+    float* grid = grid_all[wid];
+    float* ctrl = ctrl_all[wid];
     const bool w_aligned = (W & 3) == 0;
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+    const int n_warps = gridDim.x * DEC_WARPS;
+    for (int it = blockIdx.x * DEC_WARPS + wid; it < n_items; it += n_warps) {
         const int2 item = items[it];
-        __syncthreads();  // the previous item's readers of sp/grid/ctrl are done
+        __syncwarp();  // this warp's readers of sp/grid/ctrl from the previous item are done
         if (item.x < 0 || item.x >= n_tiles) {
-            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            if (lane == 0) report(WEFTK_E_ARG);
             continue;
         }
         const WeftTileDecodeDesc d = descs[item.x];
         const int n = d.prim_count, w = d.target_w, h = d.target_h;
         if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || d.source_size <= 0) {
-            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            if (lane == 0) report(WEFTK_E_ARG);
             continue;
         }
         const int a0 = floor_div4(d.target_x0);
         const int G = floor_div4(d.target_x0 + w + 3) - a0;  // aligned groups per row
         const long long n_groups = (long long)G * h;
-        const int n_chunks = (int)((n_groups + DEC_THREADS - 1) / DEC_THREADS);
+        const int n_chunks = (int)((n_groups + 31) / 32);
         const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
-        for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
+        for (int i = lane; i < n; i += 32) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
         const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
         if (has_res1 && d.res1_index >= n_res1) {
-            if (threadIdx.x == 0) report(WEFTK_E_ARG);
+            if (lane == 0) report(WEFTK_E_ARG);
             continue;
         }
-        if (has_res1 && threadIdx.x < 48) grid[threadIdx.x] = res1[(size_t)d.res1_index * 48 + threadIdx.x];
-        __syncthreads();
+        if (has_res1)
+            for (int i = lane; i < 48; i += 32) grid[i] = res1[(size_t)d.res1_index * 48 + i];
+        __syncwarp();
         const bool bic = (n == 1 && sp[0].kind == K_BICUBIC);
         if (bic) {
             const int gi = (int)sp[0].q[0];
             if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
-                if (threadIdx.x == 0) report(WEFTK_E_ARG);
+                if (lane == 0) report(WEFTK_E_ARG);
                 continue;
             }
-            if (threadIdx.x < 48) ctrl[threadIdx.x] = cp48[(size_t)gi * 48 + threadIdx.x];
-            __syncthreads();
+            for (int i = lane; i < 48; i += 32) ctrl[i] = cp48[(size_t)gi * 48 + i];
+            __syncwarp();
         }
         const int side = max(w, h);
         const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
         const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
         for (int chunk = item.y; chunk < c_end; ++chunk) {
-            const long long g = (long long)chunk * DEC_THREADS + threadIdx.x;
+            const long long g = (long long)chunk * 32 + lane;
             const bool g_ok = g < n_groups;
             const int row = g_ok ? (int)(g / G) : 0;
             const int gxs = (a0 + (g_ok ? (int)(g % G) : 0)) * 4;
@@ -298,7 +305,7 @@ int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const in
     int dev = 0, sms = 148;
     WEFTK_CUDA(cudaGetDevice(&dev));
     WEFTK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int blocks = std::min(n_items, sms * 8 * 2);
+    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * 4 * 2);
     render_tiles_kernel<<<blocks, DEC_THREADS, 0, stream>>>(d_descs, n_tiles, d_items, n_items, d_prims, d_cp48,
                                                             n_cp48, d_res1, n_res1, d_out, out_h, out_w);
     WEFTK_CUDA(cudaGetLastError());

@@ -21,8 +21,8 @@ from . import _lib
 from ._lib import PRIM_DTYPE, TILE_DECODE_DTYPE
 
 MAX_TILE_PRIMS = 48
-DECODE_CHUNK_GROUPS = 128  # WEFTK_DECODE_CHUNK_GROUPS
-DECODE_ITEM_CHUNKS = 2     # WEFTK_DECODE_ITEM_CHUNKS
+DECODE_CHUNK_GROUPS = 32   # WEFTK_DECODE_CHUNK_GROUPS
+DECODE_ITEM_CHUNKS = 8     # WEFTK_DECODE_ITEM_CHUNKS
 
 
 def decode_items(descs: np.ndarray) -> np.ndarray:

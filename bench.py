@@ -227,6 +227,70 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
             "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims))}
 
 
+def _recon_of(stack_set, params, tiles, size):
+    """Per-tile clipped renders of parameter rows (no residuals), via the GPU decoder walk."""
+    from weft_b200 import render
+
+    class _R:
+        def __init__(self, p):
+            self.primitives = p
+            self.residual_rgb = (0, 0, 0)
+
+    stacks = stack_set.to_stacks(params)
+    pw = ((size + 63) // 64) * 64
+    full = render.render_scene_adaptive([_R(s) for s in stacks], tiles, pw, pw)
+    return stacks, [full[t.y:t.y + t.size, t.x:t.x + t.size] for t in tiles]
+
+
+def rd_compare(args, fit, tiles, patches, pools, img, stream):
+    """RD of the plain fit vs a fast fit (init over non-curve candidates) refined with Adam.
+
+    Both are written as WEFT files (RES0/RES1 included) and decoded; RD = PSNR - 4 BPP.
+    Times are CUDA-event device times of the whole fit, state resident, after warm-up.
+    """
+    import torch
+
+    from weft_b200.encode import encode_fit, rd_score
+    from weft_b200.fit import BatchedFit
+    from weft_b200.refine import refine
+
+    size = args.size
+    plain_stacks = fit.selected()
+    plain = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, plain_stacks, fit.recon_tiles()), QUALITY)
+    fast_pools = [p[p["kind"] != 3] for p in pools]
+    fast = BatchedFit.from_arrays(np.concatenate([p.reshape(-1, 3) for p in patches]),
+                                  np.array([p.shape[0] for p in patches], np.int32), np.concatenate(fast_pools),
+                                  np.array([len(p) for p in fast_pools], np.int64), QUALITY, caps=[CAP] * len(patches),
+                                  device=torch.cuda.current_device())
+
+    def refined_step():
+        fast.reset()
+        fast.run(max_rounds=0)
+        ss, params = fast.stack_set()
+        out, hist = refine(ss, params, steps=args.refine_steps, lr=args.refine_lr)
+        return ss, out, hist
+
+    for _ in range(2):
+        refined_step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ss, out, hist = refined_step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_ref = a.elapsed_time(b)
+    q = ss.quantize(out)
+    stacks_r, recon_r = _recon_of(ss, out, tiles, size)
+    refined = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, ss.to_stacks(q), recon_r), QUALITY)
+    n_px = size * size
+    return {"plain": {**plain, "prims": sum(len(s) for s in plain_stacks)},
+            "refined": {**refined, "ms": ms_ref, "mpix_per_s": n_px / (ms_ref * 1e-3) / 1e6,
+                        "adam_steps": args.refine_steps, "lr": args.refine_lr,
+                        "init": "best single non-curve candidate per tile, no greedy rounds",
+                        "loss_first_last": [hist[0], hist[-1]] if hist else None},
+            "rd_delta_db": refined["rd_score"] - plain["rd_score"]}
+
+
 def _hbm_peak() -> tuple[float, str]:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -291,6 +355,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--decode-iters", type=int, default=10)
+    ap.add_argument("--refine-steps", type=int, default=20, help="Adam steps of the refined fit (-1: skip)")
+    ap.add_argument("--refine-lr", type=float, default=1e-2)
     args = ap.parse_args()
 
     # Process pools first: spawned before any CUDA initialisation.
@@ -396,6 +462,8 @@ def run_weft(args, world, rank, local, executor, cores):
     decode = decode_bench(fit, tiles, args.size, args.size, 3840, 2160, args.decode_iters, _hbm_peak()) \
         if args.decode_iters > 0 else None
 
+    rd = rd_compare(args, fit, tiles, patches, pools, img, stream) if args.refine_steps >= 0 else None
+
     # e2e through the public API from host buffers
     e2e_ms = []
     h2d = d2h = 0
@@ -446,6 +514,7 @@ def run_weft(args, world, rank, local, executor, cores):
                 "cand_gen_s": cand_s, "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
                 "prim_payload_bytes": prim_bytes},
         "decode": decode,
+        "rd": rd,
     }
     print(json.dumps(line), flush=True)
 

@@ -127,8 +127,8 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
  *   d_cp48  [n_cp48 * 48]  control grids for kind-5 tiles (may be NULL)
  *   d_res1  [n_res1 * 48]  RES1 grids, (4, 4, 3) row-major, float (may be NULL;
  *                          res1_index is ignored when n_res1 == 0)
- * Tiles with more than 48 primitives, a bad rect or an out-of-range grid index
- * are skipped and reported through weftk_device_status.
+ * Tiles with more than 48 primitives, a rect side outside 1..8192 or an
+ * out-of-range grid index are skipped and reported through weftk_device_status.
  */
 #define WEFTK_DECODE_CHUNK_GROUPS 32
 #define WEFTK_DECODE_ITEM_CHUNKS 8

@@ -25,6 +25,9 @@ What is captured (reference function -> fixture):
                                                            -> quadtree.npz
   * ``encoder._worker_gen_cands`` / ``_generate_residual_candidates``
     (src/weft/encoder.py:2490, :1255)                       -> candidates.npz
+  * ``encoder.encode_image`` + ``decoder.decode_to_array`` of a small image, and the
+    reference decoder reading this repo's re-encode of the same records
+    (src/weft/encoder.py:3573, src/weft/decoder.py:650)     -> container.npz
   * ``encoder._fit_adaptive_state`` greedy (src/weft/encoder.py:2520-2831),
     driven by a CPU scorer that renders each eval with the reference's own
     ``render_tile`` at pixel centres (the reference GPU launcher
@@ -499,9 +502,59 @@ def gen_fit(ref, name: str = "fit_small.npz", size: int = 64, n_prims: int = 10,
           **{"rs_" + k: v for k, v in rs.items()})
 
 
+def gen_container(ref) -> None:
+    """Reference encode -> file A (+ its decode); this repo's writer re-encodes A's
+    records -> file B, which the reference decoder must read (+ its decode)."""
+    from PIL import Image
+
+    from weft_b200 import bitstream
+    from weft_b200.candidates import Cand
+    from weft_b200.synth import make_image_u8
+
+    enc = ref["encoder"]
+    gr = ref["gpu_render"]
+    dec_mod = ref["decoder"]
+    prim_chunks = ref["prim_chunks"]
+    score, _ = _cpu_score_prepacked(ref)
+    saved = (gr.gpu_batch_score_prepacked, enc._get_persistent_worker_pool, dec_mod._decode_prim_payload)
+    gr.gpu_batch_score_prepacked = score
+    enc._get_persistent_worker_pool = lambda: None
+    dec_mod._decode_prim_payload = lambda weft: (
+        prim_chunks.decode_prim_payload(weft.prim_payload, weft.toc, weft.chunk_index), "cpu")
+    try:
+        img_u8 = make_image_u8(64, 64, 8, 21)
+        with tempfile.TemporaryDirectory() as td:
+            src = os.path.join(td, "in.png")
+            Image.fromarray(img_u8).save(src)
+            fa = os.path.join(td, "a.weft")
+            enc.encode_image(src, fa, ref["EncodeConfig"](quality=75))
+            blob_a = open(fa, "rb").read()
+            dec_a = dec_mod.decode_to_array(fa)
+            wf = bitstream.decode_weft(blob_a)
+            tiles = [type("QT", (), {"x": x, "y": y, "size": sz})() for x, y, sz in wf.qtree]
+            stacks = [[Cand(k, g, c0, c1, a) for k, g, c0, c1, a in st]
+                      for st in bitstream.decode_tiles(wf.prim_raw, wf.toc)]
+            blob_b = bitstream.encode_weft(wf.width, wf.height, wf.quality, tiles, stacks, wf.residuals, wf.res1_maps)
+            fb = os.path.join(td, "b.weft")
+            open(fb, "wb").write(blob_b)
+            dec_b = dec_mod.decode_to_array(fb)
+            ra = ref["bitstream"].decode_weft(blob_a)
+            rb = ref["bitstream"].decode_weft(blob_b)
+            for attr in ("prim_payload", "res0_payload", "res1_payload", "qtree_payload", "cidx_payload"):
+                assert getattr(ra, attr) == getattr(rb, attr), attr
+            assert ra.toc == rb.toc
+    finally:
+        gr.gpu_batch_score_prepacked, enc._get_persistent_worker_pool, dec_mod._decode_prim_payload = saved
+    print(f"container: reference file {len(blob_a)} B, re-encoded {len(blob_b)} B; payload blocks identical")
+    _save("container.npz", image_u8=img_u8, file_a=np.frombuffer(blob_a, np.uint8), decoded_a=dec_a.astype(np.float32),
+          file_b=np.frombuffer(blob_b, np.uint8), decoded_b=dec_b.astype(np.float32))
+
+
 def main() -> None:
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     sys.path.insert(0, src)
+    import weft.bitstream as bitstream_mod
+    import weft.decoder as decoder
     import weft.encoder as encoder
     import weft.entropy as entropy
     import weft.gpu_render as gpu_render
@@ -515,12 +568,13 @@ def main() -> None:
         "encoder": encoder, "entropy": entropy, "gpu_render": gpu_render, "prim_chunks": prim_chunks,
         "primitives": primitives, "quadtree": quadtree, "render": render,
         "Primitive": primitives.Primitive, "TileRecord": primitives.TileRecord, "EncodeConfig": EncodeConfig,
+        "decoder": decoder, "bitstream": bitstream_mod,
     }
     which = set(sys.argv[2:]) if len(sys.argv) > 2 else None
     for name, fn in (("render_tiles", gen_render_tiles), ("render_scene", gen_render_scene), ("rate", gen_rate),
                      ("entropy", gen_entropy), ("quant", gen_quant), ("quadtree", gen_quadtree),
                      ("candidates", gen_candidates), ("fit", gen_fit),
-                     ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92))):
+                     ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("container", gen_container)):
         if which is None or name in which:
             fn(ref)
 

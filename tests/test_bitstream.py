@@ -1,0 +1,54 @@
+"""The product's WEFT writer/reader against the reference's bytes (golden fixtures)."""
+
+from __future__ import annotations
+
+import numpy as np
+
+from oracle.primitives import prims_from_pack
+from tests.test_oracle_golden import _pack
+from weft_b200 import bitstream
+from weft_b200.candidates import Cand
+
+
+def test_rans_and_chunks_bit_exact(golden):
+    g = golden("entropy.npz")
+    pay, po, enc, eo = g["payload"], g["payload_off"], g["encoded"], g["encoded_off"]
+    for i in range(len(po) - 1):
+        data = pay[po[i]:po[i + 1]].tobytes()
+        want = enc[eo[i]:eo[i + 1]].tobytes()
+        assert bitstream.encode_bytes(data) == want, f"payload {i}"
+        assert bitstream.decode_bytes(want) == data
+    raw = g["prim_raw"].tobytes()
+    toc = [int(v) for v in g["toc"]]
+    for n, key in ((64, "64"), (7, "7")):
+        coded, entries = bitstream.build_prim_chunks(raw, toc, n)
+        assert coded == g["coded" + key].tobytes()
+        assert entries == [tuple(int(v) for v in e) for e in g["entries" + key]]
+
+
+def test_tile_payloads_bit_exact(golden):
+    g = golden("quant.npz")
+    a = _pack(g, "in_")
+    prims = prims_from_pack(a, 0, len(a["kind"]))
+    stacks, k = [], 0
+    for c in g["tile_counts"]:
+        stacks.append(prims[k:k + int(c)])
+        k += int(c)
+    blob, toc = bitstream.encode_tiles(stacks)
+    assert blob == g["tiles_raw"].tobytes()
+    assert toc == [int(v) for v in g["toc"]]
+    back = bitstream.decode_tiles(blob, toc)
+    assert [len(t) for t in back] == [len(s) for s in stacks]
+
+
+def test_reader_parses_reference_file_and_writer_reproduces_its_payloads(golden):
+    g = golden("container.npz")
+    blob_a = g["file_a"].tobytes()
+    wf = bitstream.decode_weft(blob_a)
+    tiles = [type("QT", (), {"x": x, "y": y, "size": s})() for x, y, s in wf.qtree]
+    stacks = [[Cand(k, gg, c0, c1, al) for k, gg, c0, c1, al in st] for st in bitstream.decode_tiles(wf.prim_raw, wf.toc)]
+    blob = bitstream.encode_weft(wf.width, wf.height, wf.quality, tiles, stacks, wf.residuals, wf.res1_maps)
+    assert blob == g["file_b"].tobytes()  # the file the reference decoder was shown to read
+    wb = bitstream.decode_weft(blob)
+    assert wb.prim_raw == wf.prim_raw and wb.toc == wf.toc and wb.residuals == wf.residuals
+    assert all(np.array_equal(x, y) for x, y in zip(wb.res1_maps, wf.res1_maps))

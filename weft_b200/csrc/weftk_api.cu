@@ -177,7 +177,8 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
             for (long long c = 0; c < chunks; c += WEFTK_DECODE_ITEM_CHUNKS) items.push_back(make_int2(i, (int)c));
         }
         if (d.prim_count < 0 || d.prim_count > 48 || d.prim_offset < 0 || (int64_t)d.prim_offset + d.prim_count > n_prims ||
-            d.target_w <= 0 || d.target_h <= 0 || d.source_size <= 0 || (n_res1 > 0 && d.res1_index >= n_res1))
+            d.target_w <= 0 || d.target_h <= 0 || d.target_w > 8192 || d.target_h > 8192 || d.source_size <= 0 ||
+            (n_res1 > 0 && d.res1_index >= n_res1))
             return fail(WEFTK_E_ARG, "render_tiles_host: tile " + std::to_string(i) + " is out of range");
         if (d.prim_count == 1 && h_prims[d.prim_offset].kind == 5) {
             int idx = (int)h_prims[d.prim_offset].geom[0];

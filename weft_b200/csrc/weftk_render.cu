@@ -138,7 +138,7 @@ constexpr int DEC_WARPS = DEC_THREADS / 32;
 
 __device__ __forceinline__ int floor_div4(int v) { return v >= 0 ? (v >> 2) : -((-v + 3) >> 2); }
 
-__global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
+__global__ void __launch_bounds__(DEC_THREADS, 6) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
     const WeftPrim* __restrict__ prims, const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1,
     int n_res1, float* __restrict__ out, int H, int W) {
@@ -160,14 +160,15 @@ __global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
         }
         const WeftTileDecodeDesc d = descs[item.x];
         const int n = d.prim_count, w = d.target_w, h = d.target_h;
-        if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || d.source_size <= 0) {
+        if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || w > 8192 || h > 8192 || d.source_size <= 0) {
             if (lane == 0) report(WEFTK_E_ARG);
             continue;
         }
         const int a0 = floor_div4(d.target_x0);
         const int G = floor_div4(d.target_x0 + w + 3) - a0;  // aligned groups per row
-        const long long n_groups = (long long)G * h;
-        const int n_chunks = (int)((n_groups + 31) / 32);
+        const int n_groups = G * h;                          // < 2^24 for any rect the host accepts
+        const int n_chunks = (n_groups + 31) / 32;
+        const float invG = 1.0f / (float)G;
         const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
         for (int i = lane; i < n; i += 32) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
         const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
@@ -192,10 +193,14 @@ __global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
         const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
         const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
         for (int chunk = item.y; chunk < c_end; ++chunk) {
-            const long long g = (long long)chunk * 32 + lane;
+            const int g = chunk * 32 + lane;
             const bool g_ok = g < n_groups;
-            const int row = g_ok ? (int)(g / G) : 0;
-            const int gxs = (a0 + (g_ok ? (int)(g % G) : 0)) * 4;
+            // row = g / G via the float reciprocal, corrected by one step (exact for g < 2^24)
+            int row = __float2int_rz(((float)g + 0.5f) * invG);
+            row -= (row * G > g) ? 1 : 0;
+            row += ((row + 1) * G <= g) ? 1 : 0;
+            if (!g_ok) row = 0;
+            const int gxs = (a0 + (g_ok ? g - row * G : 0)) * 4;
             float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
             int lx[DEC_PPL];
             bool valid[DEC_PPL];
@@ -305,7 +310,7 @@ int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const in
     int dev = 0, sms = 148;
     WEFTK_CUDA(cudaGetDevice(&dev));
     WEFTK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * 4 * 2);
+    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * 6 * 2);
     render_tiles_kernel<<<blocks, DEC_THREADS, 0, stream>>>(d_descs, n_tiles, d_items, n_items, d_prims, d_cp48,
                                                             n_cp48, d_res1, n_res1, d_out, out_h, out_w);
     WEFTK_CUDA(cudaGetLastError());

@@ -400,6 +400,29 @@ class BatchedFit:
         """The selected primitives of every tile as ``Cand`` objects (float32-rounded values)."""
         return [unpack_cands(r) for r in self.selected_records()]
 
+    def stack_set(self):
+        """The selected stacks as a ``refine.StackSet`` over this fit's resident tiles, with the
+        parameter rows gathered on the device (no host round trip of the records)."""
+        from .refine import StackSet
+
+        n_sel = self.t_n_sel.to(torch.int64)
+        counts = n_sel.cpu().numpy()
+        prim_off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        sel = self.t_sel.view(self.n, self.cap_max).to(torch.int64)
+        col = torch.arange(self.cap_max, device=self.device)[None, :]
+        mask = col < n_sel[:, None]
+        slots = (torch.from_numpy(self.pool_off).to(self.device)[:, None] + sel)[mask]
+        recs = self.t_cand.view(-1, PRIM_DTYPE.itemsize)[slots]
+        f = recs.view(torch.float32).view(-1, 15)
+        kinds = recs.view(torch.int32)[:, 0].contiguous()
+        params = torch.zeros((slots.numel(), 16), dtype=torch.float32, device=self.device)
+        params[:, 0:7] = f[:, 1:8]
+        params[:, 7:10] = f[:, 8:11]
+        params[:, 10:13] = f[:, 11:14]
+        params[:, 13] = f[:, 14]
+        ss = StackSet(self.t_src, self.t_px_off, self.t_size, prim_off, kinds.cpu().numpy(), self.device.index or 0)
+        return ss, params
+
     def objectives(self) -> np.ndarray:
         return self.t_cur_obj.cpu().numpy()
 

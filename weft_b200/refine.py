@@ -150,6 +150,16 @@ class StackSet:
         return p.to(torch.float32)
 
 
+    def to_stacks(self, params: torch.Tensor) -> list[list]:
+        """Parameter rows -> per-tile ``Cand`` lists (host)."""
+        from .fit import unpack_cands
+
+        recs = rows_to_records(params.detach().cpu().numpy(), self.kinds_np)
+        cands = unpack_cands(recs)
+        off = self.prim_off_np
+        return [cands[off[t]:off[t + 1]] for t in range(self.n)]
+
+
 def ctypes_addr(st) -> int:
     import ctypes
 

@@ -242,53 +242,59 @@ def _recon_of(stack_set, params, tiles, size):
     return stacks, [full[t.y:t.y + t.size, t.x:t.x + t.size] for t in tiles]
 
 
-def rd_compare(args, fit, tiles, patches, pools, img, stream):
-    """RD of the plain fit vs a fast fit (init over non-curve candidates) refined with Adam.
+REFINE_POOLS = {"nocurve": (0, 1, 2, 4, 5), "smooth": (0, 1, 2), "constlin": (0, 1)}
 
-    Both are written as WEFT files (RES0/RES1 included) and decoded; RD = PSNR - 4 BPP.
-    Times are CUDA-event device times of the whole fit, state resident, after warm-up.
+
+def rd_compare(args, fit, tiles, patches, pools, img, stream):
+    """RD of the plain fit vs refined fast fits, both written as WEFT files (RES0/RES1
+    included) and decoded; RD = PSNR - 4 BPP.
+
+    A refined fast fit scores only the init round over a kind-filtered pool (best single
+    candidate per tile), then runs fused Adam steps on that primitive; the whole pipeline
+    is one CUDA graph.  Times are CUDA-event device times of a graph replay, state
+    resident, after warm-up (mean of ``--refine-reps`` replays).
     """
     import torch
 
     from weft_b200.encode import encode_fit, rd_score
     from weft_b200.fit import BatchedFit
-    from weft_b200.refine import refine
+    from weft_b200.refine import RefinedFit
 
     size = args.size
+    n_px = size * size
     plain_stacks = fit.selected()
     plain = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, plain_stacks, fit.recon_tiles()), QUALITY)
-    fast_pools = [p[p["kind"] != 3] for p in pools]
-    fast = BatchedFit.from_arrays(np.concatenate([p.reshape(-1, 3) for p in patches]),
-                                  np.array([p.shape[0] for p in patches], np.int32), np.concatenate(fast_pools),
-                                  np.array([len(p) for p in fast_pools], np.int64), QUALITY, caps=[CAP] * len(patches),
-                                  device=torch.cuda.current_device())
-
-    def refined_step():
-        fast.reset()
-        fast.run(max_rounds=0)
-        ss, params = fast.stack_set()
-        out, hist = refine(ss, params, steps=args.refine_steps, lr=args.refine_lr)
-        return ss, out, hist
-
-    for _ in range(2):
-        refined_step()
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    ss, out, hist = refined_step()
-    b.record(stream)
-    torch.cuda.synchronize()
-    ms_ref = a.elapsed_time(b)
-    q = ss.quantize(out)
-    stacks_r, recon_r = _recon_of(ss, out, tiles, size)
-    refined = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, ss.to_stacks(q), recon_r), QUALITY)
-    n_px = size * size
-    return {"plain": {**plain, "prims": sum(len(s) for s in plain_stacks)},
-            "refined": {**refined, "ms": ms_ref, "mpix_per_s": n_px / (ms_ref * 1e-3) / 1e6,
-                        "adam_steps": args.refine_steps, "lr": args.refine_lr,
-                        "init": "best single non-curve candidate per tile, no greedy rounds",
-                        "loss_first_last": [hist[0], hist[-1]] if hist else None},
-            "rd_delta_db": refined["rd_score"] - plain["rd_score"]}
+    pixels = np.concatenate([p.reshape(-1, 3) for p in patches])
+    sizes = np.array([p.shape[0] for p in patches], np.int32)
+    variants = []
+    for spec in args.refine_variants.split(","):
+        name, steps = spec.split(":")
+        keep = REFINE_POOLS[name]
+        fast_pools = [p[np.isin(p["kind"], keep)] for p in pools]
+        fast = BatchedFit.from_arrays(pixels, sizes, np.concatenate(fast_pools),
+                                      np.array([len(p) for p in fast_pools], np.int64), QUALITY,
+                                      caps=[CAP] * len(patches), device=torch.cuda.current_device(), reserve=0)
+        rf = RefinedFit(fast, steps=int(steps), lr=args.refine_lr, use_graph=True)
+        for _ in range(2):
+            rf.run()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.refine_reps):
+            out = rf.run()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.refine_reps
+        ss = rf.ss
+        q = ss.quantize(out)
+        recon = _recon_of(ss, q, tiles, size)[1]
+        sc = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, ss.to_stacks(q), recon), QUALITY)
+        variants.append({"pool": name, "kinds": list(keep), "adam_steps": int(steps), **sc, "ms": ms,
+                         "mpix_per_s": n_px / (ms * 1e-3) / 1e6, "rd_delta_db": sc["rd_score"] - plain["rd_score"]})
+        del rf, fast
+    return {"plain": {**plain, "prims": sum(len(s) for s in plain_stacks)}, "lr": args.refine_lr,
+            "refined": variants,
+            "init": "best single candidate per tile from the kind-filtered pool, no greedy rounds"}
 
 
 def _hbm_peak() -> tuple[float, str]:
@@ -355,7 +361,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--decode-iters", type=int, default=10)
-    ap.add_argument("--refine-steps", type=int, default=20, help="Adam steps of the refined fit (-1: skip)")
+    ap.add_argument("--refine-variants", default="nocurve:20,smooth:20,constlin:20,constlin:0",
+                    help="refined fits to compare, pool:adam_steps (empty: skip)")
+    ap.add_argument("--refine-reps", type=int, default=5)
     ap.add_argument("--refine-lr", type=float, default=1e-2)
     args = ap.parse_args()
 
@@ -462,7 +470,7 @@ def run_weft(args, world, rank, local, executor, cores):
     decode = decode_bench(fit, tiles, args.size, args.size, 3840, 2160, args.decode_iters, _hbm_peak()) \
         if args.decode_iters > 0 else None
 
-    rd = rd_compare(args, fit, tiles, patches, pools, img, stream) if args.refine_steps >= 0 else None
+    rd = rd_compare(args, fit, tiles, patches, pools, img, stream) if args.refine_variants else None
 
     # e2e through the public API from host buffers
     e2e_ms = []

@@ -45,9 +45,19 @@ typedef struct WeftStackSet {
 int weftk_stack_loss(const WeftStackSet* set, const float* d_params, float* d_loss, int flags, void* stream);
 
 /* grad_params = sum_t grad_loss[t] * d loss[t] / d params (rows of untouched
- * tiles are written with zeros; rows are owned by one tile, so no atomics). */
+ * tiles are written with zeros; rows are owned by one tile, so no atomics).
+ * d_loss (may be NULL) receives loss[t] from the same pass (the backward
+ * re-renders every pixel anyway). */
 int weftk_stack_loss_backward(const WeftStackSet* set, const float* d_params, const float* d_grad_loss,
-                              float* d_grad_params, int flags, void* stream);
+                              float* d_grad_params, float* d_loss, int flags, void* stream);
+
+/* One Adam step (PyTorch's update rule, FP32 moments) on every row, fused with the
+ * projection onto what the wire format carries: colours and alpha in [0, 1],
+ * coordinates in [0, 15], thickness in [0, 4] (src/weft/primitives.py:102-177).
+ * d_step holds the step count t-1 on entry and is incremented by the call, so a
+ * captured sequence of calls replays correctly. */
+int weftk_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, const int32_t* d_kind,
+                    int n_rows, float lr, float beta1, float beta2, float eps, int32_t* d_step, void* stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,80 @@
+"""The fused refine path (one loss+gradient launch and one Adam+projection launch per
+step) against the autograd + torch.optim.Adam path, and the graph-captured refined fit
+against the same work launched eagerly.
+
+Workload: a 256x256 synthetic image (40 primitives, seed 0), quadtree 8-64 px on u8
+luminance variance > 100, q=75 candidate pools.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _fit(kinds_out=()):
+    from weft_b200 import candidates, quadtree
+    from weft_b200.fit import BatchedFit
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(256, 256, 40, 0)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    pools = [[c for c in candidates.tile_candidates(p, 75) if c.kind not in kinds_out] for p in patches]
+    return BatchedFit(patches, pools, 75, caps=[16] * len(qts))
+
+
+def test_backward_loss_output_equals_forward():
+    from weft_b200.refine import FusedRefiner
+
+    fit = _fit().run()
+    ss, params = fit.stack_set()
+    fr = FusedRefiner(ss, params)
+    want = ss.loss(fr.p).cpu().numpy()
+    fr.step()
+    got = fr.loss.cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-9)
+
+
+def test_fused_refiner_matches_torch_adam():
+    from weft_b200.refine import FusedRefiner, refine
+
+    fit = _fit().run()
+    ss, params = fit.stack_set()
+    steps = 15
+    want, hist = refine(ss, params, steps=steps, lr=1e-2)
+    fr = FusedRefiner(ss, params, lr=1e-2)
+    losses = []
+    for _ in range(steps):
+        fr.step()
+        losses.append(float((fr.loss * ss.weights).sum()))
+    got = fr.p
+    # Same update rule; the bias corrections are computed in float32 on the device
+    # versus double on the host, so trajectories agree to rounding, not bit for bit.
+    assert float((got[:, :14] - want[:, :14]).abs().max()) < 2e-3
+    np.testing.assert_allclose(losses, hist, rtol=1e-4)
+    assert int(fr.step_ctr.item()) == steps
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_refined_fit_matches_unfused_pipeline(use_graph):
+    from weft_b200.refine import FusedRefiner, RefinedFit
+
+    fit = _fit(kinds_out=(3,))
+    rf = RefinedFit(fit, steps=10, lr=1e-2, use_graph=use_graph)
+    got = rf.run().clone()
+    got2 = rf.run().clone()  # replays start from the same state
+    assert torch.equal(got, got2)
+
+    fit.reset()
+    fit.run(max_rounds=0)
+    ss, params = fit.stack_set()
+    assert np.array_equal(ss.prim_off_np, rf.ss.prim_off_np)
+    assert torch.equal(ss.t_kind, rf.kinds)
+    fr = FusedRefiner(ss, params, lr=1e-2)
+    fr.run(10)
+    assert torch.equal(fr.p[:, :14], got[:, :14])

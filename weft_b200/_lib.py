@@ -86,7 +86,9 @@ SIGNATURES: dict[str, list] = {
     "weftk_fit_round_static": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P],
     "weftk_fit_reseed": [_P, _I, _P],
     "weftk_stack_loss": [_P, _P, _P, _I, _P],
-    "weftk_stack_loss_backward": [_P, _P, _P, _P, _I, _P],
+    "weftk_stack_loss_backward": [_P, _P, _P, _P, _P, _I, _P],
+    "weftk_adam_step": [_P, _P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P,
+                        _P],
     "weftk_measure_fp32_peak": [_P],
 }
 

@@ -309,7 +309,8 @@ __global__ void __launch_bounds__(RF_THREADS) stack_loss_kernel(WeftStackSet set
 
 __global__ void __launch_bounds__(RF_THREADS) stack_backward_kernel(WeftStackSet set, const float* __restrict__ params,
                                                                     const float* __restrict__ grad_loss,
-                                                                    float* __restrict__ grad, int flags) {
+                                                                    float* __restrict__ grad, float* __restrict__ loss,
+                                                                    int flags) {
     extern __shared__ float hist[];  // [K][RF_THREADS][3]: composite before each layer
     __shared__ RfShared s;
     const int t = blockIdx.x;
@@ -323,6 +324,7 @@ __global__ void __launch_bounds__(RF_THREADS) stack_backward_kernel(WeftStackSet
     const float4* src = reinterpret_cast<const float4*>(set.src) + set.px_off[t];
     const int n = ts * ts, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const float scale = grad_loss[t] * 2.0f / (3.0f * (float)n);
+    double sse = 0.0;
     for (int base = 0; base < n; base += RF_THREADS) {
         const int p = base + tid;
         const bool valid = p < n;
@@ -343,8 +345,11 @@ __global__ void __launch_bounds__(RF_THREADS) stack_backward_kernel(WeftStackSet
             const float4 v = src[p];
             const float sv[3] = {v.x, v.y, v.z};
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch)
-                g[ch] = (c[ch] >= 0.0f && c[ch] <= 1.0f) ? scale * (clamp01(c[ch]) - sv[ch]) : 0.0f;
+            for (int ch = 0; ch < 3; ++ch) {
+                const float e = clamp01(c[ch]) - sv[ch];
+                sse += (double)(e * e);
+                g[ch] = (c[ch] >= 0.0f && c[ch] <= 1.0f) ? scale * e : 0.0f;
+            }
         }
         for (int k = K - 1; k >= 0; --k) {
             const float* h = hist + ((size_t)k * RF_THREADS + tid) * 3;
@@ -374,7 +379,46 @@ __global__ void __launch_bounds__(RF_THREADS) stack_backward_kernel(WeftStackSet
         const int k = i / 16, j = i % 16;
         grad[(size_t)(p0 + k) * 16 + j] = j < 14 ? s.gacc[k][j] : 0.0f;
     }
+    if (loss != nullptr) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(FULL, sse, o);
+        if (lane == 0) s.lred[warp] = sse;
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < RF_WARPS; ++w) tot += s.lred[w];
+            loss[t] = (float)(tot / (3.0 * n));
+        }
+    }
 }
+
+// Adam (PyTorch's rule) + projection onto the wire-representable box, one thread per value.
+__global__ void adam_project_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                    float* __restrict__ v, const int* __restrict__ kind, int n_rows, float lr,
+                                    float b1, float b2, float eps, const int* __restrict__ step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rows * 16) return;
+    const int col = i & 15, row = i >> 4;
+    if (col >= 14) return;
+    const float t = (float)(*step + 1);
+    const float gi = g[i];
+    const float mi = fmaf(b1, m[i], (1.0f - b1) * gi);
+    const float vi = fmaf(b2, v[i], (1.0f - b2) * gi * gi);
+    m[i] = mi;
+    v[i] = vi;
+    const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
+    float x = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    const int k = kind[row];
+    if (col >= 7) {
+        x = fminf(fmaxf(x, 0.0f), 1.0f);
+    } else {
+        const bool thick = (k == K_LINE && col == 4) || (k == K_CURVE && col == 6);
+        x = fminf(fmaxf(x, 0.0f), thick ? 4.0f : 15.0f);
+    }
+    p[i] = x;
+}
+
+__global__ void step_increment_kernel(int* step) { *step += 1; }
 
 }  // namespace weftk
 
@@ -390,8 +434,22 @@ extern "C" int weftk_stack_loss(const WeftStackSet* set, const float* d_params, 
     return WEFTK_OK;
 }
 
+extern "C" int weftk_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, const int32_t* d_kind,
+                               int n_rows, float lr, float beta1, float beta2, float eps, int32_t* d_step,
+                               void* stream) {
+    WEFTK_REQUIRE(n_rows >= 0 && (n_rows == 0 || (d_params && d_grads && d_m && d_v && d_kind && d_step)),
+                  "adam_step: bad arguments");
+    if (n_rows == 0) return WEFTK_OK;
+    const int n = n_rows * 16;
+    adam_project_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_params, d_grads, d_m, d_v, d_kind, n_rows,
+                                                                            lr, beta1, beta2, eps, d_step);
+    step_increment_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(d_step);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_stack_loss_backward(const WeftStackSet* set, const float* d_params, const float* d_grad_loss,
-                                         float* d_grad_params, int flags, void* stream) {
+                                         float* d_grad_params, float* d_loss, int flags, void* stream) {
     WEFTK_REQUIRE(set && d_grad_loss && d_grad_params, "stack_loss_backward: null argument");
     if (set->n_tiles == 0) return WEFTK_OK;
     WEFTK_REQUIRE(set->max_prims >= 0 && set->max_prims <= WEFTK_REFINE_MAX_PRIMS,
@@ -404,7 +462,7 @@ extern "C" int weftk_stack_loss_backward(const WeftStackSet* set, const float* d
         attr = MAXL * RF_THREADS * 3 * (int)sizeof(float);
     }
     stack_backward_kernel<<<set->n_tiles, RF_THREADS, smem, (cudaStream_t)stream>>>(*set, d_params, d_grad_loss,
-                                                                                     d_grad_params, flags);
+                                                                                     d_grad_params, d_loss, flags);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }

@@ -138,7 +138,7 @@ constexpr int DEC_WARPS = DEC_THREADS / 32;
 
 __device__ __forceinline__ int floor_div4(int v) { return v >= 0 ? (v >> 2) : -((-v + 3) >> 2); }
 
-__global__ void __launch_bounds__(DEC_THREADS, 6) render_tiles_kernel(
+__global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
     const WeftPrim* __restrict__ prims, const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1,
     int n_res1, float* __restrict__ out, int H, int W) {
@@ -310,7 +310,7 @@ int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const in
     int dev = 0, sms = 148;
     WEFTK_CUDA(cudaGetDevice(&dev));
     WEFTK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * 6 * 2);
+    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * 4 * 2);
     render_tiles_kernel<<<blocks, DEC_THREADS, 0, stream>>>(d_descs, n_tiles, d_items, n_items, d_prims, d_cp48,
                                                             n_cp48, d_res1, n_res1, d_out, out_h, out_w);
     WEFTK_CUDA(cudaGetLastError());

@@ -344,6 +344,34 @@ class BatchedFit:
         self.stats = FitStats()
         self.device_reseeded = False
 
+    # -------------------------------------------------------------- graph-capturable init-only fit
+    def _device_consts(self) -> None:
+        if not hasattr(self, "t_init_cnt"):
+            self.t_init_cnt = _dev(self.init_cnt, self.device)
+            self.t_zero_first = torch.zeros(self.n, dtype=torch.int32, device=self.device)
+
+    def run_init_only(self) -> None:
+        """Reset and run only the init round (best single candidate per tile), launching
+        device work only: no host copies or syncs, so it can be captured in a CUDA graph."""
+        self._device_consts()
+        self.t_pool_cnt.copy_(self.t_init_cnt)
+        self.t_bg.zero_()
+        self.t_n_alive.zero_()
+        self.t_n_sel.zero_()
+        self.t_sel_bits.fill_(8)
+        self.t_flags.zero_()
+        self.t_cur_obj.zero_()
+        self.t_sel.fill_(-1)
+        self.t_alive.zero_()
+        self.t_work.zero_()
+        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), self._stream()),
+                   "weftk_fit_prepare")
+        ti = self.t_items
+        rc = self.lib.weftk_fit_round(ctypes_ref(self.st), FIT_INIT, self.lam, self.thr, _lib.ptr(self.t_perm),
+                                      _lib.ptr(ti[8]), self.n_items[8], _lib.ptr(ti[16]), self.n_items[16],
+                                      _lib.ptr(ti[32]), self.n_items[32], self._stream())
+        _lib.check(rc, "weftk_fit_round")
+
     def work_counters(self) -> tuple[int, int]:
         """(candidate-pixels scored, algorithmic FP32 ops) since the last reset."""
         w = self.t_work.cpu().numpy()

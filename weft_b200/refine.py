@@ -52,7 +52,8 @@ class StackSet:
     """Per-tile stacks over tile pixels resident on the GPU."""
 
     def __init__(self, src: torch.Tensor, px_off: torch.Tensor, sizes: torch.Tensor, prim_off: np.ndarray,
-                 kinds: np.ndarray, device: int = 0):
+                 kinds, device: int = 0):
+        """``kinds``: per-row primitive kinds, a numpy array or a device int32 tensor (kept by reference)."""
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
         self.n = int(sizes.numel())
@@ -62,9 +63,13 @@ class StackSet:
             raise ValueError(f"stacks longer than {MAX_PRIMS} primitives are not supported")
         self.src, self.px_off, self.sizes = src, px_off, sizes
         self.prim_off_np = np.asarray(prim_off, np.int64)
-        self.kinds_np = np.asarray(kinds, np.int32)
+        if isinstance(kinds, torch.Tensor):
+            self.t_kind = kinds
+            self.kinds_np = None
+        else:
+            self.kinds_np = np.asarray(kinds, np.int32)
+            self.t_kind = torch.from_numpy(self.kinds_np).to(self.device)
         self.t_prim_off = torch.from_numpy(self.prim_off_np.astype(np.int32)).to(self.device)
-        self.t_kind = torch.from_numpy(self.kinds_np).to(self.device)
         self.st = _lib.WeftStackSet(self.n, self.max_prims, _lib.ptr(src), _lib.ptr(px_off), _lib.ptr(sizes),
                                     _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind))
         n_px = (sizes.to(torch.int64) ** 2)
@@ -115,23 +120,20 @@ class StackSet:
         g = grad_loss.detach().to(torch.float32).contiguous()
         out = torch.zeros_like(params)
         _lib.check(self.lib.weftk_stack_loss_backward(ctypes_addr(self.st), _lib.ptr(params), _lib.ptr(g),
-                                                      _lib.ptr(out), SOFT_TRIANGLES if soft else 0, self._stream()),
+                                                      _lib.ptr(out), 0, SOFT_TRIANGLES if soft else 0, self._stream()),
                    "weftk_stack_loss_backward")
         return out
 
     # --------------------------------------------------------------- parameter space
     def project_(self, params: torch.Tensor) -> None:
-        """Clamp rows onto what the wire format can represent (in place)."""
+        """Clamp rows onto what the wire format can represent (in place; no host sync,
+        so it can be captured in a CUDA graph)."""
         with torch.no_grad():
             params[:, 7:14].clamp_(0.0, 1.0)
+            params[:, 0:7].clamp_(0.0, 15.0)
             k = self.t_kind
-            geo = params[:, 0:7]
-            geo.clamp_(0.0, 15.0)
-            thick = torch.where(k == 2, 4, torch.where(k == 3, 6, -1))
-            rows = torch.nonzero(thick >= 0).flatten()
-            if rows.numel():
-                cols = thick[rows].long()
-                params[rows, cols] = params[rows, cols].clamp(0.0, 4.0)
+            for kind, col in ((2, 4), (3, 6)):
+                params[:, col] = torch.where(k == kind, params[:, col].clamp(0.0, 4.0), params[:, col])
 
     def quantize(self, params: torch.Tensor) -> torch.Tensor:
         """Snap to the wire grid: coordinates u16 over [0, 15], thickness u16 over [0, 4],
@@ -154,7 +156,8 @@ class StackSet:
         """Parameter rows -> per-tile ``Cand`` lists (host)."""
         from .fit import unpack_cands
 
-        recs = rows_to_records(params.detach().cpu().numpy(), self.kinds_np)
+        kinds = self.kinds_np if self.kinds_np is not None else self.t_kind.cpu().numpy()
+        recs = rows_to_records(params.detach().cpu().numpy(), kinds)
         cands = unpack_cands(recs)
         off = self.prim_off_np
         return [cands[off[t]:off[t + 1]] for t in range(self.n)]
@@ -200,3 +203,99 @@ def refine(stack_set: StackSet, params: torch.Tensor, steps: int = 200, lr: floa
         stack_set.project_(p.data)
         hist.append(loss.detach())
     return p.detach(), [float(h) for h in torch.stack(hist).cpu()] if hist else []
+
+
+class FusedRefiner:
+    """Adam refinement with one fused loss+gradient launch and one fused Adam+projection
+    launch per step (no autograd, no torch optimizer), optionally replayed from a CUDA
+    graph.  Same update rule as ``refine`` (PyTorch's Adam, FP32 moments)."""
+
+    def __init__(self, stack_set: StackSet, params: torch.Tensor, lr: float = 1e-2, betas=(0.9, 0.999),
+                 eps: float = 1e-8):
+        self.ss = stack_set
+        self.p = params.detach().clone().contiguous()
+        stack_set.project_(self.p)
+        self.g = torch.zeros_like(self.p)
+        self.m = torch.zeros_like(self.p)
+        self.v = torch.zeros_like(self.p)
+        self.loss = torch.zeros(stack_set.n, dtype=torch.float32, device=self.p.device)
+        self.step_ctr = torch.zeros(1, dtype=torch.int32, device=self.p.device)
+        self.w = stack_set.weights.contiguous()
+        self.lr, self.b1, self.b2, self.eps = float(lr), float(betas[0]), float(betas[1]), float(eps)
+
+    def step(self) -> None:
+        lib, ss = self.ss.lib, self.ss
+        s = ss._stream()
+        _lib.check(lib.weftk_stack_loss_backward(ctypes_addr(ss.st), _lib.ptr(self.p), _lib.ptr(self.w),
+                                                 _lib.ptr(self.g), _lib.ptr(self.loss), 0, s),
+                   "weftk_stack_loss_backward")
+        _lib.check(lib.weftk_adam_step(_lib.ptr(self.p), _lib.ptr(self.g), _lib.ptr(self.m), _lib.ptr(self.v),
+                                       _lib.ptr(ss.t_kind), int(self.p.shape[0]), self.lr, self.b1, self.b2, self.eps,
+                                       _lib.ptr(self.step_ctr), s), "weftk_adam_step")
+
+    def run(self, steps: int) -> torch.Tensor:
+        for _ in range(int(steps)):
+            self.step()
+        return self.p
+
+    def restart(self, params: torch.Tensor) -> None:
+        """New starting point, fresh moments (device ops only; capturable)."""
+        self.p.copy_(params)
+        self.ss.project_(self.p)
+        self.m.zero_()
+        self.v.zero_()
+        self.step_ctr.zero_()
+
+
+class RefinedFit:
+    """The refined batched fit as one CUDA graph: init-only candidate scoring over the
+    fit's (possibly kind-filtered) pools, gather of each tile's selected primitive, and
+    ``steps`` fused Adam steps.  Every launch is device work on torch's current stream."""
+
+    def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True):
+        self.fit = fit
+        dev = fit.device
+        has = fit.init_cnt > 0
+        self.rows = torch.from_numpy(np.nonzero(has)[0]).to(dev)
+        prim_off = np.concatenate([[0], np.cumsum(has.astype(np.int64))])
+        n_rows = int(has.sum())
+        self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
+        self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0)
+        self.start = torch.zeros((n_rows, 16), dtype=torch.float32, device=dev)
+        self.refiner = FusedRefiner(self.ss, self.start, lr=lr)
+        self.steps = int(steps)
+        self.pool_off = torch.from_numpy(fit.pool_off).to(dev)
+        self.graph = None
+        self.use_graph = use_graph
+
+    def _body(self) -> None:
+        f = self.fit
+        f.run_init_only()
+        sel = f.t_sel.view(f.n, f.cap_max)[self.rows, 0].to(torch.int64)
+        slots = self.pool_off[self.rows] + sel
+        recs = f.t_cand.view(-1, PRIM_DTYPE.itemsize)[slots]
+        fl = recs.view(torch.float32)
+        self.kinds.copy_(recs.view(torch.int32)[:, 0])
+        self.start[:, 0:7] = fl[:, 1:8]
+        self.start[:, 7:10] = fl[:, 8:11]
+        self.start[:, 10:13] = fl[:, 11:14]
+        self.start[:, 13] = fl[:, 14]
+        self.refiner.restart(self.start)
+        for _ in range(self.steps):
+            self.refiner.step()
+
+    def run(self) -> torch.Tensor:
+        if not self.use_graph:
+            self._body()
+            return self.refiner.p
+        if self.graph is None:
+            side = torch.cuda.Stream(self.fit.device)
+            side.wait_stream(torch.cuda.current_stream(self.fit.device))
+            with torch.cuda.stream(side):
+                self._body()  # warm-up outside capture (lazy allocations, attributes)
+            torch.cuda.current_stream(self.fit.device).wait_stream(side)
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph):
+                self._body()
+        self.graph.replay()
+        return self.refiner.p

@@ -268,13 +268,14 @@ def rd_compare(args, fit, tiles, patches, pools, img, stream):
     sizes = np.array([p.shape[0] for p in patches], np.int32)
     variants = []
     for spec in args.refine_variants.split(","):
-        name, steps = spec.split(":")
+        name, steps, *opt = spec.split(":")
+        residual = "r" in opt
         keep = REFINE_POOLS[name]
         fast_pools = [p[np.isin(p["kind"], keep)] for p in pools]
         fast = BatchedFit.from_arrays(pixels, sizes, np.concatenate(fast_pools),
                                       np.array([len(p) for p in fast_pools], np.int64), QUALITY,
                                       caps=[CAP] * len(patches), device=torch.cuda.current_device(), reserve=0)
-        rf = RefinedFit(fast, steps=int(steps), lr=args.refine_lr, use_graph=True)
+        rf = RefinedFit(fast, steps=int(steps), lr=args.refine_lr, use_graph=True, residual=residual)
         for _ in range(2):
             rf.run()
         torch.cuda.synchronize()
@@ -289,7 +290,8 @@ def rd_compare(args, fit, tiles, patches, pools, img, stream):
         q = ss.quantize(out)
         recon = _recon_of(ss, q, tiles, size)[1]
         sc = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, ss.to_stacks(q), recon), QUALITY)
-        variants.append({"pool": name, "kinds": list(keep), "adam_steps": int(steps), **sc, "ms": ms,
+        variants.append({"pool": name, "kinds": list(keep), "adam_steps": int(steps),
+                         "loss": "decoded (after residual grid)" if residual else "primitives only", **sc, "ms": ms,
                          "mpix_per_s": n_px / (ms * 1e-3) / 1e6, "rd_delta_db": sc["rd_score"] - plain["rd_score"]})
         del rf, fast
     return {"plain": {**plain, "prims": sum(len(s) for s in plain_stacks)}, "lr": args.refine_lr,
@@ -361,8 +363,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--decode-iters", type=int, default=10)
-    ap.add_argument("--refine-variants", default="nocurve:20,smooth:20,constlin:20,constlin:0",
-                    help="refined fits to compare, pool:adam_steps (empty: skip)")
+    ap.add_argument("--refine-variants", default="constlin:0,constlin:20,constlin:20:r,nocurve:20:r",
+                    help="refined fits to compare, pool:adam_steps[:r] (r: decoded-error loss; empty: skip)")
     ap.add_argument("--refine-reps", type=int, default=5)
     ap.add_argument("--refine-lr", type=float, default=1e-2)
     args = ap.parse_args()

@@ -29,6 +29,11 @@ extern "C" {
 #endif
 
 #define WEFTK_SOFT_TRIANGLES 2
+/* Loss of the decoded tile: the error left after the decoder adds back the 4x4
+ * grid of block-mean errors with bilinear interpolation (the tile's RES1 map,
+ * src/weft/encoder.py:3248-3372, src/weft/render.py:474-515), ignoring the grid's
+ * 8-bit quantisation.  Tile sides must be 8, 16, 32 or 64. */
+#define WEFTK_LOSS_RESIDUAL 4
 #define WEFTK_REFINE_MAX_PRIMS 32 /* longest stack the refine kernels accept */
 
 typedef struct WeftStackSet {
@@ -39,6 +44,15 @@ typedef struct WeftStackSet {
     const int32_t* size;      /* [n_tiles] tile side (1..64) */
     const int32_t* prim_off;  /* [n_tiles + 1] tile t owns parameter rows [prim_off[t], prim_off[t+1]) */
     const int32_t* kind;      /* [n_prims] primitive kind of each row */
+    /* Optional work split by tile side (NULL: four warps per tile): a permutation
+     * of the tiles listing n_big tiles of side > 32 (eight warps each), then n_mid
+     * of side 17..32 (four warps), then n_s16 of side 9..16 (two warps), then the
+     * rest (one warp).  The split only affects speed; any valid split gives the
+     * same results. */
+    const int32_t* order;
+    int32_t n_big;
+    int32_t n_mid;
+    int32_t n_s16;
 } WeftStackSet;
 
 /* loss[t] for every tile (float32). */
@@ -58,6 +72,15 @@ int weftk_stack_loss_backward(const WeftStackSet* set, const float* d_params, co
  * captured sequence of calls replays correctly. */
 int weftk_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, const int32_t* d_kind,
                     int n_rows, float lr, float beta1, float beta2, float eps, int32_t* d_step, void* stream);
+
+/* One refinement step in one launch: the loss and gradient of every tile (as
+ * weftk_stack_loss_backward) followed, inside the same tile group, by the Adam
+ * step and projection of weftk_adam_step on the tile's own rows.  d_params is
+ * updated in place.  Each row's step count is kept in d_m[row * 16 + 15] (zero
+ * it with the moments to restart).  d_loss and d_grad_params may be NULL. */
+int weftk_refine_step(const WeftStackSet* set, float* d_params, float* d_m, float* d_v, const float* d_grad_loss,
+                      float* d_loss, float* d_grad_params, float lr, float beta1, float beta2, float eps, int flags,
+                      void* stream);
 
 #ifdef __cplusplus
 }

@@ -28,26 +28,28 @@ def _fit(kinds_out=()):
     return BatchedFit(patches, pools, 75, caps=[16] * len(qts))
 
 
-def test_backward_loss_output_equals_forward():
+@pytest.mark.parametrize("residual", [False, True])
+def test_backward_loss_output_equals_forward(residual):
     from weft_b200.refine import FusedRefiner
 
     fit = _fit().run()
     ss, params = fit.stack_set()
-    fr = FusedRefiner(ss, params)
-    want = ss.loss(fr.p).cpu().numpy()
+    fr = FusedRefiner(ss, params, residual=residual)
+    want = ss.loss(fr.p, residual=residual).cpu().numpy()
     fr.step()
     got = fr.loss.cpu().numpy()
     np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-9)
 
 
-def test_fused_refiner_matches_torch_adam():
+@pytest.mark.parametrize("residual", [False, True])
+def test_fused_refiner_matches_torch_adam(residual):
     from weft_b200.refine import FusedRefiner, refine
 
     fit = _fit().run()
     ss, params = fit.stack_set()
     steps = 15
-    want, hist = refine(ss, params, steps=steps, lr=1e-2)
-    fr = FusedRefiner(ss, params, lr=1e-2)
+    want, hist = refine(ss, params, steps=steps, lr=1e-2, residual=residual)
+    fr = FusedRefiner(ss, params, lr=1e-2, residual=residual)
     losses = []
     for _ in range(steps):
         fr.step()
@@ -57,15 +59,15 @@ def test_fused_refiner_matches_torch_adam():
     # versus double on the host, so trajectories agree to rounding, not bit for bit.
     assert float((got[:, :14] - want[:, :14]).abs().max()) < 2e-3
     np.testing.assert_allclose(losses, hist, rtol=1e-4)
-    assert int(fr.step_ctr.item()) == steps
+    assert float(fr.m[:, 15].min()) == steps and float(fr.m[:, 15].max()) == steps  # per-row step counts
 
 
-@pytest.mark.parametrize("use_graph", [False, True])
-def test_refined_fit_matches_unfused_pipeline(use_graph):
+@pytest.mark.parametrize("use_graph,residual", [(False, False), (True, False), (True, True)])
+def test_refined_fit_matches_unfused_pipeline(use_graph, residual):
     from weft_b200.refine import FusedRefiner, RefinedFit
 
     fit = _fit(kinds_out=(3,))
-    rf = RefinedFit(fit, steps=10, lr=1e-2, use_graph=use_graph)
+    rf = RefinedFit(fit, steps=10, lr=1e-2, use_graph=use_graph, residual=residual)
     got = rf.run().clone()
     got2 = rf.run().clone()  # replays start from the same state
     assert torch.equal(got, got2)
@@ -75,6 +77,23 @@ def test_refined_fit_matches_unfused_pipeline(use_graph):
     ss, params = fit.stack_set()
     assert np.array_equal(ss.prim_off_np, rf.ss.prim_off_np)
     assert torch.equal(ss.t_kind, rf.kinds)
-    fr = FusedRefiner(ss, params, lr=1e-2)
+    fr = FusedRefiner(ss, params, lr=1e-2, residual=residual)
     fr.run(10)
     assert torch.equal(fr.p[:, :14], got[:, :14])
+
+
+@pytest.mark.parametrize("residual", [False, True])
+def test_single_launch_step_equals_two_launch_step(residual):
+    from weft_b200.refine import FusedRefiner
+
+    fit = _fit().run()
+    ss, params = fit.stack_set()
+    one = FusedRefiner(ss, params, lr=1e-2, residual=residual, single_launch=True)
+    two = FusedRefiner(ss, params, lr=1e-2, residual=residual, single_launch=False)
+    for _ in range(8):
+        one.step()
+        two.step()
+        assert torch.equal(one.loss, two.loss)
+    assert torch.equal(one.p[:, :14], two.p[:, :14])
+    assert torch.equal(one.m[:, :14], two.m[:, :14]) and torch.equal(one.v[:, :14], two.v[:, :14])
+    assert float(one.m[:, 15].min()) == 8.0 and float(one.m[:, 15].max()) == 8.0

@@ -7,6 +7,8 @@ backward's surrogate differentiates.
 
 from __future__ import annotations
 
+import functools
+
 import numpy as np
 import pytest
 import torch
@@ -31,9 +33,9 @@ def _rand_stack(rng, ts, n):
     return out
 
 
-def _workload(seed=1234, n_tiles=64):
+def _workload(seed=1234, n_tiles=64, sizes=(8, 16, 32)):
     rng = np.random.default_rng(seed)
-    sizes = rng.choice([8, 16, 32], n_tiles)
+    sizes = rng.choice(list(sizes), n_tiles)
     patches = [rng.random((int(s), int(s), 3), dtype=np.float32) for s in sizes]
     stacks = [_rand_stack(rng, int(s), int(rng.integers(1, 5))) for s in sizes]
     return patches, stacks
@@ -46,8 +48,32 @@ def _seg_d2(px, py, ax, ay, bx, by):
     return ex * ex + ey * ey
 
 
-def ref_tile_loss(rows, kinds, src, soft):
-    """Float64 restatement of the renderer + tile MSE, differentiable by torch."""
+@functools.lru_cache(maxsize=None)
+def residual_operator(ts):
+    """Dense float64 (n, n) matrix I - B M: M = 4x4 block means, B = the decoder's bilinear
+    upsampling of the 4x4 grid at pixel centres with edge clamping."""
+    n = ts * ts
+    b = ts // 4
+    M = np.zeros((16, n))
+    B = np.zeros((n, 16))
+    for y in range(ts):
+        for x in range(ts):
+            p = y * ts + x
+            M[(y // b) * 4 + x // b, p] = 1.0 / (b * b)
+            gx = min(max((x + 0.5) * 4.0 / ts - 0.5, 0.0), 3.0)
+            gy = min(max((y + 0.5) * 4.0 / ts - 0.5, 0.0), 3.0)
+            x0, y0 = int(np.floor(gx)), int(np.floor(gy))
+            x1, y1 = min(x0 + 1, 3), min(y0 + 1, 3)
+            wx, wy = gx - x0, gy - y0
+            for nx, ny, w in ((x0, y0, (1 - wx) * (1 - wy)), (x1, y0, wx * (1 - wy)), (x0, y1, (1 - wx) * wy),
+                              (x1, y1, wx * wy)):
+                B[p, ny * 4 + nx] += w
+    return torch.from_numpy(np.eye(n) - B @ M)
+
+
+def ref_tile_loss(rows, kinds, src, soft, residual=False):
+    """Float64 restatement of the renderer + tile MSE, differentiable by torch.  With
+    ``residual`` the error is first passed through I - B M (the decoded residual grid)."""
     ts = src.shape[0]
     base = torch.arange(ts, dtype=F64) + 0.5
     py, px = torch.meshgrid(base, base, indexing="ij")
@@ -88,7 +114,10 @@ def ref_tile_loss(rows, kinds, src, soft):
             assert soft
         a = (A * cov)[..., None]
         c = s * a + c * (1 - a)
-    return ((c.clamp(0.0, 1.0) - torch.from_numpy(src).to(F64)) ** 2).mean()
+    e = c.clamp(0.0, 1.0) - torch.from_numpy(src).to(F64)
+    if residual:
+        e = (residual_operator(ts) @ e.reshape(-1, 3)).reshape(ts, ts, 3)
+    return (e ** 2).mean()
 
 
 def _split(stacks):
@@ -98,11 +127,11 @@ def _split(stacks):
     return smooth, tri
 
 
-@pytest.mark.parametrize("soft", [False, True])
-def test_backward_matches_float64_autograd(soft):
+@pytest.mark.parametrize("soft,residual", [(False, False), (True, False), (False, True), (True, True)])
+def test_backward_matches_float64_autograd(soft, residual):
     from weft_b200.refine import StackSet
 
-    patches, stacks = _workload()
+    patches, stacks = _workload(sizes=(8, 16, 32, 64) if residual else (8, 16, 32))
     stacks = [[p for p in s if (p.kind == 4) == soft] for s in stacks]
     keep = [i for i, s in enumerate(stacks) if s]
     patches = [patches[i] for i in keep]
@@ -110,26 +139,28 @@ def test_backward_matches_float64_autograd(soft):
     assert len(stacks) >= 20
     ss, params = StackSet.from_stacks(patches, stacks)
     g = torch.rand(ss.n, device=params.device) + 0.5
-    got = ss.loss_backward(params, g, soft=soft).cpu().numpy()
+    got = ss.loss_backward(params, g, soft=soft, residual=residual).cpu().numpy()
     rows = params.cpu().numpy().astype(np.float64)
     off = ss.prim_off_np
     worst = 0.0
     for t in range(ss.n):
         r = torch.tensor(rows[off[t]:off[t + 1]], dtype=F64, requires_grad=True)
-        L = ref_tile_loss(list(r), [p.kind for p in stacks[t]], patches[t], soft) * float(g[t])
+        L = ref_tile_loss(list(r), [p.kind for p in stacks[t]], patches[t], soft, residual) * float(g[t])
         L.backward()
         want = r.grad.numpy()[:, :14]
         have = got[off[t]:off[t + 1], :14]
-        scale = np.abs(want).max() + 1e-12
+        # absolute floor: under the residual loss a lone constant layer's gradient is
+        # zero up to rounding (the residual grid absorbs any constant shift)
+        scale = max(np.abs(want).max(), 1e-5)
         err = np.abs(have - want).max() / scale
         worst = max(worst, err)
         assert err < 2e-3, f"tile {t} kinds {[p.kind for p in stacks[t]]}: rel err {err}"
     # loss values agree too
-    loss = ss.loss(params, soft=soft).cpu().numpy()
+    loss = ss.loss(params, soft=soft, residual=residual).cpu().numpy()
     for t in range(0, ss.n, 5):
         r = torch.tensor(rows[off[t]:off[t + 1]], dtype=F64)
-        assert loss[t] == pytest.approx(float(ref_tile_loss(list(r), [p.kind for p in stacks[t]], patches[t], soft)),
-                                        rel=2e-5)
+        want = float(ref_tile_loss(list(r), [p.kind for p in stacks[t]], patches[t], soft, residual))
+        assert loss[t] == pytest.approx(want, rel=2e-5 if not residual else 1e-4)
 
 
 @pytest.mark.parametrize("soft", [False, True])

@@ -48,7 +48,8 @@ class WeftFitState(ctypes.Structure):
 class WeftStackSet(ctypes.Structure):
     """Device pointers of a set of per-tile stacks (include/weftk_refine.h)."""
     _fields_ = [("n_tiles", ctypes.c_int32), ("max_prims", ctypes.c_int32)] + [
-        (n, ctypes.c_void_p) for n in ("src", "px_off", "size", "prim_off", "kind")]
+        (n, ctypes.c_void_p) for n in ("src", "px_off", "size", "prim_off", "kind", "order")] + [
+        ("n_big", ctypes.c_int32), ("n_mid", ctypes.c_int32), ("n_s16", ctypes.c_int32)]
 
 
 # numpy mirrors of the C structs (same byte layout)
@@ -89,6 +90,8 @@ SIGNATURES: dict[str, list] = {
     "weftk_stack_loss_backward": [_P, _P, _P, _P, _P, _I, _P],
     "weftk_adam_step": [_P, _P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P,
                         _P],
+    "weftk_refine_step": [_P, _P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                          ctypes.c_float, _I, _P],
     "weftk_measure_fp32_peak": [_P],
 }
 

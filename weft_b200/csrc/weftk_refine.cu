@@ -1,17 +1,35 @@
 // weftk_refine.cu — per-tile stack loss and its hand-written backward (see include/weftk_refine.h).
 //
-// One CTA per tile; the tile's parameter rows are prepared once into shared
-// memory (and a curve's 31 polyline segments into a segment table).  Each
-// thread owns one pixel of a chunk.  The backward re-renders the chunk's pixels
+// One launch covers every tile.  Tiles are grouped by side so that each warp
+// has at most 16 chunks of 32 pixels: a tile of side > 32 gets eight warps,
+// 17..32 four, 9..16 two, <= 8 one; every CTA has eight warps and holds one or
+// more such tile groups, and CTAs of the largest tiles come first so they start
+// first.  Each warp of a tile owns a contiguous range of chunks and prefetches
+// the next chunk's source pixels while it works on the current one.  The tile's
+// parameter rows are prepared once into shared memory (and a curve's 31
+// polyline segments into a segment table).  The backward re-renders a chunk
 // front to back, keeping the composite *before* every layer in shared memory
-// (layers x threads x 3 floats, the only per-pixel state, never written to HBM),
-// then sweeps the layers back to front:
+// (layers x 32 lanes x 3 floats per warp, the only per-pixel state, never
+// written to HBM), then sweeps the layers back to front:
 //     c_k = s_k a_k + c_{k-1} (1 - a_k)
 //     dL/ds_k = g a_k,  dL/da_k = g . (s_k - c_{k-1}),  g <- g (1 - a_k)
 // and chains dL/ds, dL/da into the layer's parameters with the coverage
-// recomputed at that pixel.  Per-layer gradients are reduced over the CTA in a
-// fixed order, so results are deterministic.
+// recomputed at that pixel.  Every sum (gradients over pixels, block and
+// quadrant sums of the residual loss) has a single owner and a fixed order, so
+// results are deterministic.
+//
+// Residual-aware loss (WEFTK_LOSS_RESIDUAL): the file a fit becomes carries a
+// per-tile 4x4 grid of block-mean errors that the decoder adds back with
+// bilinear interpolation (src/weft/encoder.py:3248-3372, src/weft/render.py:474-515).
+// With e = clamp(render) - src, M the 4x4 block-mean operator and B the decoder's
+// bilinear upsampling, the decoded error is r = e - B M e (before the grid's
+// 8-bit quantisation and clamping), and the loss is mean(r^2) with gradient
+// 2 (I - M^T B^T) r / (3n).  Pixels are visited block-major, quadrant-major
+// inside a block, so block sums and the per-quadrant sums of B^T r are
+// segmented warp reductions over aligned lane groups.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "../../include/weftk_refine.h"
 #include "weftk_common.cuh"
@@ -21,18 +39,14 @@ namespace weftk {
 
 extern __device__ int g_device_status;
 
-constexpr int RF_THREADS = 128;
-constexpr int RF_WARPS = RF_THREADS / 32;
 constexpr int MAXL = WEFTK_REFINE_MAX_PRIMS;
 constexpr float TRI_SOFT_W = 0.5f;  // surrogate edge width in pixels
 
-struct RfShared {
-    Prep prep[MAXL];
-    float raw[MAXL][16];
-    float4 seg[MAXL][31][2];
-    float red[RF_WARPS][14];
-    float gacc[MAXL][14];
-    double lred[RF_WARPS];
+// The layers of one tile, staged in shared memory.
+struct Layers {
+    const Prep* prep;
+    const float (*raw)[16];
+    const float4 (*seg)[31][2];
 };
 
 __device__ __forceinline__ WeftPrim row_to_prim(const float* r, int kind) {
@@ -47,33 +61,6 @@ __device__ __forceinline__ WeftPrim row_to_prim(const float* r, int kind) {
     }
     p.alpha = r[13];
     return p;
-}
-
-// Stage the tile's rows: raw parameters, prepared terms, curve segment tables.
-__device__ bool stage_tile(const WeftStackSet& set, const float* params, int t, RfShared& s, int& K) {
-    const int p0 = set.prim_off[t];
-    K = set.prim_off[t + 1] - p0;
-    if (K < 0 || K > MAXL) return false;
-    for (int i = threadIdx.x; i < K * 16; i += blockDim.x) s.raw[i / 16][i % 16] = params[(size_t)p0 * 16 + i];
-    __syncthreads();
-    if ((int)threadIdx.x < K) {
-        const int k = threadIdx.x;
-        Prep P = prep_prim(row_to_prim(s.raw[k], set.kind[p0 + k]));
-        if (P.kind == K_BICUBIC) P.kind = K_SKIP;
-        s.prep[k] = P;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < K * 31; i += blockDim.x) {
-        const int k = i / 31, j = i % 31;
-        if (s.prep[k].kind == K_CURVE) {
-            const Seg g = lane_segment(s.prep[k], j);
-            s.seg[k][j][0] = make_float4(g.ax, g.ay, g.vx, g.vy);
-            s.seg[k][j][1] = make_float4(g.ux, g.uy, 0.0f, 0.0f);
-        }
-    }
-    for (int i = threadIdx.x; i < K * 14; i += blockDim.x) s.gacc[i / 14][i % 14] = 0.0f;
-    __syncthreads();
-    return true;
 }
 
 __device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + __expf(-x)); }
@@ -120,7 +107,7 @@ __device__ float tri_soft(const float* g, float px, float py, float* grad) {
 }
 
 // Source colour and alpha of layer k at one pixel (the renderer's formulas).
-__device__ __forceinline__ void layer_eval(const RfShared& s, int k, float px, float py, bool soft, float (&src)[3],
+__device__ __forceinline__ void layer_eval(const Layers& s, int k, float px, float py, bool soft, float (&src)[3],
                                            float& a) {
     const Prep& P = s.prep[k];
     float fx[1] = {px}, fy[1] = {py}, av[1], sr[1], sg[1], sb[1];
@@ -144,7 +131,7 @@ __device__ __forceinline__ void layer_eval(const RfShared& s, int k, float px, f
 }
 
 // Gradient contribution of layer k at one pixel.  g = dL/dc_k, cp = c_{k-1}.
-__device__ void layer_grad(const RfShared& s, int k, float px, float py, bool soft, const float (&g)[3],
+__device__ void layer_grad(const Layers& s, int k, float px, float py, bool soft, const float (&g)[3],
                            const float (&cp)[3], float& a_out, float (&d)[14]) {
     const Prep& P = s.prep[k];
     const float* r = s.raw[k];
@@ -266,130 +253,514 @@ __device__ void layer_grad(const RfShared& s, int k, float px, float py, bool so
     }
 }
 
-__global__ void __launch_bounds__(RF_THREADS) stack_loss_kernel(WeftStackSet set, const float* __restrict__ params,
-                                                                float* __restrict__ loss, int flags) {
-    __shared__ RfShared s;
-    const int t = blockIdx.x;
-    int K = 0;
-    const int ts = set.size[t];
-    if (ts <= 0 || ts > 64 || !stage_tile(set, params, t, s, K)) {
-        if (threadIdx.x == 0) {
-            atomicCAS(&g_device_status, 0, WEFTK_E_ARG);
-            loss[t] = __int_as_float(0x7fc00000);
-        }
-        return;
-    }
-    const bool soft = flags & WEFTK_SOFT_TRIANGLES;
-    const float4* src = reinterpret_cast<const float4*>(set.src) + set.px_off[t];
-    const int n = ts * ts;
-    double acc = 0.0;
-    for (int p = threadIdx.x; p < n; p += RF_THREADS) {
-        const float px = (float)(p % ts) + 0.5f, py = (float)(p / ts) + 0.5f;
-        float c[3] = {0.0f, 0.0f, 0.0f};
-        for (int k = 0; k < K; ++k) {
-            float sv[3], a;
-            layer_eval(s, k, px, py, soft, sv, a);
-#pragma unroll
-            for (int ch = 0; ch < 3; ++ch) c[ch] = blend(sv[ch], a, c[ch]);
-        }
-        const float4 v = src[p];
-        const float dr = clamp01(c[0]) - v.x, dg = clamp01(c[1]) - v.y, db = clamp01(c[2]) - v.z;
-        acc += (double)fmaf(dr, dr, fmaf(dg, dg, db * db));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
-    if ((threadIdx.x & 31) == 0) s.lred[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int w = 0; w < RF_WARPS; ++w) tot += s.lred[w];
-        loss[t] = (float)(tot / (3.0 * n));
+// Shared-memory carve-up of one tile group (the WPT warps working on one tile).
+// Byte offsets for L staged layers; every region starts on a 16-byte boundary
+// except the trailing doubles (8-byte aligned).
+struct GroupLayout {
+    int prep, seg, raw, msum, quad, hnode, hist, gacc, lacc, lred, bytes;
+};
+
+// Stacks of at most this many layers accumulate gradients per lane (one slot per
+// lane, column and layer) and reduce once per tile; longer stacks reduce every chunk.
+constexpr int RF_LANE_ACC_MAX = 2;
+
+// msum/quad/hnode exist only for the residual loss, lacc only for short stacks.
+__host__ __device__ __forceinline__ GroupLayout group_layout(int L, int wpt, bool resid) {
+    GroupLayout g;
+    g.prep = 0;
+    g.seg = g.prep + L * 64;
+    g.raw = g.seg + L * 992;
+    g.msum = g.raw + L * 64;
+    g.quad = g.msum + (resid ? 48 * 4 : 0);
+    g.hnode = g.quad + (resid ? 768 * 4 : 0);
+    g.hist = g.hnode + (resid ? 48 * 4 : 0);
+    g.gacc = g.hist + wpt * L * 384;
+    g.lacc = (g.gacc + wpt * L * 56 + 15) & ~15;
+    g.lred = g.lacc + (L <= RF_LANE_ACC_MAX ? wpt * L * 14 * 32 * 4 : 0);
+    g.bytes = (g.lred + wpt * 8 + 15) & ~15;
+    return g;
+}
+
+// Adam (PyTorch's update rule, FP32) for one value at step t (1-based), then the
+// projection onto what the wire format carries: colours and alpha in [0, 1],
+// coordinates in [0, 15], thickness in [0, 4] (src/weft/primitives.py:102-177).
+__device__ __forceinline__ float adam_update(float p, float g, float& m, float& v, float t, float lr, float b1,
+                                             float b2, float eps, int kind, int col) {
+    m = fmaf(b1, m, (1.0f - b1) * g);
+    v = fmaf(b2, v, (1.0f - b2) * g * g);
+    const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
+    float x = p - lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+    if (col >= 7) return fminf(fmaxf(x, 0.0f), 1.0f);
+    const bool thick = (kind == K_LINE && col == 4) || (kind == K_CURVE && col == 6);
+    return fminf(fmaxf(x, 0.0f), thick ? 4.0f : 15.0f);
+}
+
+// Optimiser state of the fused refine step; the per-row step count lives in m[row * 16 + 15].
+struct AdamArgs {
+    float* m;
+    float* v;
+    float lr, b1, b2, eps;
+};
+
+// CTA classes of one launch, in launch order: tiles of side > 32 (8 warps per
+// tile), 17..32 (4 warps), 9..16 (2 warps), <= 8 (1 warp).  Every CTA has 8
+// warps; a CTA of class c holds groups[c] tiles.
+constexpr int RF_THREADS = 256;
+constexpr int RF_CLASSES = 4;
+constexpr int RF_SMEM_MAX = 227 * 1024;
+
+struct RefinePlan {
+    int cta_end[RF_CLASSES];  // exclusive prefix sums of the classes' CTA counts
+    int list_off[RF_CLASSES];
+    int n_list[RF_CLASSES];
+    int groups[RF_CLASSES];
+};
+
+__host__ __device__ __forceinline__ int class_wpt(int c) { return 8 >> c; }
+
+// a[c] without dynamic indexing (keeps the plan in registers, off the stack)
+__device__ __forceinline__ int pick(const int (&a)[RF_CLASSES], int c) {
+    return c == 0 ? a[0] : c == 1 ? a[1] : c == 2 ? a[2] : a[3];
+}
+
+// Gradient columns a layer of this kind can produce (bit i = column i).
+__device__ __forceinline__ unsigned grad_columns(int kind) {
+    switch (kind) {
+        case K_CONST: return 0x2380u;   // 7 8 9 13
+        case K_LINEAR: return 0x3f8fu;  // 0-3 7-13
+        case K_LINE: return 0x239fu;    // 0-4 7 8 9 13
+        case K_CURVE: return 0x23ffu;   // 0-6 7 8 9 13
+        case K_TRI: return 0x23bfu;     // 0-5 7 8 9 13
+        default: return 0u;
     }
 }
 
-__global__ void __launch_bounds__(RF_THREADS) stack_backward_kernel(WeftStackSet set, const float* __restrict__ params,
-                                                                    const float* __restrict__ grad_loss,
-                                                                    float* __restrict__ grad, float* __restrict__ loss,
-                                                                    int flags) {
-    extern __shared__ float hist[];  // [K][RF_THREADS][3]: composite before each layer
-    __shared__ RfShared s;
-    const int t = blockIdx.x;
-    int K = 0;
+// Bilinear node pair (lo, hi) and weight of the decoder's 4x4 residual grid for a
+// pixel index along one axis of a tile with gscale = 4 / side (src/weft/render.py:474-515:
+// centre sampling, edge clamp).
+__device__ __forceinline__ void grid_coord(int p, float gscale, int& lo, int& hi, float& w) {
+    const float g = fminf(fmaxf(__fsub_rn(__fmul_rn((float)p + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+    lo = (int)floorf(g);
+    hi = min(lo + 1, 3);
+    w = g - (float)lo;
+}
+
+// Quadrant columns (0..7: block q / 2, half q % 2) whose pixels interpolate from grid
+// node n along one axis, with the slot (0: lower node, 1: upper node) they use.  Lower
+// node n: the right half of block n, the left half of block n + 1, and for n = 0 the left
+// half of block 0 (clamped).  Upper node n: the right half of block n - 1, the left half
+// of block n (n >= 1), and for n = 3 the right half of block 3 (clamped, weight 0).  The
+// left half of block 0 also names node 1 as its upper node, with weight 0; it is skipped.
+// Returns the count (<= 4); entries are (column << 1) | slot.
+__device__ __forceinline__ int node_sources(int n, int (&out)[4]) {
+    int c = 0;
+    if (n == 0) out[c++] = (0 << 1) | 0;
+    if (2 * n + 1 <= 7) out[c++] = ((2 * n + 1) << 1) | 0;
+    if (2 * n + 2 <= 7) out[c++] = ((2 * n + 2) << 1) | 0;
+    if (n >= 1) out[c++] = ((2 * n - 1) << 1) | 1;
+    if (n >= 1) out[c++] = ((2 * n) << 1) | 1;
+    if (n == 3) out[c++] = (7 << 1) | 1;
+    return c;
+}
+
+// Barrier over the warps of one tile group (named barrier 1 + group; one warp: __syncwarp).
+__device__ __forceinline__ void group_sync(int wpt, int grp) {
+    if (wpt == 1)
+        __syncwarp();
+    else
+        asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(wpt * 32) : "memory");
+}
+
+// One kernel for the loss (MODE 0), loss + gradient (MODE 1), and loss + gradient +
+// Adam step on the tile's own rows (MODE 2: params are updated in place; a group reads
+// its rows once at staging and writes them once at the end, and rows belong to one tile).
+constexpr int RF_LOSS = 0, RF_GRAD = 1, RF_STEP = 2;
+
+template <int MODE>
+__global__ void __launch_bounds__(RF_THREADS, 3)
+    refine_tiles_kernel(WeftStackSet set, float* __restrict__ params, const float* __restrict__ grad_loss,
+                        float* __restrict__ grad, float* __restrict__ loss, int flags, RefinePlan plan, int L,
+                        AdamArgs adam) {
+    constexpr bool BWD = MODE != RF_LOSS;
+    extern __shared__ __align__(16) unsigned char rf_smem[];
+    const int bx = blockIdx.x;
+    const int cls = (bx >= plan.cta_end[0]) + (bx >= plan.cta_end[1]) + (bx >= plan.cta_end[2]);
+    const int cta0 = cls ? pick(plan.cta_end, cls - 1) : 0;
+    const int wpt = class_wpt(cls), G = pick(plan.groups, cls);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = warp / wpt, wig = warp - grp * wpt;  // group, warp inside the group
+    if (grp >= G) return;
+    const int li = ((int)blockIdx.x - cta0) * G + grp;
+    if (li >= pick(plan.n_list, cls)) return;  // uniform over the group
+    const int lo = pick(plan.list_off, cls);
+    const int t = set.order ? set.order[lo + li] : lo + li;
+    const bool resid = flags & WEFTK_LOSS_RESIDUAL;
+    const bool soft = flags & WEFTK_SOFT_TRIANGLES;
+    const bool lane_acc = L <= RF_LANE_ACC_MAX;
+    const GroupLayout lay = group_layout(L, wpt, resid);
+    unsigned char* base = rf_smem + (size_t)grp * lay.bytes;
+    Prep* prep = reinterpret_cast<Prep*>(base + lay.prep);
+    float4(*seg)[31][2] = reinterpret_cast<float4(*)[31][2]>(base + lay.seg);
+    float(*raw)[16] = reinterpret_cast<float(*)[16]>(base + lay.raw);
+    float* msum = reinterpret_cast<float*>(base + lay.msum);
+    float* quad = reinterpret_cast<float*>(base + lay.quad);
+    float* hnode = reinterpret_cast<float*>(base + lay.hnode);
+    float* hist = reinterpret_cast<float*>(base + lay.hist) + (size_t)wig * L * 96;
+    float* gacc_all = reinterpret_cast<float*>(base + lay.gacc);
+    float* gacc = gacc_all + (size_t)wig * L * 14;
+    float* lacc = reinterpret_cast<float*>(base + lay.lacc) + (size_t)wig * L * 14 * 32;
+    double* lred = reinterpret_cast<double*>(base + lay.lred);
+
     const int ts = set.size[t];
-    if (ts <= 0 || ts > 64 || !stage_tile(set, params, t, s, K)) {
-        if (threadIdx.x == 0) atomicCAS(&g_device_status, 0, WEFTK_E_ARG);
+    const int p0 = set.prim_off[t];
+    const int K = set.prim_off[t + 1] - p0;
+    bool ok = ts >= 1 && ts <= 64 && K >= 0 && K <= L;
+    if (resid) ok = ok && (ts == 8 || ts == 16 || ts == 32 || ts == 64);
+    if (!ok) {
+        if (wig == 0 && lane == 0) {
+            atomicCAS(&g_device_status, 0, WEFTK_E_ARG);
+            if (loss) loss[t] = __int_as_float(0x7fc00000);
+        }
         return;
     }
-    const bool soft = flags & WEFTK_SOFT_TRIANGLES;
+    const int gt = wig * 32 + lane, GT = wpt * 32;
+
+    // ---- stage the layers
+    for (int i = gt; i < K * 16; i += GT) raw[i >> 4][i & 15] = params[(size_t)p0 * 16 + i];
+    group_sync(wpt, grp);
+    for (int k = gt; k < K; k += GT) {
+        Prep P = prep_prim(row_to_prim(raw[k], set.kind[p0 + k]));
+        if (P.kind == K_BICUBIC) P.kind = K_SKIP;
+        prep[k] = P;
+    }
+    group_sync(wpt, grp);
+    for (int i = gt; i < K * 31; i += GT) {
+        const int k = i / 31, j = i - k * 31;
+        if (prep[k].kind == K_CURVE) {
+            const Seg g = lane_segment(prep[k], j);
+            seg[k][j][0] = make_float4(g.ax, g.ay, g.vx, g.vy);
+            seg[k][j][1] = make_float4(g.ux, g.uy, 0.0f, 0.0f);
+        }
+    }
+    if (BWD) {
+        for (int i = lane; i < K * 14; i += 32) gacc[i] = 0.0f;
+        if (lane_acc)
+            for (int i = lane; i < K * 14 * 32; i += 32) lacc[i] = 0.0f;
+    }
+    if (resid)
+        for (int i = gt; i < 48 + 768; i += GT) {
+            if (i < 48)
+                msum[i] = 0.0f;
+            else
+                quad[i - 48] = 0.0f;
+        }
+    group_sync(wpt, grp);
+    const Layers S{prep, raw, seg};
+
     const float4* src = reinterpret_cast<const float4*>(set.src) + set.px_off[t];
-    const int n = ts * ts, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float scale = grad_loss[t] * 2.0f / (3.0f * (float)n);
-    double sse = 0.0;
-    for (int base = 0; base < n; base += RF_THREADS) {
-        const int p = base + tid;
-        const bool valid = p < n;
-        const float px = (float)(p % ts) + 0.5f, py = (float)(p / ts) + 0.5f;
-        float c[3] = {0.0f, 0.0f, 0.0f};
+    const int n = ts * ts;
+    const int chunks = (n + 31) >> 5;
+    const int c_begin = (chunks * wig) / wpt, c_end = (chunks * (wig + 1)) / wpt;
+    // Residual-mode geometry (side a power of two >= 8): block side b, block pixels bb,
+    // quadrant side h = b / 2, quadrant pixels Q = bb / 4.
+    const int lb = resid ? (__ffs(ts) - 1) - 2 : 0;  // log2(b)
+    const int b = 1 << lb, lbb = 2 * lb, bb = 1 << lbb;
+    const int lq = resid ? lbb - 2 : 0, Q = 1 << lq, lh = resid ? lb - 1 : 0, h = 1 << lh;
+    const float gscale = resid ? 4.0f / (float)ts : 0.0f;
+    const float inv_bb = resid ? 1.0f / (float)bb : 0.0f;
+    const int lts = (ts & (ts - 1)) == 0 ? __ffs(ts) - 1 : -1;  // log2(side) for power-of-two sides
+
+    // pixel (x, y) of visit index q: row-major, or block-major / quadrant-major in residual mode
+    auto pixel_of = [&](int q, int& x, int& y) {
+        if (resid) {
+            const int j = q >> lbb, o = q & (bb - 1), qd = o >> lq, u = o & (Q - 1);
+            x = (j & 3) * b + (qd & 1) * h + (u & (h - 1));
+            y = (j >> 2) * b + (qd >> 1) * h + (u >> lh);
+        } else if (lts >= 0) {
+            y = q >> lts;
+            x = q & (ts - 1);
+        } else {
+            y = q / ts;
+            x = q - y * ts;
+        }
+    };
+    auto load_src = [&](int q) -> float4 {
+        if (q >= n) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        int x, y;
+        pixel_of(q, x, y);
+        return src[y * ts + x];
+    };
+    auto composite = [&](float px, float py, float (&c)[3], float* hrow) {
+        c[0] = c[1] = c[2] = 0.0f;
         for (int k = 0; k < K; ++k) {
-            float* h = hist + ((size_t)k * RF_THREADS + tid) * 3;
-            h[0] = c[0];
-            h[1] = c[1];
-            h[2] = c[2];
+            if (hrow) {
+                float* hh = hrow + ((size_t)k * 32 + lane) * 3;
+                hh[0] = c[0];
+                hh[1] = c[1];
+                hh[2] = c[2];
+            }
             float sv[3], a;
-            layer_eval(s, k, px, py, soft, sv, a);
+            layer_eval(S, k, px, py, soft, sv, a);
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) c[ch] = blend(sv[ch], a, c[ch]);
         }
-        float g[3] = {0.0f, 0.0f, 0.0f};
-        if (valid) {
-            const float4 v = src[p];
-            const float sv[3] = {v.x, v.y, v.z};
+    };
+    // decoded-error correction B M e at a pixel (block means in msum, already divided)
+    auto correction = [&](int x, int y, float (&v)[3]) {
+        int x0, x1, y0, y1;
+        float wx, wy;
+        grid_coord(x, gscale, x0, x1, wx);
+        grid_coord(y, gscale, y0, y1, wy);
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) {
-                const float e = clamp01(c[ch]) - sv[ch];
-                sse += (double)(e * e);
-                g[ch] = (c[ch] >= 0.0f && c[ch] <= 1.0f) ? scale * e : 0.0f;
+        for (int ch = 0; ch < 3; ++ch) {
+            const float c00 = msum[(y0 * 4 + x0) * 3 + ch], c01 = msum[(y0 * 4 + x1) * 3 + ch];
+            const float c10 = msum[(y1 * 4 + x0) * 3 + ch], c11 = msum[(y1 * 4 + x1) * 3 + ch];
+            const float top = fmaf(c01 - c00, wx, c00), bot = fmaf(c11 - c10, wx, c10);
+            v[ch] = fmaf(bot - top, wy, top);
+        }
+    };
+
+    double sse = 0.0;
+    if (resid) {
+        // ---- pass 1: block sums of e (segments of bb visits; one owner per block)
+        float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int cidx = c_begin; cidx < c_end; ++cidx) {
+            const int q = cidx * 32 + lane;
+            const float4 v = vn;
+            if (cidx + 1 < c_end) vn = load_src(q + 32);
+            int x, y;
+            pixel_of(q, x, y);
+            float c[3];
+            composite((float)x + 0.5f, (float)y + 0.5f, c, nullptr);
+            float e[3] = {clamp01(c[0]) - v.x, clamp01(c[1]) - v.y, clamp01(c[2]) - v.z};
+            const int span = bb < 32 ? bb : 32;
+            for (int o = 1; o < span; o <<= 1)
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) e[ch] += __shfl_xor_sync(FULL, e[ch], o);
+            if ((lane & (span - 1)) == 0) {
+                const int j = q >> lbb;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) msum[j * 3 + ch] += e[ch];
             }
         }
-        for (int k = K - 1; k >= 0; --k) {
-            const float* h = hist + ((size_t)k * RF_THREADS + tid) * 3;
-            const float cp[3] = {h[0], h[1], h[2]};
-            float d[14], a;
-            layer_grad(s, k, px, py, soft, g, cp, a, d);
+        group_sync(wpt, grp);
+        for (int i = gt; i < 48; i += GT) msum[i] *= inv_bb;
+        group_sync(wpt, grp);
+        // ---- pass 2: r = e - B M e; loss; per-quadrant sums of (bilinear weight x r)
+        vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int cidx = c_begin; cidx < c_end; ++cidx) {
+            const int q = cidx * 32 + lane;
+            const float4 v = vn;
+            if (cidx + 1 < c_end) vn = load_src(q + 32);
+            int x, y;
+            pixel_of(q, x, y);
+            float c[3], corr[3];
+            composite((float)x + 0.5f, (float)y + 0.5f, c, nullptr);
+            correction(x, y, corr);
+            const float r[3] = {clamp01(c[0]) - v.x - corr[0], clamp01(c[1]) - v.y - corr[1],
+                                clamp01(c[2]) - v.z - corr[2]};
+            sse += (double)fmaf(r[0], r[0], fmaf(r[1], r[1], r[2] * r[2]));
+            if (BWD) {
+                int x0, x1, y0, y1;
+                float wx, wy;
+                grid_coord(x, gscale, x0, x1, wx);
+                grid_coord(y, gscale, y0, y1, wy);
+                const float w4[4] = {(1.0f - wx) * (1.0f - wy), wx * (1.0f - wy), (1.0f - wx) * wy, wx * wy};
+                float acc[12];
 #pragma unroll
-            for (int ch = 0; ch < 3; ++ch) g[ch] *= (1.0f - a);
+                for (int s4 = 0; s4 < 4; ++s4)
 #pragma unroll
-            for (int i = 0; i < 14; ++i) {
-                float v = d[i];
+                    for (int ch = 0; ch < 3; ++ch) acc[s4 * 3 + ch] = w4[s4] * r[ch];
+                const int span = Q < 32 ? Q : 32;
+                for (int o = 1; o < span; o <<= 1)
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-                if (lane == 0) s.red[warp][i] = v;
+                    for (int i = 0; i < 12; ++i) acc[i] += __shfl_xor_sync(FULL, acc[i], o);
+                if ((lane & (span - 1)) == 0) {
+                    const int qi = q >> lq;  // quadrant index, block-major
+#pragma unroll
+                    for (int i = 0; i < 12; ++i) quad[qi * 12 + i] += acc[i];
+                }
             }
-            __syncthreads();
-            if (tid < 14) {
-                float v = s.red[0][tid];
-                for (int w = 1; w < RF_WARPS; ++w) v += s.red[w][tid];
-                s.gacc[k][tid] += v;
+        }
+        if (BWD) {
+            group_sync(wpt, grp);
+            // B^T r per node: sum of the (column, slot) x (row, slot) quadrant entries that
+            // interpolate from this node.
+            for (int i = gt; i < 48; i += GT) {
+                const int node = i / 3, ch = i - node * 3;
+                int sx[4], sy[4];
+                const int nsx = node_sources(node & 3, sx), nsy = node_sources(node >> 2, sy);
+                float acc = 0.0f;
+                for (int a = 0; a < nsy; ++a) {
+                    const int qy = sy[a] >> 1, sly = sy[a] & 1;
+                    for (int c = 0; c < nsx; ++c) {
+                        const int qx = sx[c] >> 1, slx = sx[c] & 1;
+                        const int qi = (((qy >> 1) * 4 + (qx >> 1)) << 2) + ((qy & 1) << 1) + (qx & 1);
+                        acc += quad[qi * 12 + (sly * 2 + slx) * 3 + ch];
+                    }
+                }
+                hnode[i] = acc * inv_bb;
             }
-            __syncthreads();
+            group_sync(wpt, grp);
         }
     }
-    const int p0 = set.prim_off[t];
-    for (int i = tid; i < K * 16; i += RF_THREADS) {
-        const int k = i / 16, j = i % 16;
-        grad[(size_t)(p0 + k) * 16 + j] = j < 14 ? s.gacc[k][j] : 0.0f;
+
+    if (BWD) {
+        // ---- backward pass
+        const float scale = grad_loss[t] * 2.0f / (3.0f * (float)n);
+        float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int cidx = c_begin; cidx < c_end; ++cidx) {
+            const int q = cidx * 32 + lane;
+            const bool valid = q < n;
+            const float4 v = vn;
+            if (cidx + 1 < c_end) vn = load_src(q + 32);
+            int x, y;
+            pixel_of(q, x, y);
+            const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+            float c[3];
+            composite(px, py, c, hist);
+            float g[3] = {0.0f, 0.0f, 0.0f};
+            if (valid) {
+                float e[3] = {clamp01(c[0]) - v.x, clamp01(c[1]) - v.y, clamp01(c[2]) - v.z};
+                if (resid) {
+                    float corr[3];
+                    correction(x, y, corr);
+                    const int j = q >> lbb;
+#pragma unroll
+                    for (int ch = 0; ch < 3; ++ch) e[ch] = e[ch] - corr[ch] - hnode[j * 3 + ch];
+                } else {
+                    sse += (double)fmaf(e[0], e[0], fmaf(e[1], e[1], e[2] * e[2]));
+                }
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) g[ch] = (c[ch] >= 0.0f && c[ch] <= 1.0f) ? scale * e[ch] : 0.0f;
+            }
+            for (int k = K - 1; k >= 0; --k) {
+                const float* hh = hist + ((size_t)k * 32 + lane) * 3;
+                const float cp[3] = {hh[0], hh[1], hh[2]};
+                float d[14], a;
+                layer_grad(S, k, px, py, soft, g, cp, a, d);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) g[ch] *= (1.0f - a);
+                const unsigned cols = grad_columns(prep[k].kind);
+                if (lane_acc) {
+                    float* la = lacc + (size_t)k * 14 * 32 + lane;
+#pragma unroll
+                    for (int i = 0; i < 14; ++i)
+                        if ((cols >> i) & 1u) la[i * 32] += d[i];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 14; ++i) {
+                        if (!((cols >> i) & 1u)) continue;
+                        float s = d[i];
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+                        if (lane == 0) gacc[k * 14 + i] += s;
+                    }
+                }
+            }
+        }
+        if (lane_acc) {
+            // lane j sums slot j's 32 lane partials, starting at lane j (no bank conflicts)
+            __syncwarp();
+            for (int j = lane; j < K * 14; j += 32) {
+                const float* la = lacc + (size_t)j * 32;
+                float s = 0.0f;
+                for (int l = 0; l < 32; ++l) s += la[(l + j) & 31];
+                gacc[j] = s;
+            }
+        }
+        group_sync(wpt, grp);
+        for (int i = gt; i < K * 16; i += GT) {
+            const int k = i >> 4, j = i & 15;
+            float s = 0.0f;
+            if (j < 14)
+                for (int w = 0; w < wpt; ++w) s += gacc_all[((size_t)w * L + k) * 14 + j];
+            const size_t at = (size_t)(p0 + k) * 16 + j;
+            if (grad) grad[at] = s;
+            if (MODE == RF_STEP && j < 14) {
+                const float tstep = adam.m[(size_t)(p0 + k) * 16 + 15] + 1.0f;
+                float m = adam.m[at], v = adam.v[at];
+                params[at] = adam_update(raw[k][j], s, m, v, tstep, adam.lr, adam.b1, adam.b2, adam.eps,
+                                         set.kind[p0 + k], j);
+                adam.m[at] = m;
+                adam.v[at] = v;
+            }
+        }
+        if (MODE == RF_STEP) {
+            group_sync(wpt, grp);  // every column of a row has read its step count
+            for (int k = gt; k < K; k += GT) adam.m[(size_t)(p0 + k) * 16 + 15] += 1.0f;
+        }
+    } else if (!resid) {
+        float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int cidx = c_begin; cidx < c_end; ++cidx) {
+            const int q = cidx * 32 + lane;
+            const float4 v = vn;
+            if (cidx + 1 < c_end) vn = load_src(q + 32);
+            if (q >= n) continue;
+            int x, y;
+            pixel_of(q, x, y);
+            float c[3];
+            composite((float)x + 0.5f, (float)y + 0.5f, c, nullptr);
+            const float dr = clamp01(c[0]) - v.x, dg = clamp01(c[1]) - v.y, db = clamp01(c[2]) - v.z;
+            sse += (double)fmaf(dr, dr, fmaf(dg, dg, db * db));
+        }
     }
     if (loss != nullptr) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(FULL, sse, o);
-        if (lane == 0) s.lred[warp] = sse;
-        __syncthreads();
-        if (tid == 0) {
+        if (lane == 0) lred[wig] = sse;
+        group_sync(wpt, grp);
+        if (gt == 0) {
             double tot = 0.0;
-            for (int w = 0; w < RF_WARPS; ++w) tot += s.lred[w];
+            for (int w = 0; w < wpt; ++w) tot += lred[w];
             loss[t] = (float)(tot / (3.0 * n));
         }
     }
+}
+
+template <int MODE>
+static int launch_refine(const WeftStackSet& set, float* params, const float* grad_loss, float* grad, float* loss,
+                         int flags, AdamArgs adam, cudaStream_t stream, const char* what) {
+    if (set.n_tiles == 0) return WEFTK_OK;
+    if (set.max_prims < 0 || set.max_prims > MAXL) return fail(WEFTK_E_RANGE, std::string(what) + ": stack too long");
+    if (!params || !set.src || !set.px_off || !set.size || !set.prim_off || (set.max_prims > 0 && !set.kind))
+        return fail(WEFTK_E_ARG, std::string(what) + ": null pointer in the stack set");
+    const int L = set.max_prims > 0 ? set.max_prims : 1;
+    RefinePlan plan{};
+    int counts[RF_CLASSES] = {0, 0, 0, 0};
+    if (set.order == nullptr) {
+        counts[1] = set.n_tiles;  // no split: four warps per tile
+    } else {
+        if (set.n_big < 0 || set.n_mid < 0 || set.n_s16 < 0 ||
+            (long long)set.n_big + set.n_mid + set.n_s16 > set.n_tiles)
+            return fail(WEFTK_E_ARG, std::string(what) + ": bad size-class counts");
+        counts[0] = set.n_big;
+        counts[1] = set.n_mid;
+        counts[2] = set.n_s16;
+        counts[3] = set.n_tiles - set.n_big - set.n_mid - set.n_s16;
+    }
+    int smem = 0, ctas = 0, off = 0;
+    for (int c = 0; c < RF_CLASSES; ++c) {
+        const int wpt = class_wpt(c);
+        const int bytes = group_layout(L, wpt, (flags & WEFTK_LOSS_RESIDUAL) != 0).bytes;
+        const int g = std::min(8 / wpt, RF_SMEM_MAX / bytes);
+        plan.groups[c] = g;
+        plan.list_off[c] = off;
+        plan.n_list[c] = counts[c];
+        off += counts[c];
+        ctas += (counts[c] + g - 1) / g;
+        plan.cta_end[c] = ctas;
+        if (counts[c]) smem = std::max(smem, g * bytes);
+    }
+    static int attr = 48 * 1024;
+    if (smem > attr) {
+        WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr = smem;
+    }
+    refine_tiles_kernel<MODE><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags, plan, L,
+                                                                  adam);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
 }
 
 // Adam (PyTorch's rule) + projection onto the wire-representable box, one thread per value.
@@ -400,22 +771,10 @@ __global__ void adam_project_kernel(float* __restrict__ p, const float* __restri
     if (i >= n_rows * 16) return;
     const int col = i & 15, row = i >> 4;
     if (col >= 14) return;
-    const float t = (float)(*step + 1);
-    const float gi = g[i];
-    const float mi = fmaf(b1, m[i], (1.0f - b1) * gi);
-    const float vi = fmaf(b2, v[i], (1.0f - b2) * gi * gi);
+    float mi = m[i], vi = v[i];
+    p[i] = adam_update(p[i], g[i], mi, vi, (float)(*step + 1), lr, b1, b2, eps, kind[row], col);
     m[i] = mi;
     v[i] = vi;
-    const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
-    float x = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
-    const int k = kind[row];
-    if (col >= 7) {
-        x = fminf(fmaxf(x, 0.0f), 1.0f);
-    } else {
-        const bool thick = (k == K_LINE && col == 4) || (k == K_CURVE && col == 6);
-        x = fminf(fmaxf(x, 0.0f), thick ? 4.0f : 15.0f);
-    }
-    p[i] = x;
 }
 
 __global__ void step_increment_kernel(int* step) { *step += 1; }
@@ -427,11 +786,8 @@ using namespace weftk;
 extern "C" int weftk_stack_loss(const WeftStackSet* set, const float* d_params, float* d_loss, int flags,
                                 void* stream) {
     WEFTK_REQUIRE(set && d_loss, "stack_loss: null argument");
-    if (set->n_tiles == 0) return WEFTK_OK;
-    WEFTK_REQUIRE(set->max_prims >= 0 && set->max_prims <= WEFTK_REFINE_MAX_PRIMS, "stack_loss: stack too long");
-    stack_loss_kernel<<<set->n_tiles, RF_THREADS, 0, (cudaStream_t)stream>>>(*set, d_params, d_loss, flags);
-    WEFTK_CUDA(cudaGetLastError());
-    return WEFTK_OK;
+    return launch_refine<RF_LOSS>(*set, const_cast<float*>(d_params), nullptr, nullptr, d_loss, flags, AdamArgs{},
+                                  (cudaStream_t)stream, "stack_loss");
 }
 
 extern "C" int weftk_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, const int32_t* d_kind,
@@ -451,18 +807,14 @@ extern "C" int weftk_adam_step(float* d_params, const float* d_grads, float* d_m
 extern "C" int weftk_stack_loss_backward(const WeftStackSet* set, const float* d_params, const float* d_grad_loss,
                                          float* d_grad_params, float* d_loss, int flags, void* stream) {
     WEFTK_REQUIRE(set && d_grad_loss && d_grad_params, "stack_loss_backward: null argument");
-    if (set->n_tiles == 0) return WEFTK_OK;
-    WEFTK_REQUIRE(set->max_prims >= 0 && set->max_prims <= WEFTK_REFINE_MAX_PRIMS,
-                  "stack_loss_backward: stack too long");
-    const int smem = (set->max_prims > 0 ? set->max_prims : 1) * RF_THREADS * 3 * (int)sizeof(float);
-    static int attr = 0;
-    if (smem > attr) {
-        WEFTK_CUDA(cudaFuncSetAttribute(stack_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        MAXL * RF_THREADS * 3 * (int)sizeof(float)));
-        attr = MAXL * RF_THREADS * 3 * (int)sizeof(float);
-    }
-    stack_backward_kernel<<<set->n_tiles, RF_THREADS, smem, (cudaStream_t)stream>>>(*set, d_params, d_grad_loss,
-                                                                                     d_grad_params, d_loss, flags);
-    WEFTK_CUDA(cudaGetLastError());
-    return WEFTK_OK;
+    return launch_refine<RF_GRAD>(*set, const_cast<float*>(d_params), d_grad_loss, d_grad_params, d_loss, flags,
+                                  AdamArgs{}, (cudaStream_t)stream, "stack_loss_backward");
+}
+
+extern "C" int weftk_refine_step(const WeftStackSet* set, float* d_params, float* d_m, float* d_v,
+                                 const float* d_grad_loss, float* d_loss, float* d_grad_params, float lr, float beta1,
+                                 float beta2, float eps, int flags, void* stream) {
+    WEFTK_REQUIRE(set && d_params && d_m && d_v && d_grad_loss, "refine_step: null argument");
+    return launch_refine<RF_STEP>(*set, d_params, d_grad_loss, d_grad_params, d_loss, flags,
+                                  AdamArgs{d_m, d_v, lr, beta1, beta2, eps}, (cudaStream_t)stream, "refine_step");
 }

@@ -24,6 +24,7 @@ from . import _lib
 from ._lib import PRIM_DTYPE
 
 SOFT_TRIANGLES = 2
+LOSS_RESIDUAL = 4
 MAX_PRIMS = 32
 GEOM_LEN = {0: 0, 1: 4, 2: 5, 3: 7, 4: 6, 5: 0}
 
@@ -70,8 +71,15 @@ class StackSet:
             self.kinds_np = np.asarray(kinds, np.int32)
             self.t_kind = torch.from_numpy(self.kinds_np).to(self.device)
         self.t_prim_off = torch.from_numpy(self.prim_off_np.astype(np.int32)).to(self.device)
+        # work split by tile side (largest first): > 32 px eight warps, 17-32 four, 9-16 two, <= 8 one
+        sz = sizes.cpu().numpy()
+        classes = [sz > 32, (sz > 16) & (sz <= 32), (sz > 8) & (sz <= 16), sz <= 8]
+        order = np.concatenate([np.nonzero(c)[0] for c in classes]).astype(np.int32)
+        self.t_order = torch.from_numpy(order).to(self.device)
+        n_big, n_mid, n_s16 = (int(c.sum()) for c in classes[:3])
         self.st = _lib.WeftStackSet(self.n, self.max_prims, _lib.ptr(src), _lib.ptr(px_off), _lib.ptr(sizes),
-                                    _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind))
+                                    _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind), _lib.ptr(self.t_order),
+                                    n_big, n_mid, n_s16)
         n_px = (sizes.to(torch.int64) ** 2)
         self.weights = (n_px.to(torch.float32) / float(n_px.sum().item())) if self.n else n_px.float()
 
@@ -108,19 +116,21 @@ class StackSet:
     def _stream(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
 
-    def loss(self, params: torch.Tensor, soft: bool = False) -> torch.Tensor:
+    def loss(self, params: torch.Tensor, soft: bool = False, residual: bool = False) -> torch.Tensor:
+        """Per-tile loss; ``residual`` scores the error left after the tile's residual grid."""
         params = params.detach().contiguous()
         out = torch.empty(self.n, dtype=torch.float32, device=self.device)
         _lib.check(self.lib.weftk_stack_loss(ctypes_addr(self.st), _lib.ptr(params), _lib.ptr(out),
-                                             SOFT_TRIANGLES if soft else 0, self._stream()), "weftk_stack_loss")
+                                             loss_flags(soft, residual), self._stream()), "weftk_stack_loss")
         return out
 
-    def loss_backward(self, params: torch.Tensor, grad_loss: torch.Tensor, soft: bool = False) -> torch.Tensor:
+    def loss_backward(self, params: torch.Tensor, grad_loss: torch.Tensor, soft: bool = False,
+                      residual: bool = False) -> torch.Tensor:
         params = params.detach().contiguous()
         g = grad_loss.detach().to(torch.float32).contiguous()
         out = torch.zeros_like(params)
         _lib.check(self.lib.weftk_stack_loss_backward(ctypes_addr(self.st), _lib.ptr(params), _lib.ptr(g),
-                                                      _lib.ptr(out), 0, SOFT_TRIANGLES if soft else 0, self._stream()),
+                                                      _lib.ptr(out), 0, loss_flags(soft, residual), self._stream()),
                    "weftk_stack_loss_backward")
         return out
 
@@ -163,6 +173,10 @@ class StackSet:
         return [cands[off[t]:off[t + 1]] for t in range(self.n)]
 
 
+def loss_flags(soft: bool = False, residual: bool = False) -> int:
+    return (SOFT_TRIANGLES if soft else 0) | (LOSS_RESIDUAL if residual else 0)
+
+
 def ctypes_addr(st) -> int:
     import ctypes
 
@@ -173,22 +187,24 @@ class StackLoss(torch.autograd.Function):
     """Per-tile losses of the stacks; backward is the hand-written kernel."""
 
     @staticmethod
-    def forward(ctx, params: torch.Tensor, stack_set: StackSet, soft: bool = False):
+    def forward(ctx, params: torch.Tensor, stack_set: StackSet, soft: bool = False, residual: bool = False):
         ctx.stack_set = stack_set
         ctx.soft = soft
+        ctx.residual = residual
         ctx.save_for_backward(params)
-        return stack_set.loss(params, soft)
+        return stack_set.loss(params, soft, residual)
 
     @staticmethod
     def backward(ctx, grad_loss):
         (params,) = ctx.saved_tensors
-        return ctx.stack_set.loss_backward(params, grad_loss, ctx.soft), None, None
+        return ctx.stack_set.loss_backward(params, grad_loss, ctx.soft, ctx.residual), None, None, None
 
 
-def refine(stack_set: StackSet, params: torch.Tensor, steps: int = 200, lr: float = 1e-2
+def refine(stack_set: StackSet, params: torch.Tensor, steps: int = 200, lr: float = 1e-2, residual: bool = False
            ) -> tuple[torch.Tensor, list[float]]:
     """Adam (FP32 parameters and moments) on the pixel-weighted total loss, projecting
-    onto the wire-representable box after every step; returns (params, loss history)."""
+    onto the wire-representable box after every step; returns (params, loss history).
+    ``residual`` optimises the error left after the tile's residual grid."""
     p = params.detach().clone().contiguous()
     stack_set.project_(p)
     p.requires_grad_(True)
@@ -197,7 +213,7 @@ def refine(stack_set: StackSet, params: torch.Tensor, steps: int = 200, lr: floa
     hist = []
     for _ in range(int(steps)):
         opt.zero_grad(set_to_none=False)
-        loss = (StackLoss.apply(p, stack_set, False) * w).sum()
+        loss = (StackLoss.apply(p, stack_set, False, residual) * w).sum()
         loss.backward()
         opt.step()
         stack_set.project_(p.data)
@@ -206,13 +222,17 @@ def refine(stack_set: StackSet, params: torch.Tensor, steps: int = 200, lr: floa
 
 
 class FusedRefiner:
-    """Adam refinement with one fused loss+gradient launch and one fused Adam+projection
-    launch per step (no autograd, no torch optimizer), optionally replayed from a CUDA
-    graph.  Same update rule as ``refine`` (PyTorch's Adam, FP32 moments)."""
+    """Adam refinement without autograd or a torch optimizer: one launch per step
+    (``weftk_refine_step``: loss, gradient, Adam and projection per tile group), or with
+    ``single_launch=False`` a loss+gradient launch followed by an Adam+projection launch.
+    Same update rule as ``refine`` (PyTorch's Adam, FP32 moments); capturable in a CUDA
+    graph."""
 
     def __init__(self, stack_set: StackSet, params: torch.Tensor, lr: float = 1e-2, betas=(0.9, 0.999),
-                 eps: float = 1e-8):
+                 eps: float = 1e-8, residual: bool = False, single_launch: bool = True):
         self.ss = stack_set
+        self.single_launch = single_launch
+        self.flags = loss_flags(False, residual)
         self.p = params.detach().clone().contiguous()
         stack_set.project_(self.p)
         self.g = torch.zeros_like(self.p)
@@ -226,8 +246,13 @@ class FusedRefiner:
     def step(self) -> None:
         lib, ss = self.ss.lib, self.ss
         s = ss._stream()
+        if self.single_launch:
+            _lib.check(lib.weftk_refine_step(ctypes_addr(ss.st), _lib.ptr(self.p), _lib.ptr(self.m), _lib.ptr(self.v),
+                                             _lib.ptr(self.w), _lib.ptr(self.loss), 0, self.lr, self.b1, self.b2,
+                                             self.eps, self.flags, s), "weftk_refine_step")
+            return
         _lib.check(lib.weftk_stack_loss_backward(ctypes_addr(ss.st), _lib.ptr(self.p), _lib.ptr(self.w),
-                                                 _lib.ptr(self.g), _lib.ptr(self.loss), 0, s),
+                                                 _lib.ptr(self.g), _lib.ptr(self.loss), self.flags, s),
                    "weftk_stack_loss_backward")
         _lib.check(lib.weftk_adam_step(_lib.ptr(self.p), _lib.ptr(self.g), _lib.ptr(self.m), _lib.ptr(self.v),
                                        _lib.ptr(ss.t_kind), int(self.p.shape[0]), self.lr, self.b1, self.b2, self.eps,
@@ -252,7 +277,7 @@ class RefinedFit:
     fit's (possibly kind-filtered) pools, gather of each tile's selected primitive, and
     ``steps`` fused Adam steps.  Every launch is device work on torch's current stream."""
 
-    def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True):
+    def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True, residual: bool = False):
         self.fit = fit
         dev = fit.device
         has = fit.init_cnt > 0
@@ -262,7 +287,7 @@ class RefinedFit:
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
         self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0)
         self.start = torch.zeros((n_rows, 16), dtype=torch.float32, device=dev)
-        self.refiner = FusedRefiner(self.ss, self.start, lr=lr)
+        self.refiner = FusedRefiner(self.ss, self.start, lr=lr, residual=residual)
         self.steps = int(steps)
         self.pool_off = torch.from_numpy(fit.pool_off).to(dev)
         self.graph = None

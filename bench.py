@@ -164,11 +164,14 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
-    """Decoder primitive walk of the fitted stacks at out_w x out_h (one launch renders the image).
+def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=None):
+    """Decoder primitive walk of the fitted stacks at out_w x out_h (one launch renders the image),
+    with each tile's RES0 offset and RES1 grid (computed from ``patches`` as the encoder does)
+    when ``patches`` is given.
 
     Each launch is timed alone with CUDA events; a 256 MiB buffer is written between launches so the
-    99.5 MB output is not served from L2.
+    99.5 MB output is not served from L2, and a short GPU sleep after it keeps the stream busy while
+    the host enqueues the timed launch (host launch latency is not counted).
     """
     import ctypes
 
@@ -185,11 +188,21 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
             self.residual_rgb = (0, 0, 0)
 
     recs = [_Rec(s) for s in fit.selected()]
-    descs, prims, cp48, _, th, tw = build_scene(recs, tiles, width, height, None, out_w, out_h)
+    maps = None
+    if patches is not None:
+        from weft_b200.encode import residuals_from_recon
+
+        res0, res1 = residuals_from_recon(patches, fit.recon_tiles())
+        for r, v in zip(recs, res0):
+            r.residual_rgb = v
+        maps = [g.astype(np.float32) / np.float32(255.0) for g in res1]
+    descs, prims, cp48, res1_tab, th, tw = build_scene(recs, tiles, width, height, maps, out_w, out_h)
     dev = torch.device("cuda", torch.cuda.current_device())
     t_d = torch.from_numpy(descs.view(np.uint8)).to(dev)
     t_p = torch.from_numpy(prims.view(np.uint8)).to(dev)
     t_c = torch.from_numpy(np.ascontiguousarray(cp48)).to(dev)
+    n_res1 = 0 if res1_tab is None else len(res1_tab)
+    t_r = torch.from_numpy(np.ascontiguousarray(res1_tab)).to(dev) if n_res1 else None
     out = torch.empty((th, tw, 3), dtype=torch.float32, device=dev)
     items = decode_items(descs)
     t_i = torch.from_numpy(items).to(dev)
@@ -199,7 +212,8 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
 
     def launch():
         _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_i), len(items), _lib.ptr(t_p),
-                                          _lib.ptr(t_c), len(cp48), 0, 0, _lib.ptr(out), th, tw, 0,
+                                          _lib.ptr(t_c), len(cp48), _lib.ptr(t_r) if n_res1 else 0, n_res1,
+                                          _lib.ptr(out), th, tw, 0,
                                           stream.cuda_stream), "weftk_render_tiles")
 
     for _ in range(3):
@@ -207,6 +221,7 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
     times = []
     for _ in range(iters):
         flush.fill_(1.0)
+        torch.cuda._sleep(100000)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         launch()
@@ -218,13 +233,14 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak):
     if st.value:
         raise RuntimeError("decode walk reported a bad descriptor")
     ms = statistics.median(times)
-    nbytes = 12 * tw * th + 48 * len(descs) + 60 * len(prims)
+    nbytes = 12 * tw * th + 48 * len(descs) + 60 * len(prims) + 192 * n_res1
     gbs = nbytes / (ms * 1e-3) / 1e9
     peak_gbs, peak_source = peak
     return {"target": f"{tw}x{th}", "ms": ms, "mpix_per_s": tw * th / (ms * 1e-3) / 1e6, "bytes": nbytes,
             "achieved_gbs": gbs, "peak_gbs": peak_gbs, "frac": gbs / peak_gbs,
             "peak_source": peak_source,
-            "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims))}
+            "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims)),
+            "residuals": "RES0 + RES1 grids" if n_res1 else "none"}
 
 
 def _recon_of(stack_set, params, tiles, size):
@@ -243,6 +259,16 @@ def _recon_of(stack_set, params, tiles, size):
 
 
 REFINE_POOLS = {"nocurve": (0, 1, 2, 4, 5), "smooth": (0, 1, 2), "constlin": (0, 1)}
+
+
+def rd_of_params(ss, params, tiles, patches, img, size) -> dict:
+    """RD of refined parameter rows written as a WEFT file (quantised rows, RES0/RES1 from
+    their render) and decoded."""
+    from weft_b200.encode import encode_fit, rd_score
+
+    q = ss.quantize(params)
+    recon = _recon_of(ss, q, tiles, size)[1]
+    return rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, ss.to_stacks(q), recon), QUALITY)
 
 
 def rd_compare(args, fit, tiles, patches, pools, img, stream):
@@ -287,9 +313,7 @@ def rd_compare(args, fit, tiles, patches, pools, img, stream):
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / args.refine_reps
         ss = rf.ss
-        q = ss.quantize(out)
-        recon = _recon_of(ss, q, tiles, size)[1]
-        sc = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, ss.to_stacks(q), recon), QUALITY)
+        sc = rd_of_params(ss, out, tiles, patches, img, size)
         variants.append({"pool": name, "kinds": list(keep), "adam_steps": int(steps),
                          "loss": "decoded (after residual grid)" if residual else "primitives only", **sc, "ms": ms,
                          "mpix_per_s": n_px / (ms * 1e-3) / 1e6, "rd_delta_db": sc["rd_score"] - plain["rd_score"]})
@@ -297,6 +321,90 @@ def rd_compare(args, fit, tiles, patches, pools, img, stream):
     return {"plain": {**plain, "prims": sum(len(s) for s in plain_stacks)}, "lr": args.refine_lr,
             "refined": variants,
             "init": "best single candidate per tile from the kind-filtered pool, no greedy rounds"}
+
+
+# FP32 operations per pixel and layer of one refine step (loss + gradient + Adam is
+# negligible per pixel): the forward composite evaluates the layer (the scoring kernel's
+# per-kind count) and blends it (9), the backward re-evaluates it and chains the gradient
+# (per-kind count of the chain rule in layer_grad), plus 9 per pixel for the loss.
+REFINE_EVAL = {0: 10, 1: 24, 2: 28, 3: 509, 4: 26, 5: 0}
+REFINE_CHAIN = {0: 12, 1: 45, 2: 40, 3: 60, 4: 40, 5: 0}
+
+
+def refine_flops(stack_set) -> float:
+    """FP32 operations of one refine launch over the stack set."""
+    import torch
+
+    kinds = stack_set.t_kind.cpu().numpy()
+    off = stack_set.prim_off_np
+    px = (stack_set.sizes.to(torch.int64) ** 2).cpu().numpy().astype(np.float64)
+    per_row = np.array([2 * REFINE_EVAL.get(int(k), 0) + 9 + REFINE_CHAIN.get(int(k), 0) for k in kinds], np.float64)
+    starts = np.minimum(off[:-1], max(len(per_row) - 1, 0))
+    tile_cost = np.add.reduceat(per_row, starts) if len(per_row) else np.zeros(len(px))
+    tile_cost[np.diff(off) == 0] = 0.0
+    return float((px * (tile_cost + 9.0)).sum())
+
+
+def refined_headline(args, local, pixels, sizes, pools, stream, world):
+    """The gradient-refined batched fit: init round over the kind-filtered pool, then
+    ``--refine-steps`` fused Adam steps, replayed from one CUDA graph.  Each timed step is
+    preceded by a 256 MiB write (the step's working set fits in L2) and a short GPU sleep
+    (host launch latency is not counted)."""
+    import torch
+
+    from weft_b200.fit import BatchedFit
+    from weft_b200.refine import RefinedFit
+
+    keep = REFINE_POOLS[args.refine_pool]
+    fast_pools = [p[np.isin(p["kind"], keep)] for p in pools]
+    rec = np.concatenate(fast_pools)
+    cnt = np.array([len(p) for p in fast_pools], np.int64)
+    fast = BatchedFit.from_arrays(pixels, sizes, rec, cnt, QUALITY, caps=[CAP] * len(sizes), device=local, reserve=0)
+    rf = RefinedFit(fast, steps=args.refine_steps, lr=args.refine_lr, use_graph=True)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    for _ in range(args.warmup):
+        rf.run()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda._sleep(100000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rf.run()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    del flush
+    return rf, fast, rec, cnt, statistics.mean(times)
+
+
+def refined_breakdown(args, rf, fast, lib, stream):
+    """Eager run of the same pipeline: scoring-kernel time of the init round (events inside
+    the library) and the mean refine-step kernel time (events around the steps)."""
+    import ctypes
+
+    import torch
+
+    lib.weftk_fit_timing(1, None, None)
+    fast.run_init_only()
+    torch.cuda.synchronize()
+    score_ms, n_score = ctypes.c_double(0), ctypes.c_int(0)
+    lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
+    fr = rf.refiner
+    fr.restart(rf.start)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fr.run(args.refine_steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    step_ms = a.elapsed_time(b) / max(args.refine_steps, 1)
+    return score_ms.value, n_score.value, step_ms, fast.work_counters()
 
 
 def _hbm_peak() -> tuple[float, str]:
@@ -363,8 +471,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--decode-iters", type=int, default=10)
-    ap.add_argument("--refine-variants", default="constlin:0,constlin:20,constlin:20:r,nocurve:20:r",
-                    help="refined fits to compare, pool:adam_steps[:r] (r: decoded-error loss; empty: skip)")
+    ap.add_argument("--refine-pool", default="constlin", choices=sorted(REFINE_POOLS),
+                    help="candidate kinds the refined fit's init round scores")
+    ap.add_argument("--refine-steps", type=int, default=10, help="Adam steps of the refined fit")
+    ap.add_argument("--refine-variants", default="constlin:0,constlin:10,constlin:20,constlin:20:r,nocurve:20:r",
+                    help="refined fits whose RD is reported, pool:adam_steps[:r] (r: decoded-error loss)")
     ap.add_argument("--refine-reps", type=int, default=5)
     ap.add_argument("--refine-lr", type=float, default=1e-2)
     args = ap.parse_args()
@@ -471,59 +582,126 @@ def run_weft(args, world, rank, local, executor, cores):
 
     decode = decode_bench(fit, tiles, args.size, args.size, 3840, 2160, args.decode_iters, _hbm_peak()) \
         if args.decode_iters > 0 else None
+    decode_res = decode_bench(fit, tiles, args.size, args.size, 3840, 2160, args.decode_iters, _hbm_peak(),
+                              patches) if args.decode_iters > 0 else None
 
     rd = rd_compare(args, fit, tiles, patches, pools, img, stream) if args.refine_variants else None
+    plain_value, plain_ms = value, ms_step
 
-    # e2e through the public API from host buffers
-    e2e_ms = []
-    h2d = d2h = 0
-    for _ in range(args.e2e_steps):
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
+    # e2e of the plain fit through the public API from host buffers
+    def plain_e2e():
         f2 = BatchedFit.from_arrays(pixels, sizes, records, counts, QUALITY, caps=caps, device=local)
         f2.run()
-        idx = f2.selected_indices()
-        b.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms.append(a.elapsed_time(b))
-        h2d = int(pixels.nbytes + records.nbytes + 4 * 6 * f2.n)
-        d2h = int(f2.t_sel.numel() * 4 + f2.t_n_sel.numel() * 4 + 16 * len(f2.stats.per_round))
-        del f2
-    e2e_val = world * n_px / (statistics.mean(e2e_ms) * 1e-3) / 1e6 if e2e_ms else None
+        f2.selected_indices()
+        return (int(pixels.nbytes + records.nbytes + 4 * 6 * f2.n),
+                int(f2.t_sel.numel() * 4 + f2.t_n_sel.numel() * 4 + 16 * len(f2.stats.per_round)))
+
+    def timed_e2e(fn):
+        ms, io = [], (0, 0)
+        for _ in range(args.e2e_steps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            io = fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return (world * n_px / (statistics.mean(ms) * 1e-3) / 1e6 if ms else None), io
+
+    plain_e2e_val, (p_h2d, p_d2h) = timed_e2e(plain_e2e)
+
+    # headline: the gradient-refined fit, at iso RD with the plain fit
+    sampler2 = ClockSampler(local)
+    sampler2.start()
+    rf, fast, frec, fcnt, ref_ms = refined_headline(args, local, pixels, sizes, pools, stream, world)
+    clocks2 = sampler2.stop()
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ref_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ref_ms = float(t.item())
+    ref_value = world * n_px / (ref_ms * 1e-3) / 1e6
+    plain_rd = rd["plain"] if rd else rd_of_params(*fit.stack_set(), tiles, patches, img, args.size)
+    ref_rd = rd_of_params(rf.ss, rf.refiner.p, tiles, patches, img, args.size)
+    rd_delta = ref_rd["rd_score"] - plain_rd["rd_score"]
+    iso = rd_delta >= -0.05
+    r_score_ms, r_n_score, r_step_ms, r_work = refined_breakdown(args, rf, fast, lib, stream)
+    r_flops = refine_flops(rf.ss)
+    refine_tflops = r_flops / (r_step_ms * 1e-3) / 1e12 if r_step_ms > 0 else 0.0
+    init_tflops = r_work[1] / (r_score_ms * 1e-3) / 1e12 if r_score_ms > 0 else 0.0
+    refine_share = args.refine_steps * r_step_ms
+    n_cls = sum(1 for k in (8, 16, 32) if fast.n_items[k])
+    ref_launches = 1 + 3 + n_cls + args.refine_steps  # prepare, begin/select/end + scoring, refine steps
+
+    def refined_e2e():
+        from weft_b200.refine import RefinedFit
+
+        f2 = BatchedFit.from_arrays(pixels, sizes, frec, fcnt, QUALITY, caps=caps, device=local, reserve=0)
+        out_rows = RefinedFit(f2, steps=args.refine_steps, lr=args.refine_lr, use_graph=False).run().cpu()
+        return int(pixels.nbytes + frec.nbytes + sizes.nbytes + fcnt.nbytes), int(out_rows.numel() * 4)
+
+    ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         pick = cpu_sample(patches, pools, args.cpu_budget_s, executor)
         v, wall, px = run_cpu(patches, pools, pick, executor, cores)
         cpu = {"value": v, "unit": "MPix/s", "cores": cores, "kind": "port",
-               "sample": f"oracle greedy over {len(pick)} of {len(tiles)} tiles ({px / 1e6:.3f} MPix), "
+               "sample": f"oracle greedy (plain fit) over {len(pick)} of {len(tiles)} tiles ({px / 1e6:.3f} MPix), "
                          f"{wall:.1f} s wall on {cores} processes"}
     if rank != 0:
         return
+    score_roof = {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                  "frac": achieved_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+                  "kernel": "fit_score_kernel (3 tile-size classes), plain fit",
+                  "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
+                  "score_ms_per_step": score_ms.value / args.steps, "score_launches": n_score.value,
+                  "candidate_pixels_per_step": cand_px // args.steps}
+    refine_roof = {"bound": "fp32", "achieved": refine_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                   "frac": refine_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+                   "kernel": "refine_tiles_kernel (loss + gradient + Adam, one launch per step)",
+                   "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
+                   "ms_per_launch": r_step_ms, "launches_per_step": args.refine_steps,
+                   "flops_per_launch": r_flops}
+    init_roof = {"bound": "fp32", "achieved": init_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                 "frac": init_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+                 "kernel": "fit_score_kernel, init round of the refined fit", "ms_per_step": r_score_ms,
+                 "launches": r_n_score}
+    dominant, other = (refine_roof, init_roof) if refine_share >= r_score_ms else (init_roof, refine_roof)
+    head_value, head_ms = (ref_value, ref_ms) if iso else (plain_value, plain_ms)
     line = {
-        "metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": head_value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plain batched fit, {args.size}x{args.size} synthetic, {args.prims} prims, "
-                               "quadtree 8-64 px (u8 lum variance > 100), q=75, cap 16",
-                   "tiles": len(tiles), "candidates": int(sum(len(p) for p in pools)), "global_batch": world,
-                   "seq_len": 0, "parallelism": f"replicas x{world}",
-                   "l2": "per-step working set (pixels + pools) exceeds L2; no flush"},
-        "e2e": {"value": e2e_val, "unit": "MPix/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
-                     "frac": achieved_tflops / peak_tflops if peak_tflops else None, "traffic": None,
-                     "kernel": "fit_score_kernel (3 tile-size classes)",
-                     "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
-                     "score_ms_per_step": score_ms.value / args.steps, "score_launches": n_score.value,
-                     "candidate_pixels_per_step": cand_px // args.steps},
+        "config": {"workload": (f"gradient-refined batched fit ({args.refine_pool} init round + {args.refine_steps} "
+                                f"fused Adam steps, lr {args.refine_lr}) at iso RD with the plain batched fit"
+                                if iso else "plain batched fit (the refined fit missed iso RD)") +
+                               f", {args.size}x{args.size} synthetic, {args.prims} prims, quadtree 8-64 px "
+                               "(u8 lum variance > 100), q=75, cap 16",
+                   "tiles": len(tiles), "candidates": int(sum(len(p) for p in pools)),
+                   "refined_candidates": int(len(frec)), "global_batch": world, "seq_len": 0,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "refined fit: 256 MiB written before each timed step (working set fits in L2); "
+                         "plain fit: per-step working set (pixels + pools) exceeds L2, no flush"},
+        "e2e": {"value": ref_e2e_val if iso else plain_e2e_val, "unit": "MPix/s",
+                "h2d_bytes_per_step": r_h2d if iso else p_h2d, "d2h_bytes_per_step": r_d2h if iso else p_d2h},
+        "roofline": dominant if iso else score_roof,
+        "roofline_other": other if iso else None,
         "cpu_baseline": cpu,
-        "clocks": clocks,
-        "gpu_launches": launches_per_step * args.steps,
-        "fit": {"rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds, "reseed_host_s": fit.stats.t_reseed_s,
-                "cand_gen_s": cand_s, "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
-                "prim_payload_bytes": prim_bytes},
+        "clocks": clocks2 if iso else clocks,
+        "gpu_launches": (ref_launches if iso else launches_per_step) * args.steps,
+        "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
+                   "plain_psnr_db": plain_rd["psnr_db"], "refined_psnr_db": ref_rd["psnr_db"],
+                   "plain_bpp": plain_rd["bpp"], "refined_bpp": ref_rd["bpp"], "tolerance_db": 0.05},
+        "plain": {"value": plain_value, "ms_per_step": plain_ms, "e2e": plain_e2e_val, "roofline": score_roof,
+                  "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
+                  "rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds,
+                  "reseed_host_s": fit.stats.t_reseed_s, "cand_gen_s": cand_s,
+                  "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
+                  "prim_payload_bytes": prim_bytes},
         "decode": decode,
+        "decode_with_residuals": decode_res,
         "rd": rd,
     }
     print(json.dumps(line), flush=True)

@@ -132,154 +132,187 @@ __device__ __noinline__ void bicubic_pixel(const float* ctrl, int lx, int ly, in
 // (48 bytes) as three 16-byte stores.  A chunk is 32 groups (one per lane) and an item is
 // up to DEC_ITEM_CHUNKS chunks, rendered by ONE warp: the warp stages its tile's
 // primitives in its own slice of shared memory and never waits on the rest of the CTA,
-// so every resident warp works on a different item.  A persistent grid walks the list.
+// so every resident warp works on a different item.  A persistent grid of one wave
+// (every CTA resident) walks the list.  A warp's items are it, it + n_warps, ...; it
+// fetches the records of its next DEC_BATCH items at once (item, descriptor and first
+// primitive, one item per lane), so the dependent-load chain item -> descriptor ->
+// primitive is paid once per batch instead of once per item.
 constexpr int DEC_ITEM_CHUNKS = WEFTK_DECODE_ITEM_CHUNKS;
 constexpr int DEC_WARPS = DEC_THREADS / 32;
+constexpr int DEC_MINB = 4;  // resident CTAs per SM the register budget is set for
+constexpr int DEC_BATCH = 8;
 
 __device__ __forceinline__ int floor_div4(int v) { return v >= 0 ? (v >> 2) : -((-v + 3) >> 2); }
 
-__global__ void __launch_bounds__(DEC_THREADS, 4) render_tiles_kernel(
+__global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
     const WeftPrim* __restrict__ prims, const float* __restrict__ cp48, int n_cp48, const float* __restrict__ res1,
     int n_res1, float* __restrict__ out, int H, int W) {
     __shared__ Prep sp_all[DEC_WARPS][MAX_TILE_PRIMS];
     __shared__ float grid_all[DEC_WARPS][48];
     __shared__ float ctrl_all[DEC_WARPS][48];
+    __shared__ int2 bitem_all[DEC_WARPS][DEC_BATCH];
+    __shared__ WeftTileDecodeDesc bdesc_all[DEC_WARPS][DEC_BATCH];
+    __shared__ WeftPrim bprim_all[DEC_WARPS][DEC_BATCH];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     Prep* sp = sp_all[wid];
     float* grid = grid_all[wid];
     float* ctrl = ctrl_all[wid];
+    int2* bitem = bitem_all[wid];
+    WeftTileDecodeDesc* bdesc = bdesc_all[wid];
+    WeftPrim* bprim = bprim_all[wid];
     const bool w_aligned = (W & 3) == 0;
     const int n_warps = gridDim.x * DEC_WARPS;
-    for (int it = blockIdx.x * DEC_WARPS + wid; it < n_items; it += n_warps) {
-        const int2 item = items[it];
-        __syncwarp();  // this warp's readers of sp/grid/ctrl from the previous item are done
-        if (item.x < 0 || item.x >= n_tiles) {
-            if (lane == 0) report(WEFTK_E_ARG);
-            continue;
+    auto desc_ok = [](const WeftTileDecodeDesc& d) {
+        return d.prim_count >= 0 && d.prim_count <= MAX_TILE_PRIMS && d.target_w > 0 && d.target_h > 0 &&
+               d.target_w <= 8192 && d.target_h <= 8192 && d.source_size > 0;
+    };
+    for (int base = blockIdx.x * DEC_WARPS + wid; base < n_items; base += n_warps * DEC_BATCH) {
+        __syncwarp();  // this warp's readers of the previous batch are done
+        if (lane < DEC_BATCH) {
+            const int idx = base + lane * n_warps;
+            int2 itm = make_int2(-1, 0);
+            if (idx < n_items) itm = items[idx];
+            bitem[lane] = itm;
+            if (itm.x >= 0 && itm.x < n_tiles) {
+                const WeftTileDecodeDesc dd = descs[itm.x];
+                bdesc[lane] = dd;
+                if (desc_ok(dd) && dd.prim_count >= 1) bprim[lane] = load_prim(prims + dd.prim_offset);
+            }
         }
-        const WeftTileDecodeDesc d = descs[item.x];
-        const int n = d.prim_count, w = d.target_w, h = d.target_h;
-        if (n < 0 || n > MAX_TILE_PRIMS || w <= 0 || h <= 0 || w > 8192 || h > 8192 || d.source_size <= 0) {
-            if (lane == 0) report(WEFTK_E_ARG);
-            continue;
-        }
-        const int a0 = floor_div4(d.target_x0);
-        const int G = floor_div4(d.target_x0 + w + 3) - a0;  // aligned groups per row
-        const int n_groups = G * h;                          // < 2^24 for any rect the host accepts
-        const int n_chunks = (n_groups + 31) / 32;
-        const float invG = 1.0f / (float)G;
-        const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
-        for (int i = lane; i < n; i += 32) sp[i] = prep_prim(load_prim(prims + d.prim_offset + i));
-        const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
-        if (has_res1 && d.res1_index >= n_res1) {
-            if (lane == 0) report(WEFTK_E_ARG);
-            continue;
-        }
-        if (has_res1)
-            for (int i = lane; i < 48; i += 32) grid[i] = res1[(size_t)d.res1_index * 48 + i];
         __syncwarp();
-        const bool bic = (n == 1 && sp[0].kind == K_BICUBIC);
-        if (bic) {
-            const int gi = (int)sp[0].q[0];
-            if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
+        for (int b = 0; b < DEC_BATCH; ++b) {
+            if (base + b * n_warps >= n_items) break;
+            const int2 item = bitem[b];
+            __syncwarp();  // this warp's readers of sp/grid/ctrl from the previous item are done
+            if (item.x < 0 || item.x >= n_tiles) {
                 if (lane == 0) report(WEFTK_E_ARG);
                 continue;
             }
-            for (int i = lane; i < 48; i += 32) ctrl[i] = cp48[(size_t)gi * 48 + i];
+            const WeftTileDecodeDesc d = bdesc[b];
+            const int n = d.prim_count, w = d.target_w, h = d.target_h;
+            if (!desc_ok(d)) {
+                if (lane == 0) report(WEFTK_E_ARG);
+                continue;
+            }
+            const int a0 = floor_div4(d.target_x0);
+            const int G = floor_div4(d.target_x0 + w + 3) - a0;  // aligned groups per row
+            const int n_groups = G * h;                          // < 2^24 for any rect the host accepts
+            const int n_chunks = (n_groups + 31) / 32;
+            const float invG = 1.0f / (float)G;
+            const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
+            for (int i = lane; i < n; i += 32)
+                sp[i] = prep_prim(i == 0 ? bprim[b] : load_prim(prims + d.prim_offset + i));
+            const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
+            if (has_res1 && d.res1_index >= n_res1) {
+                if (lane == 0) report(WEFTK_E_ARG);
+                continue;
+            }
+            if (has_res1)
+                for (int i = lane; i < 48; i += 32) grid[i] = res1[(size_t)d.res1_index * 48 + i];
             __syncwarp();
-        }
-        const int side = max(w, h);
-        const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
-        const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
-        for (int chunk = item.y; chunk < c_end; ++chunk) {
-            const int g = chunk * 32 + lane;
-            const bool g_ok = g < n_groups;
-            // row = g / G via the float reciprocal, corrected by one step (exact for g < 2^24)
-            int row = __float2int_rz(((float)g + 0.5f) * invG);
-            row -= (row * G > g) ? 1 : 0;
-            row += ((row + 1) * G <= g) ? 1 : 0;
-            if (!g_ok) row = 0;
-            const int gxs = (a0 + (g_ok ? g - row * G : 0)) * 4;
-            float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
-            int lx[DEC_PPL];
-            bool valid[DEC_PPL];
-#pragma unroll
-            for (int j = 0; j < DEC_PPL; ++j) {
-                lx[j] = gxs + j - d.target_x0;
-                valid[j] = g_ok && lx[j] >= 0 && lx[j] < w;
-                const int lxc = min(max(lx[j], 0), w - 1);
-                fx[j] = __fmul_rn((float)lxc + 0.5f, step);
-                fy[j] = __fmul_rn((float)row + 0.5f, step);
-                cr[j] = cg[j] = cb[j] = 0.0f;
-                lx[j] = lxc;
-            }
+            const bool bic = (n == 1 && sp[0].kind == K_BICUBIC);
             if (bic) {
-                for (int j = 0; j < DEC_PPL; ++j) {
-                    float rgb[3];
-                    bicubic_pixel(ctrl, lx[j], min(row, side - 1), side, rgb);
-                    cr[j] = rgb[0];
-                    cg[j] = rgb[1];
-                    cb[j] = rgb[2];
+                const int gi = (int)sp[0].q[0];
+                if (cp48 == nullptr || gi < 0 || gi >= n_cp48) {
+                    if (lane == 0) report(WEFTK_E_ARG);
+                    continue;
                 }
-            } else {
-                for (int k = 0; k < n; ++k) {
-                    Prep pr = sp[k];
-                    if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
-                    float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
-                    prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
-#pragma unroll
+                for (int i = lane; i < 48; i += 32) ctrl[i] = cp48[(size_t)gi * 48 + i];
+                __syncwarp();
+            }
+            const int side = max(w, h);
+            const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
+            const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
+            for (int chunk = item.y; chunk < c_end; ++chunk) {
+                const int g = chunk * 32 + lane;
+                const bool g_ok = g < n_groups;
+                // row = g / G via the float reciprocal, corrected by one step (exact for g < 2^24)
+                int row = __float2int_rz(((float)g + 0.5f) * invG);
+                row -= (row * G > g) ? 1 : 0;
+                row += ((row + 1) * G <= g) ? 1 : 0;
+                if (!g_ok) row = 0;
+                const int gxs = (a0 + (g_ok ? g - row * G : 0)) * 4;
+                float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
+                int lx[DEC_PPL];
+                bool valid[DEC_PPL];
+    #pragma unroll
+                for (int j = 0; j < DEC_PPL; ++j) {
+                    lx[j] = gxs + j - d.target_x0;
+                    valid[j] = g_ok && lx[j] >= 0 && lx[j] < w;
+                    const int lxc = min(max(lx[j], 0), w - 1);
+                    fx[j] = __fmul_rn((float)lxc + 0.5f, step);
+                    fy[j] = __fmul_rn((float)row + 0.5f, step);
+                    cr[j] = cg[j] = cb[j] = 0.0f;
+                    lx[j] = lxc;
+                }
+                if (bic) {
                     for (int j = 0; j < DEC_PPL; ++j) {
-                        cr[j] = blend(sr[j], a[j], cr[j]);
-                        cg[j] = blend(sg[j], a[j], cg[j]);
-                        cb[j] = blend(sb[j], a[j], cb[j]);
+                        float rgb[3];
+                        bicubic_pixel(ctrl, lx[j], min(row, side - 1), side, rgb);
+                        cr[j] = rgb[0];
+                        cg[j] = rgb[1];
+                        cb[j] = rgb[2];
+                    }
+                } else {
+                    for (int k = 0; k < n; ++k) {
+                        Prep pr = sp[k];
+                        if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
+                        float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
+                        prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
+    #pragma unroll
+                        for (int j = 0; j < DEC_PPL; ++j) {
+                            cr[j] = blend(sr[j], a[j], cr[j]);
+                            cg[j] = blend(sg[j], a[j], cg[j]);
+                            cb[j] = blend(sb[j], a[j], cb[j]);
+                        }
                     }
                 }
-            }
-            float o[DEC_PPL][3];
-#pragma unroll
-            for (int j = 0; j < DEC_PPL; ++j) {
-                float r = clamp01(cr[j] + d.res0_r), gg = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
-                if (has_res1) {
-                    // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
-                    float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
-                    float gy = fminf(fmaxf(__fsub_rn(__fmul_rn((float)row + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
-                    int x0 = (int)floorf(gx), y0 = (int)floorf(gy);
-                    float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
-                    int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
-                    float v[3];
-#pragma unroll
-                    for (int ch = 0; ch < 3; ++ch) {
-                        float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
-                        float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
-                        float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
-                        float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
-                        v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
-                    }
-                    r = clamp01(r + v[0]);
-                    gg = clamp01(gg + v[1]);
-                    b = clamp01(b + v[2]);
-                }
-                o[j][0] = r;
-                o[j][1] = gg;
-                o[j][2] = b;
-            }
-            const int gy = d.target_y0 + row;
-            if (!g_ok || gy < 0 || gy >= H) continue;
-            float* dst = out + ((size_t)gy * W + gxs) * 3;
-            if (w_aligned && valid[0] && valid[DEC_PPL - 1] && gxs >= 0 && gxs + DEC_PPL <= W) {
-                float4* d4 = reinterpret_cast<float4*>(dst);
-                d4[0] = make_float4(o[0][0], o[0][1], o[0][2], o[1][0]);
-                d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
-                d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
-            } else {
-#pragma unroll
+                float o[DEC_PPL][3];
+    #pragma unroll
                 for (int j = 0; j < DEC_PPL; ++j) {
-                    const int gxp = gxs + j;
-                    if (valid[j] && gxp >= 0 && gxp < W) {
-                        dst[3 * j] = o[j][0];
-                        dst[3 * j + 1] = o[j][1];
-                        dst[3 * j + 2] = o[j][2];
+                    float r = clamp01(cr[j] + d.res0_r), gg = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
+                    if (has_res1) {
+                        // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
+                        float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                        float gy = fminf(fmaxf(__fsub_rn(__fmul_rn((float)row + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                        int x0 = (int)floorf(gx), y0 = (int)floorf(gy);
+                        float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
+                        int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
+                        float v[3];
+    #pragma unroll
+                        for (int ch = 0; ch < 3; ++ch) {
+                            float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
+                            float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
+                            float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
+                            float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
+                            v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
+                        }
+                        r = clamp01(r + v[0]);
+                        gg = clamp01(gg + v[1]);
+                        b = clamp01(b + v[2]);
+                    }
+                    o[j][0] = r;
+                    o[j][1] = gg;
+                    o[j][2] = b;
+                }
+                const int gy = d.target_y0 + row;
+                if (!g_ok || gy < 0 || gy >= H) continue;
+                float* dst = out + ((size_t)gy * W + gxs) * 3;
+                if (w_aligned && valid[0] && valid[DEC_PPL - 1] && gxs >= 0 && gxs + DEC_PPL <= W) {
+                    float4* d4 = reinterpret_cast<float4*>(dst);
+                    d4[0] = make_float4(o[0][0], o[0][1], o[0][2], o[1][0]);
+                    d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
+                    d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
+                } else {
+    #pragma unroll
+                    for (int j = 0; j < DEC_PPL; ++j) {
+                        const int gxp = gxs + j;
+                        if (valid[j] && gxp >= 0 && gxp < W) {
+                            dst[3 * j] = o[j][0];
+                            dst[3 * j + 1] = o[j][1];
+                            dst[3 * j + 2] = o[j][2];
+                        }
                     }
                 }
             }
@@ -310,7 +343,7 @@ int launch_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const in
     int dev = 0, sms = 148;
     WEFTK_CUDA(cudaGetDevice(&dev));
     WEFTK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * 4 * 2);
+    const int blocks = std::min((n_items + DEC_WARPS - 1) / DEC_WARPS, sms * DEC_MINB);
     render_tiles_kernel<<<blocks, DEC_THREADS, 0, stream>>>(d_descs, n_tiles, d_items, n_items, d_prims, d_cp48,
                                                             n_cp48, d_res1, n_res1, d_out, out_h, out_w);
     WEFTK_CUDA(cudaGetLastError());

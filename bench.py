@@ -272,8 +272,9 @@ def rd_of_params(ss, params, tiles, patches, img, size) -> dict:
 
 
 def rd_compare(args, fit, tiles, patches, pools, img, stream):
-    """RD of the plain fit vs refined fast fits, both written as WEFT files (RES0/RES1
-    included) and decoded; RD = PSNR - 4 BPP.
+    """RD of the plain fit vs refined fast fits, both written as WEFT files the same way
+    (quantised primitives, RES0/RES1 from the render of the quantised primitives) and
+    decoded; RD = PSNR - 4 BPP.
 
     A refined fast fit scores only the init round over a kind-filtered pool (best single
     candidate per tile), then runs fused Adam steps on that primitive; the whole pipeline
@@ -282,14 +283,13 @@ def rd_compare(args, fit, tiles, patches, pools, img, stream):
     """
     import torch
 
-    from weft_b200.encode import encode_fit, rd_score
     from weft_b200.fit import BatchedFit
     from weft_b200.refine import RefinedFit
 
     size = args.size
     n_px = size * size
     plain_stacks = fit.selected()
-    plain = rd_score(img, encode_fit(size, size, QUALITY, tiles, patches, plain_stacks, fit.recon_tiles()), QUALITY)
+    plain = rd_of_params(*fit.stack_set(), tiles, patches, img, size)
     pixels = np.concatenate([p.reshape(-1, 3) for p in patches])
     sizes = np.array([p.shape[0] for p in patches], np.int32)
     variants = []

@@ -360,6 +360,7 @@ def refined_headline(args, local, pixels, sizes, pools, stream, world):
     rec = np.concatenate(fast_pools)
     cnt = np.array([len(p) for p in fast_pools], np.int64)
     fast = BatchedFit.from_arrays(pixels, sizes, rec, cnt, QUALITY, caps=[CAP] * len(sizes), device=local, reserve=0)
+    fast.autotune()
     rf = RefinedFit(fast, steps=args.refine_steps, lr=args.refine_lr, use_graph=True)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
     for _ in range(args.warmup):
@@ -514,6 +515,7 @@ def run_weft(args, world, rank, local, executor, cores):
     counts = np.array([len(p) for p in pools], np.int64)
     caps = [CAP] * len(patches)
     fit = BatchedFit.from_arrays(pixels, sizes, records, counts, QUALITY, caps=caps, device=local)
+    tuned_plain = fit.autotune()  # scoring shape and candidates per CTA per tile-size class
     n_px = int(sum(p.shape[0] ** 2 for p in patches))
     stream = torch.cuda.current_stream()
 
@@ -699,7 +701,11 @@ def run_weft(args, world, rank, local, executor, cores):
                   "rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds,
                   "reseed_host_s": fit.stats.t_reseed_s, "cand_gen_s": cand_s,
                   "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
-                  "prim_payload_bytes": prim_bytes},
+                  "prim_payload_bytes": prim_bytes,
+                  "autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
+                               for k, v in tuned_plain.items()}},
+        "refined_autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
+                             for k, v in (fast.tuning or {}).items()},
         "decode": decode,
         "decode_with_residuals": decode_res,
         "rd": rd,

@@ -75,7 +75,19 @@ typedef struct WeftFitState {
     int32_t* status;         /* [4] round counters: evaluated tiles, improved tiles */
     unsigned long long* work; /* [2] running totals: candidate-pixels scored, algorithmic FP32 ops
                                  (per candidate-pixel: per-kind op count + 9 for the error); may be NULL */
+    /* Scoring-kernel shape per tile-size class [8-px, 16-px, 32/64-px tiles], an index into
+     * that class's table (0 = default; WEFTK_FIT_VARIANTS per class, see weftk_fit_variant):
+     * pixels per lane x warps per candidate x CTAs per SM.  Chosen by the autotuner. */
+    int32_t variant[3];
+    int32_t _pad;
 } WeftFitState;
+
+#define WEFTK_FIT_VARIANTS 3
+
+/* Shape of scoring variant `variant` of size class `size_class` (8, 16 or 32): pixels per lane,
+ * warps per candidate, resident CTAs per SM the register budget targets. */
+int weftk_fit_variant(int size_class, int variant, int* pixels_per_lane, int* warps_per_candidate,
+                      int* ctas_per_sm);
 
 /* A unit of scoring work: tile, 1024-pixel block, and a run of candidate
  * slots (pool-local, into perm). */

@@ -83,3 +83,41 @@ def test_device_fit_is_deterministic():
     for t in range(0, len(patches), 7):
         full = render.render_tile(a.selected()[t], int(qts[t].size))
         assert np.array_equal(full, a.recon_tiles()[t])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_every_scoring_variant_matches_oracle(variant):
+    """Each autotuner choice (kernel shape per size class, candidates per CTA) picks the same
+    candidates as the oracle greedy on 8/16/32/64-px tiles."""
+    from weft_b200 import candidates, quadtree
+    from weft_b200.fit import BatchedFit
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 64, 3, 3)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    pools = [candidates.tile_candidates(p, 92) for p in patches]
+    caps = [16] * len(qts)
+    fixed = [candidates.residual_candidates(p, np.zeros_like(p), 92) for p in patches]
+    fit = BatchedFit(patches, pools, 92, caps=caps)
+    chunk = (32, 64, 128)[variant]
+    fit.configure(variants={8: variant, 16: variant, 32: variant}, chunks={8: chunk, 16: chunk, 32: chunk})
+    fit.run(reseed=lambda i, patch, pred: list(fixed[i]), max_rounds=2)
+    sel, cur, _ = ofit.greedy_fit(patches, [q.size for q in qts], pools, 92,
+                                  reseed=lambda i, patch, pred: list(fixed[i]), caps=caps, max_rounds=2)
+    assert fit.selected_indices() == sel
+    np.testing.assert_allclose(fit.objectives(), cur, rtol=1e-5)
+
+
+def test_autotune_keeps_the_reference_selection(golden):
+    from weft_b200.fit import BatchedFit
+
+    g = golden("fit_small.npz")
+    tiles, patches, pools, reseeds = _fit_inputs(g)
+    fit = BatchedFit(patches, pools, int(g["quality"]))
+    tuned = fit.autotune(reps=1)
+    assert tuned and all(0 <= v < 3 and c in (32, 64, 128) and ms >= 0 for v, c, ms in tuned.values())
+    queue = {k: list(v) for k, v in reseeds.items()}
+    fit.run(reseed=lambda i, patch, pred: queue[i].pop(0))
+    assert fit.selected_indices() == [[int(v) for v in row if v >= 0] for row in g["selected"]]

@@ -42,7 +42,10 @@ class WeftFitState(ctypes.Structure):
     _fields_ = [("n_tiles", ctypes.c_int32), ("cap_max", ctypes.c_int32), ("n_slots", ctypes.c_int64)] + [
         (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "pool_cap", "n_alive",
                                        "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive", "kind",
-                                       "partial", "status", "work")]
+                                       "partial", "status", "work")] + [
+        ("variant", ctypes.c_int32 * 3), ("_pad", ctypes.c_int32)]
+
+FIT_VARIANTS = 3
 
 
 class WeftStackSet(ctypes.Structure):
@@ -65,7 +68,7 @@ assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
 assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
 FIT_ITEM_DTYPE = np.dtype([("tile", np.int32), ("block", np.int32), ("first", np.int32), ("count", np.int32)])
 assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
-assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8
+assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8 + 16
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -93,6 +96,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_refine_step": [_P, _P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                           ctypes.c_float, _I, _P],
     "weftk_measure_fp32_peak": [_P],
+    "weftk_fit_variant": [_I, _I, _P, _P, _P],
 }
 
 _lock = threading.Lock()

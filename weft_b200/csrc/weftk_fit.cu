@@ -484,6 +484,57 @@ extern "C" int weftk_fit_round_static(const WeftFitState* st, int mode, double l
                            d_items32, n_items32, stream);
 }
 
+// Scoring variants per size class.  A class's variants cover the same pixels per candidate pass
+// (64 for 8-px tiles, 256 for 16-px tiles, one 1024-pixel block for 32/64-px tiles) with a
+// different split over lanes and warps, or a different register budget.
+static_assert(sizeof(WeftFitState) == 200, "WeftFitState layout is part of the C ABI");
+
+struct ScoreShape {
+    int ppl, wpc, minb;
+};
+static const ScoreShape kShapes[3][WEFTK_FIT_VARIANTS] = {
+    {{2, 1, 7}, {2, 1, 8}, {1, 2, 8}},
+    {{8, 1, 4}, {4, 2, 6}, {2, 4, 8}},
+    {{8, 4, 4}, {8, 4, 3}, {8, 4, 5}},
+};
+
+template <int PPL, int WPC, int MINB>
+static void launch_score(const WeftFitState& st, const int* perm, const WeftFitItem* items, int n, int lo, int hi,
+                         cudaStream_t s) {
+    fit_score_kernel<PPL, WPC, MINB><<<n, 128, 0, s>>>(st, perm, items, n, lo, hi);
+}
+
+static void launch_score_class8(int v, const WeftFitState& st, const int* perm, const WeftFitItem* it, int n,
+                                cudaStream_t s) {
+    if (v == 1) launch_score<2, 1, 8>(st, perm, it, n, 8, 8, s);
+    else if (v == 2) launch_score<1, 2, 8>(st, perm, it, n, 8, 8, s);
+    else launch_score<2, 1, 7>(st, perm, it, n, 8, 8, s);
+}
+
+static void launch_score_class16(int v, const WeftFitState& st, const int* perm, const WeftFitItem* it, int n,
+                                 cudaStream_t s) {
+    if (v == 1) launch_score<4, 2, 6>(st, perm, it, n, 16, 16, s);
+    else if (v == 2) launch_score<2, 4, 8>(st, perm, it, n, 16, 16, s);
+    else launch_score<8, 1, 4>(st, perm, it, n, 16, 16, s);
+}
+
+static void launch_score_class32(int v, const WeftFitState& st, const int* perm, const WeftFitItem* it, int n,
+                                 cudaStream_t s) {
+    if (v == 1) launch_score<8, 4, 3>(st, perm, it, n, 32, 64, s);
+    else if (v == 2) launch_score<8, 4, 5>(st, perm, it, n, 32, 64, s);
+    else launch_score<8, 4, 4>(st, perm, it, n, 32, 64, s);
+}
+
+extern "C" int weftk_fit_variant(int size_class, int variant, int* pixels_per_lane, int* warps_per_candidate,
+                                 int* ctas_per_sm) {
+    const int c = size_class == 8 ? 0 : size_class == 16 ? 1 : size_class == 32 ? 2 : -1;
+    WEFTK_REQUIRE(c >= 0 && variant >= 0 && variant < WEFTK_FIT_VARIANTS, "fit_variant: no such class or variant");
+    if (pixels_per_lane) *pixels_per_lane = kShapes[c][variant].ppl;
+    if (warps_per_candidate) *warps_per_candidate = kShapes[c][variant].wpc;
+    if (ctas_per_sm) *ctas_per_sm = kShapes[c][variant].minb;
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double complex_threshold,
                                const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
                                const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
@@ -491,6 +542,8 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
     WEFTK_REQUIRE(st && d_perm, "fit_round: null argument");
     WEFTK_REQUIRE(mode == WEFTK_FIT_INIT || mode == WEFTK_FIT_ROUND, "fit_round: bad mode");
     WEFTK_REQUIRE(n_items8 >= 0 && n_items16 >= 0 && n_items32 >= 0, "fit_round: negative item count");
+    for (int c = 0; c < 3; ++c)
+        WEFTK_REQUIRE(st->variant[c] >= 0 && st->variant[c] < WEFTK_FIT_VARIANTS, "fit_round: bad scoring variant");
     if (st->n_tiles == 0) return WEFTK_OK;
     cudaStream_t s = (cudaStream_t)stream;
     const int nt = st->n_tiles;
@@ -501,9 +554,9 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
         if (rc) return rc;
         WEFTK_CUDA(cudaEventRecord(g_timing.start, s));
     }
-    if (n_items8) fit_score_kernel<2, 1, 7><<<n_items8, 128, 0, s>>>(*st, d_perm, d_items8, n_items8, 8, 8);
-    if (n_items16) fit_score_kernel<8, 1, 4><<<n_items16, 128, 0, s>>>(*st, d_perm, d_items16, n_items16, 16, 16);
-    if (n_items32) fit_score_kernel<8, 4, 4><<<n_items32, 128, 0, s>>>(*st, d_perm, d_items32, n_items32, 32, 64);
+    if (n_items8) launch_score_class8(st->variant[0], *st, d_perm, d_items8, n_items8, s);
+    if (n_items16) launch_score_class16(st->variant[1], *st, d_perm, d_items16, n_items16, s);
+    if (n_items32) launch_score_class32(st->variant[2], *st, d_perm, d_items32, n_items32, s);
     if (g_timing.enabled) {
         WEFTK_CUDA(cudaEventRecord(g_timing.stop, s));
         g_timing.pending = true;

@@ -183,6 +183,8 @@ class BatchedFit:
         self.stats = FitStats()
         self.device_reseeded = False
         self.n_items = {}
+        self.chunk = dict(CHUNK)  # candidates per scoring CTA, per size class (set by autotune)
+        self.tuning = None
         self._prepare(np.zeros(n, np.int32))
         self._build_work()
 
@@ -224,7 +226,7 @@ class BatchedFit:
         sizes = torch.from_numpy(self.sizes.astype(np.int64)).to(d)
         items = {}
         for cls, members in ((8, (8,)), (16, (16,)), (32, (32, 64))):
-            chunk = CHUNK[cls]
+            chunk = self.chunk[cls]
             sel = torch.zeros(n, dtype=torch.bool, device=d)
             for m in members:
                 sel |= sizes == m
@@ -371,6 +373,66 @@ class BatchedFit:
                                       _lib.ptr(ti[8]), self.n_items[8], _lib.ptr(ti[16]), self.n_items[16],
                                       _lib.ptr(ti[32]), self.n_items[32], self._stream())
         _lib.check(rc, "weftk_fit_round")
+
+    # ------------------------------------------------------------------ autotuner
+    def configure(self, variants=None, chunks=None) -> "BatchedFit":
+        """Set the scoring shape per size class ({8|16|32: variant}) and candidates per CTA
+        ({8|16|32: count}, at most 128); rebuilds the work items."""
+        for ci, cls in enumerate((8, 16, 32)):
+            if variants and cls in variants:
+                v = int(variants[cls])
+                if not 0 <= v < _lib.FIT_VARIANTS:
+                    raise ValueError(f"no scoring variant {v} for {cls}-px tiles")
+                self.st.variant[ci] = v
+            if chunks and cls in chunks:
+                c = int(chunks[cls])
+                if not 1 <= c <= 128:
+                    raise ValueError("candidates per CTA must be in 1..128")
+                self.chunk[cls] = c
+        self._build_work()
+        return self
+
+    def autotune(self, chunks=(32, 64, 128), reps: int = 2) -> dict:
+        """Choose, per tile-size class, the scoring kernel's shape (pixels per lane x warps per
+        candidate x CTAs per SM, ``weftk_fit_variant``) and the candidates per CTA that score this
+        fit's init round fastest (CUDA events around the class's scoring launch, best of ``reps``).
+        Leaves the fit reset with the winners in place; returns {class: (variant, chunk, ms)}."""
+        import ctypes
+
+        result = {}
+        for ci, cls in enumerate((8, 16, 32)):
+            if not self.n_items.get(cls):
+                continue
+            best = None
+            for v in range(_lib.FIT_VARIANTS):
+                for ch in chunks:
+                    self.st.variant[ci] = v
+                    self.chunk[cls] = ch
+                    self._build_work()
+                    times = []
+                    for _ in range(reps):
+                        self.reset()
+                        ms, n = ctypes.c_double(0), ctypes.c_int(0)
+                        self.lib.weftk_fit_timing(1, None, None)
+                        ti = self.t_items
+                        args = [(_lib.ptr(ti[k]), self.n_items[k]) if k == cls else (0, 0) for k in (8, 16, 32)]
+                        rc = self.lib.weftk_fit_round(ctypes_ref(self.st), FIT_INIT, self.lam, self.thr,
+                                                      _lib.ptr(self.t_perm), *args[0], *args[1], *args[2],
+                                                      self._stream())
+                        _lib.check(rc, "weftk_fit_round")
+                        torch.cuda.current_stream(self.device).synchronize()
+                        self.lib.weftk_fit_timing(0, ctypes.addressof(ms), ctypes.addressof(n))
+                        times.append(ms.value)
+                    t = min(times)
+                    if best is None or t < best[2]:
+                        best = (v, ch, t)
+            self.st.variant[ci] = best[0]
+            self.chunk[cls] = best[1]
+            result[cls] = best
+        self._build_work()
+        self.reset()
+        self.tuning = result
+        return result
 
     def work_counters(self) -> tuple[int, int]:
         """(candidate-pixels scored, algorithmic FP32 ops) since the last reset."""

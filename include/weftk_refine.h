@@ -53,6 +53,10 @@ typedef struct WeftStackSet {
     int32_t n_big;
     int32_t n_mid;
     int32_t n_s16;
+    /* Kinds the rows may hold, bit k for kind k (0: not declared).  Sets of at most one layer
+     * per tile whose mask is within {constant, linear} run a register-only kernel; a row of
+     * another kind is then reported (WEFTK_E_ARG in the device status) and treated as absent. */
+    int32_t kinds_mask;
 } WeftStackSet;
 
 /* loss[t] for every tile (float32). */

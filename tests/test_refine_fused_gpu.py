@@ -77,6 +77,7 @@ def test_refined_fit_matches_unfused_pipeline(use_graph, residual):
     ss, params = fit.stack_set()
     assert np.array_equal(ss.prim_off_np, rf.ss.prim_off_np)
     assert torch.equal(ss.t_kind, rf.kinds)
+    ss.st.kinds_mask = rf.ss.st.kinds_mask  # same kernel choice as the refined fit (the pool's kinds)
     fr = FusedRefiner(ss, params, lr=1e-2, residual=residual)
     fr.run(10)
     assert torch.equal(fr.p[:, :14], got[:, :14])
@@ -97,3 +98,31 @@ def test_single_launch_step_equals_two_launch_step(residual):
     assert torch.equal(one.p[:, :14], two.p[:, :14])
     assert torch.equal(one.m[:, :14], two.m[:, :14]) and torch.equal(one.v[:, :14], two.v[:, :14])
     assert float(one.m[:, 15].min()) == 8.0 and float(one.m[:, 15].max()) == 8.0
+
+
+@pytest.mark.parametrize("residual", [False, True])
+def test_single_layer_register_path_matches_general_path(residual):
+    """Stacks of one constant/linear layer take the register-only kernel (declared kinds mask
+    {0, 1}); the general kernel (mask undeclared) must give the same loss and gradient."""
+    from weft_b200.refine import FusedRefiner, RefinedFit, StackSet
+
+    fit = _fit(kinds_out=(2, 3, 4, 5))
+    rf = RefinedFit(fit, steps=0, use_graph=False)
+    rf.run()
+    assert rf.ss.st.kinds_mask in (1, 2, 3)
+    gen = StackSet(rf.ss.src, rf.ss.px_off, rf.ss.sizes, rf.ss.prim_off_np, rf.kinds, kinds_mask=0)
+    p = rf.start.clone()
+    w = rf.ss.weights
+    for a, b in ((rf.ss.loss(p, residual=residual), gen.loss(p, residual=residual)),
+                 (rf.ss.loss_backward(p, w, residual=residual), gen.loss_backward(p, w, residual=residual))):
+        scale = float(b.abs().max()) + 1e-30
+        assert float((a - b).abs().max()) <= 1e-4 * scale
+    # Adam normalises each gradient component, so components that are zero up to rounding
+    # (summed in another order by the two kernels) may step differently; the objective may not.
+    one = FusedRefiner(rf.ss, p, residual=residual)
+    two = FusedRefiner(gen, p, residual=residual)
+    for _ in range(10):
+        one.step()
+        two.step()
+        l1, l2 = float((one.loss * w).sum()), float((two.loss * w).sum())
+        assert l1 == pytest.approx(l2, rel=1e-4)

@@ -52,7 +52,8 @@ class WeftStackSet(ctypes.Structure):
     """Device pointers of a set of per-tile stacks (include/weftk_refine.h)."""
     _fields_ = [("n_tiles", ctypes.c_int32), ("max_prims", ctypes.c_int32)] + [
         (n, ctypes.c_void_p) for n in ("src", "px_off", "size", "prim_off", "kind", "order")] + [
-        ("n_big", ctypes.c_int32), ("n_mid", ctypes.c_int32), ("n_s16", ctypes.c_int32)]
+        ("n_big", ctypes.c_int32), ("n_mid", ctypes.c_int32), ("n_s16", ctypes.c_int32),
+        ("kinds_mask", ctypes.c_int32)]
 
 
 # numpy mirrors of the C structs (same byte layout)

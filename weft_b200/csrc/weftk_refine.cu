@@ -371,12 +371,76 @@ __device__ __forceinline__ void group_sync(int wpt, int grp) {
         asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(wpt * 32) : "memory");
 }
 
+// Single-layer stacks of a constant or linear primitive (the refined fit's stacks): the layer's
+// source colour, alpha and the linear ramp parameter at one pixel, with the renderer's formulas
+// (prim_eval), so the forward is the same float sequence; any other kind is a no-op here.
+struct ClEval {
+    float s[3], a, t, traw;
+};
+
+__device__ __forceinline__ ClEval eval_cl(const Prep& P, float px, float py) {
+    ClEval r;
+    r.s[0] = P.cr;
+    r.s[1] = P.cg;
+    r.s[2] = P.cb;
+    r.a = (P.kind == K_CONST || P.kind == K_LINEAR) ? P.a : 0.0f;
+    r.t = r.traw = 0.0f;
+    if (P.kind == K_LINEAR) {
+        r.traw = fmaf(px - P.q[0], P.q[2], (py - P.q[1]) * P.q[3]);
+        r.t = clamp01(r.traw);
+        const float u = 1.0f - r.t;
+        r.s[0] = fmaf(P.q[4], r.t, P.cr * u);
+        r.s[1] = fmaf(P.q[5], r.t, P.cg * u);
+        r.s[2] = fmaf(P.q[6], r.t, P.cb * u);
+    }
+    return r;
+}
+
+// Gradient of that layer over black (c_{-1} = 0), accumulated into acc[14]; the same chain
+// rule as layer_grad's constant and linear cases.
+__device__ __forceinline__ void grad_cl(const Prep& P, const float* r, const ClEval& v, float px, float py,
+                                        const float (&g)[3], float (&acc)[14]) {
+    if (P.kind != K_CONST && P.kind != K_LINEAR) return;
+    const float dA = (r[13] >= 0.0f && r[13] <= 1.0f) ? 1.0f : 0.0f;
+    float dLds[3], dLda = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        dLds[c] = g[c] * v.a;
+        dLda = fmaf(g[c], v.s[c], dLda);
+    }
+    acc[13] = fmaf(dLda, dA, acc[13]);
+    if (P.kind == K_CONST) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[7 + c] += dLds[c];
+        return;
+    }
+    const float t = v.t;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        acc[7 + c] = fmaf(dLds[c], 1.0f - t, acc[7 + c]);
+        acc[10 + c] = fmaf(dLds[c], t, acc[10 + c]);
+    }
+    if (v.traw > 0.0f && v.traw < 1.0f) {
+        const float x0 = r[0], y0 = r[1], vx = r[2] - r[0], vy = r[3] - r[1];
+        const float D = vx * vx + vy * vy + 1e-8f;
+        const float qx = px - x0, qy = py - y0, N = qx * vx + qy * vy;
+        const float dLdt = dLds[0] * (r[10] - r[7]) + dLds[1] * (r[11] - r[8]) + dLds[2] * (r[12] - r[9]);
+        const float iD2 = 1.0f / (D * D);
+        acc[0] += dLdt * ((-vx - qx) * D + N * 2.0f * vx) * iD2;
+        acc[1] += dLdt * ((-vy - qy) * D + N * 2.0f * vy) * iD2;
+        acc[2] += dLdt * (qx * D - N * 2.0f * vx) * iD2;
+        acc[3] += dLdt * (qy * D - N * 2.0f * vy) * iD2;
+    }
+}
+
 // One kernel for the loss (MODE 0), loss + gradient (MODE 1), and loss + gradient +
 // Adam step on the tile's own rows (MODE 2: params are updated in place; a group reads
 // its rows once at staging and writes them once at the end, and rows belong to one tile).
 constexpr int RF_LOSS = 0, RF_GRAD = 1, RF_STEP = 2;
 
-template <int MODE>
+// CL1: every stack has at most one layer, of kind constant or linear (checked per tile): the
+// forward and backward then run out of registers (no composite history, no kind dispatch).
+template <int MODE, bool CL1>
 __global__ void __launch_bounds__(RF_THREADS, 3)
     refine_tiles_kernel(WeftStackSet set, float* __restrict__ params, const float* __restrict__ grad_loss,
                         float* __restrict__ grad, float* __restrict__ loss, int flags, RefinePlan plan, int L,
@@ -414,7 +478,7 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     const int ts = set.size[t];
     const int p0 = set.prim_off[t];
     const int K = set.prim_off[t + 1] - p0;
-    bool ok = ts >= 1 && ts <= 64 && K >= 0 && K <= L;
+    bool ok = ts >= 1 && ts <= 64 && K >= 0 && K <= L && (!CL1 || K <= 1);
     if (resid) ok = ok && (ts == 8 || ts == 16 || ts == 32 || ts == 64);
     if (!ok) {
         if (wig == 0 && lane == 0) {
@@ -456,6 +520,8 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
         }
     group_sync(wpt, grp);
     const Layers S{prep, raw, seg};
+    if (CL1 && K == 1 && gt == 0 && prep[0].kind != K_CONST && prep[0].kind != K_LINEAR && prep[0].kind != K_SKIP)
+        atomicCAS(&g_device_status, 0, WEFTK_E_ARG);  // not a constant/linear layer: treated as absent
 
     const float4* src = reinterpret_cast<const float4*>(set.src) + set.px_off[t];
     const int n = ts * ts;
@@ -492,6 +558,14 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     };
     auto composite = [&](float px, float py, float (&c)[3], float* hrow) {
         c[0] = c[1] = c[2] = 0.0f;
+        if (CL1) {
+            if (K == 1) {
+                const ClEval v = eval_cl(prep[0], px, py);
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) c[ch] = blend(v.s[ch], v.a, 0.0f);
+            }
+            return;
+        }
         for (int k = 0; k < K; ++k) {
             if (hrow) {
                 float* hh = hrow + ((size_t)k * 32 + lane) * 3;
@@ -609,7 +683,52 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
         // ---- backward pass
         const float scale = grad_loss[t] * 2.0f / (3.0f * (float)n);
         float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        for (int cidx = c_begin; cidx < c_end; ++cidx) {
+        float acc[14];
+#pragma unroll
+        for (int i = 0; i < 14; ++i) acc[i] = 0.0f;
+        for (int cidx = c_begin; CL1 && cidx < c_end; ++cidx) {
+            // single constant/linear layer over black: everything in registers
+            const int q = cidx * 32 + lane;
+            const float4 v4 = vn;
+            if (cidx + 1 < c_end) vn = load_src(q + 32);
+            if (q >= n || K == 0) {
+                continue;
+            }
+            int x, y;
+            pixel_of(q, x, y);
+            const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+            const ClEval v = eval_cl(prep[0], px, py);
+            float c[3], e[3], g[3];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) c[ch] = blend(v.s[ch], v.a, 0.0f);
+            e[0] = clamp01(c[0]) - v4.x;
+            e[1] = clamp01(c[1]) - v4.y;
+            e[2] = clamp01(c[2]) - v4.z;
+            if (resid) {
+                float corr[3];
+                correction(x, y, corr);
+                const int j = q >> lbb;
+#pragma unroll
+                for (int ch = 0; ch < 3; ++ch) e[ch] = e[ch] - corr[ch] - hnode[j * 3 + ch];
+            } else {
+                sse += (double)fmaf(e[0], e[0], fmaf(e[1], e[1], e[2] * e[2]));
+            }
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) g[ch] = (c[ch] >= 0.0f && c[ch] <= 1.0f) ? scale * e[ch] : 0.0f;
+            grad_cl(prep[0], raw[0], v, px, py, g, acc);
+        }
+        if (CL1 && K == 1) {
+            const unsigned cols = grad_columns(prep[0].kind);
+#pragma unroll
+            for (int i = 0; i < 14; ++i) {
+                if (!((cols >> i) & 1u)) continue;
+                float s2 = acc[i];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(FULL, s2, o);
+                if (lane == 0) gacc[i] = s2;
+            }
+        }
+        for (int cidx = c_begin; !CL1 && cidx < c_end; ++cidx) {
             const int q = cidx * 32 + lane;
             const bool valid = q < n;
             const float4 v = vn;
@@ -659,7 +778,7 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
                 }
             }
         }
-        if (lane_acc) {
+        if (!CL1 && lane_acc) {
             // lane j sums slot j's 32 lane partials, starting at lane j (no bank conflicts)
             __syncwarp();
             for (int j = lane; j < K * 14; j += 32) {
@@ -752,13 +871,24 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
         plan.cta_end[c] = ctas;
         if (counts[c]) smem = std::max(smem, g * bytes);
     }
-    static int attr = 48 * 1024;
-    if (smem > attr) {
-        WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr = smem;
+    // single constant/linear layers only (declared by the caller, checked per tile): register path
+    const bool cl1 = set.max_prims <= 1 && set.kinds_mask != 0 && (set.kinds_mask & ~0x3) == 0;
+    static int attr[2] = {48 * 1024, 48 * 1024};
+    if (smem > attr[cl1]) {
+        if (cl1)
+            WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE, true>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        else
+            WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE, false>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr[cl1] = smem;
     }
-    refine_tiles_kernel<MODE><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags, plan, L,
-                                                                  adam);
+    if (cl1)
+        refine_tiles_kernel<MODE, true><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags,
+                                                                            plan, L, adam);
+    else
+        refine_tiles_kernel<MODE, false><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss,
+                                                                             flags, plan, L, adam);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }

@@ -374,6 +374,10 @@ class BatchedFit:
                                       _lib.ptr(ti[32]), self.n_items[32], self._stream())
         _lib.check(rc, "weftk_fit_round")
 
+    def init_kinds(self) -> np.ndarray:
+        """Primitive kind of every filled slot of the initial pools (host copy)."""
+        return self._init_kinds[self._init_kinds < 7].astype(np.int32)
+
     # ------------------------------------------------------------------ autotuner
     def configure(self, variants=None, chunks=None) -> "BatchedFit":
         """Set the scoring shape per size class ({8|16|32: variant}) and candidates per CTA

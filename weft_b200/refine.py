@@ -53,8 +53,10 @@ class StackSet:
     """Per-tile stacks over tile pixels resident on the GPU."""
 
     def __init__(self, src: torch.Tensor, px_off: torch.Tensor, sizes: torch.Tensor, prim_off: np.ndarray,
-                 kinds, device: int = 0):
-        """``kinds``: per-row primitive kinds, a numpy array or a device int32 tensor (kept by reference)."""
+                 kinds, device: int = 0, kinds_mask: int | None = None):
+        """``kinds``: per-row primitive kinds, a numpy array or a device int32 tensor (kept by reference).
+        ``kinds_mask`` (bit k = kind k may occur) is derived from a numpy ``kinds``; pass it with a
+        device tensor whose contents change later."""
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
         self.n = int(sizes.numel())
@@ -70,6 +72,9 @@ class StackSet:
         else:
             self.kinds_np = np.asarray(kinds, np.int32)
             self.t_kind = torch.from_numpy(self.kinds_np).to(self.device)
+            if kinds_mask is None:
+                kinds_mask = int(np.bitwise_or.reduce(1 << np.unique(self.kinds_np).astype(np.int64))) \
+                    if self.kinds_np.size else 0
         self.t_prim_off = torch.from_numpy(self.prim_off_np.astype(np.int32)).to(self.device)
         # work split by tile side (largest first): > 32 px eight warps, 17-32 four, 9-16 two, <= 8 one
         sz = sizes.cpu().numpy()
@@ -79,7 +84,7 @@ class StackSet:
         n_big, n_mid, n_s16 = (int(c.sum()) for c in classes[:3])
         self.st = _lib.WeftStackSet(self.n, self.max_prims, _lib.ptr(src), _lib.ptr(px_off), _lib.ptr(sizes),
                                     _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind), _lib.ptr(self.t_order),
-                                    n_big, n_mid, n_s16)
+                                    n_big, n_mid, n_s16, int(kinds_mask or 0))
         n_px = (sizes.to(torch.int64) ** 2)
         self.weights = (n_px.to(torch.float32) / float(n_px.sum().item())) if self.n else n_px.float()
 
@@ -285,7 +290,9 @@ class RefinedFit:
         prim_off = np.concatenate([[0], np.cumsum(has.astype(np.int64))])
         n_rows = int(has.sum())
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
-        self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0)
+        pool_kinds = np.unique(fit.init_kinds())
+        mask = int(np.bitwise_or.reduce(1 << pool_kinds.astype(np.int64))) if pool_kinds.size else 0
+        self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask)
         self.start = torch.zeros((n_rows, 16), dtype=torch.float32, device=dev)
         self.refiner = FusedRefiner(self.ss, self.start, lr=lr, residual=residual)
         self.steps = int(steps)

@@ -103,6 +103,12 @@ typedef struct WeftFitItem {
  * first_new[t] = first pool-local slot to prepare (pass pool_cnt[t] to skip). */
 int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_new, void* stream);
 
+/* Start the fit over: per tile, pool_cnt = d_init_cnt (the initial pools), no selection
+ * (n_sel 0, sel -1, sel_bits 8, objective 0, flags 0), every slot dead and n_alive 0 (a
+ * following weftk_fit_prepare with zero first_new revives the initial pools), the composite bg
+ * zero; the work counters zero.  One launch; no host synchronisation. */
+int weftk_fit_reset(const WeftFitState* st, const int32_t* d_init_cnt, void* stream);
+
 /*
  * Run one fit round over all tiles.
  *   d_perm     [n_slots] pool-local scoring order of each tile's slots (any

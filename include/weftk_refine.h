@@ -86,6 +86,14 @@ int weftk_refine_step(const WeftStackSet* set, float* d_params, float* d_m, floa
                       float* d_loss, float* d_grad_params, float lr, float beta1, float beta2, float eps, int flags,
                       void* stream);
 
+/* Start a refinement from a fit: row r = the first selected primitive of tile d_tiles[r] of the
+ * fit state (weftk_fit.h), as a parameter row projected onto the wire box, its kind in
+ * d_kind[r], and zero Adam moments and step count (d_m, d_v rows).  A tile without a selection
+ * gets an all-zero row of kind -1 (no layer).  One launch. */
+struct WeftFitState;
+int weftk_refine_start(const struct WeftFitState* fit, const int32_t* d_tiles, int n_rows, float* d_params,
+                       float* d_m, float* d_v, int32_t* d_kind, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

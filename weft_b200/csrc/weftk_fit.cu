@@ -456,6 +456,38 @@ extern "C" int weftk_measure_fp32_peak(double* gflops) {
     return WEFTK_OK;
 }
 
+// One CTA per tile: the tile's state, selection row, slots and composite pixels.
+__global__ void fit_reset_kernel(WeftFitState st, const int* __restrict__ init_cnt) {
+    const int t = blockIdx.x;
+    if (t >= st.n_tiles) return;
+    if (t == 0 && threadIdx.x == 0 && st.work != nullptr) {
+        st.work[0] = 0;
+        st.work[1] = 0;
+    }
+    if (threadIdx.x == 0) {
+        st.pool_cnt[t] = init_cnt[t];
+        st.n_alive[t] = 0;
+        st.n_sel[t] = 0;
+        st.sel_bits[t] = 8;
+        st.flags[t] = 0;
+        st.cur_obj[t] = 0.0;
+    }
+    for (int i = threadIdx.x; i < st.cap_max; i += blockDim.x) st.sel[(size_t)t * st.cap_max + i] = -1;
+    const long long off = st.pool_off[t];
+    for (int i = threadIdx.x; i < st.pool_cap[t]; i += blockDim.x) st.alive[off + i] = 0;
+    const int ts = st.size[t];
+    float4* bg = reinterpret_cast<float4*>(st.bg) + st.px_off[t];
+    for (int i = threadIdx.x; i < ts * ts; i += blockDim.x) bg[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+extern "C" int weftk_fit_reset(const WeftFitState* st, const int32_t* d_init_cnt, void* stream) {
+    WEFTK_REQUIRE(st && d_init_cnt, "fit_reset: null argument");
+    if (st->n_tiles == 0) return WEFTK_OK;
+    fit_reset_kernel<<<st->n_tiles, 128, 0, (cudaStream_t)stream>>>(*st, d_init_cnt);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_new, void* stream) {
     WEFTK_REQUIRE(st && d_first_new, "fit_prepare: null argument");
     if (st->n_tiles == 0) return WEFTK_OK;

@@ -31,6 +31,7 @@
 
 #include <algorithm>
 
+#include "../../include/weftk_fit.h"
 #include "../../include/weftk_refine.h"
 #include "weftk_common.cuh"
 #include "weftk_prim.cuh"
@@ -893,6 +894,36 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
     return WEFTK_OK;
 }
 
+// Row r of a refinement started from a fit: thread per (row, column).
+__global__ void refine_start_kernel(WeftFitState fit, const int* __restrict__ tiles, int n_rows,
+                                    float* __restrict__ params, float* __restrict__ m, float* __restrict__ v,
+                                    int* __restrict__ kind_out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_rows * 16) return;
+    const int row = i >> 4, col = i & 15;
+    const int t = tiles[row];
+    m[i] = 0.0f;
+    v[i] = 0.0f;
+    float x = 0.0f;
+    int kind = -1;
+    if (t >= 0 && t < fit.n_tiles && fit.n_sel[t] >= 1) {
+        const int sel = fit.sel[(size_t)t * fit.cap_max];
+        const WeftPrim& P = fit.cand[fit.pool_off[t] + sel];
+        kind = P.kind;
+        if (col < 7) {
+            const bool thick = (kind == K_LINE && col == 4) || (kind == K_CURVE && col == 6);
+            x = fminf(fmaxf(P.geom[col], 0.0f), thick ? 4.0f : 15.0f);
+        } else if (col < 14) {
+            const float c = col < 10 ? P.color0[col - 7] : col < 13 ? P.color1[col - 10] : P.alpha;
+            x = fminf(fmaxf(c, 0.0f), 1.0f);
+        }
+    } else if (t < 0 || t >= fit.n_tiles) {
+        if (col == 0) atomicCAS(&g_device_status, 0, WEFTK_E_ARG);
+    }
+    params[i] = x;
+    if (col == 0) kind_out[row] = kind;
+}
+
 // Adam (PyTorch's rule) + projection onto the wire-representable box, one thread per value.
 __global__ void adam_project_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                                     float* __restrict__ v, const int* __restrict__ kind, int n_rows, float lr,
@@ -918,6 +949,18 @@ extern "C" int weftk_stack_loss(const WeftStackSet* set, const float* d_params, 
     WEFTK_REQUIRE(set && d_loss, "stack_loss: null argument");
     return launch_refine<RF_LOSS>(*set, const_cast<float*>(d_params), nullptr, nullptr, d_loss, flags, AdamArgs{},
                                   (cudaStream_t)stream, "stack_loss");
+}
+
+extern "C" int weftk_refine_start(const WeftFitState* fit, const int32_t* d_tiles, int n_rows, float* d_params,
+                                  float* d_m, float* d_v, int32_t* d_kind, void* stream) {
+    WEFTK_REQUIRE(fit && n_rows >= 0, "refine_start: bad arguments");
+    if (n_rows == 0) return WEFTK_OK;
+    WEFTK_REQUIRE(d_tiles && d_params && d_m && d_v && d_kind, "refine_start: null pointer");
+    const int n = n_rows * 16;
+    refine_start_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*fit, d_tiles, n_rows, d_params, d_m, d_v,
+                                                                            d_kind);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
 }
 
 extern "C" int weftk_adam_step(float* d_params, const float* d_grads, float* d_m, float* d_v, const int32_t* d_kind,

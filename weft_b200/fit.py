@@ -330,19 +330,12 @@ class BatchedFit:
             p = self.pools[t]
             if not isinstance(p, np.ndarray) and len(p) > self.init_cnt[t]:
                 del p[self.init_cnt[t]:]
-        self.kinds[:] = 7
-        self.t_pool_cnt.copy_(torch.from_numpy(self.pool_cnt))
-        self.t_bg.zero_()
-        self.t_n_alive.zero_()
-        self.t_n_sel.zero_()
-        self.t_sel_bits.fill_(8)
-        self.t_flags.zero_()
-        self.t_cur_obj.zero_()
-        self.t_sel.fill_(-1)
-        self.t_alive.zero_()
-        self.t_work.zero_()
         self.kinds[:] = self._init_kinds
-        self._prepare(np.zeros(self.n, np.int32))
+        self._device_consts()
+        _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), self._stream()),
+                   "weftk_fit_reset")
+        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), self._stream()),
+                   "weftk_fit_prepare")
         self.stats = FitStats()
         self.device_reseeded = False
 
@@ -356,16 +349,8 @@ class BatchedFit:
         """Reset and run only the init round (best single candidate per tile), launching
         device work only: no host copies or syncs, so it can be captured in a CUDA graph."""
         self._device_consts()
-        self.t_pool_cnt.copy_(self.t_init_cnt)
-        self.t_bg.zero_()
-        self.t_n_alive.zero_()
-        self.t_n_sel.zero_()
-        self.t_sel_bits.fill_(8)
-        self.t_flags.zero_()
-        self.t_cur_obj.zero_()
-        self.t_sel.fill_(-1)
-        self.t_alive.zero_()
-        self.t_work.zero_()
+        _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), self._stream()),
+                   "weftk_fit_reset")
         _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), self._stream()),
                    "weftk_fit_prepare")
         ti = self.t_items

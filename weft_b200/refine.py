@@ -287,14 +287,15 @@ class RefinedFit:
         dev = fit.device
         has = fit.init_cnt > 0
         self.rows = torch.from_numpy(np.nonzero(has)[0]).to(dev)
+        self.rows32 = self.rows.to(torch.int32)
         prim_off = np.concatenate([[0], np.cumsum(has.astype(np.int64))])
         n_rows = int(has.sum())
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
         pool_kinds = np.unique(fit.init_kinds())
         mask = int(np.bitwise_or.reduce(1 << pool_kinds.astype(np.int64))) if pool_kinds.size else 0
         self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask)
-        self.start = torch.zeros((n_rows, 16), dtype=torch.float32, device=dev)
-        self.refiner = FusedRefiner(self.ss, self.start, lr=lr, residual=residual)
+        self.refiner = FusedRefiner(self.ss, torch.zeros((n_rows, 16), dtype=torch.float32, device=dev), lr=lr,
+                                    residual=residual)
         self.steps = int(steps)
         self.pool_off = torch.from_numpy(fit.pool_off).to(dev)
         self.graph = None
@@ -303,18 +304,25 @@ class RefinedFit:
     def _body(self) -> None:
         f = self.fit
         f.run_init_only()
-        sel = f.t_sel.view(f.n, f.cap_max)[self.rows, 0].to(torch.int64)
-        slots = self.pool_off[self.rows] + sel
-        recs = f.t_cand.view(-1, PRIM_DTYPE.itemsize)[slots]
-        fl = recs.view(torch.float32)
-        self.kinds.copy_(recs.view(torch.int32)[:, 0])
-        self.start[:, 0:7] = fl[:, 1:8]
-        self.start[:, 7:10] = fl[:, 8:11]
-        self.start[:, 10:13] = fl[:, 11:14]
-        self.start[:, 13] = fl[:, 14]
-        self.refiner.restart(self.start)
+        fr = self.refiner
+        _lib.check(self.ss.lib.weftk_refine_start(ctypes_addr(f.st), _lib.ptr(self.rows32), int(self.rows32.numel()),
+                                                  _lib.ptr(fr.p), _lib.ptr(fr.m), _lib.ptr(fr.v),
+                                                  _lib.ptr(self.kinds), self.ss._stream()), "weftk_refine_start")
         for _ in range(self.steps):
-            self.refiner.step()
+            fr.step()
+
+    @property
+    def start(self) -> torch.Tensor:
+        """The starting rows of the last run (the init round's picks, projected)."""
+        f = self.fit
+        rows = torch.zeros_like(self.refiner.p)
+        m = torch.zeros_like(rows)
+        v = torch.zeros_like(rows)
+        kinds = torch.zeros_like(self.kinds)
+        _lib.check(self.ss.lib.weftk_refine_start(ctypes_addr(f.st), _lib.ptr(self.rows32), int(self.rows32.numel()),
+                                                  _lib.ptr(rows), _lib.ptr(m), _lib.ptr(v), _lib.ptr(kinds),
+                                                  self.ss._stream()), "weftk_refine_start")
+        return rows
 
     def run(self) -> torch.Tensor:
         if not self.use_graph:

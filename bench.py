@@ -408,6 +408,109 @@ def refined_breakdown(args, rf, fast, lib, stream):
     return score_ms.value, n_score.value, step_ms, fast.work_counters()
 
 
+def differentiable_fit(args, executor, local, stream):
+    """The differentiable-fit workload: a 2048x2048 synthetic image of 2500 primitives, the plain
+    batched fit, then ``--diff-steps`` Adam steps (lr 1e-2, FP32 parameters and moments) on the
+    fitted stacks through the autograd.Function (torch Adam) and, separately, through the fused
+    one-launch step; RD of the files before and after."""
+    import torch
+
+    from weft_b200.batch import ImageBatch, prepare_image
+    from weft_b200.refine import FusedRefiner, refine
+
+    size, n_prims = 2048, 2500
+    t0 = time.perf_counter()
+    im = prepare_image(make_image_u8(size, size, n_prims, 0), QUALITY, executor)
+    cand_s = time.perf_counter() - t0
+    batch = ImageBatch([im], QUALITY, CAP, device=local)
+    fit = batch.plain_fit()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b)
+
+    fit.reset()
+    fit.run()  # warm-up
+    fit.reset()
+    _, plain_ms = timed(fit.run)
+    ss, p0 = fit.stack_set()
+    steps = args.diff_steps
+    refine(ss, p0, steps=3, lr=1e-2)  # warm-up
+    (out, hist), auto_ms = timed(lambda: refine(ss, p0, steps=steps, lr=1e-2))
+    fr = FusedRefiner(ss, p0, lr=1e-2)
+    fr.run(3)
+    fr.restart(p0)
+    _, fused_ms = timed(lambda: fr.run(steps))
+    rd0 = batch.rd_per_image(ss.to_stacks(ss.quantize(p0)))[0]
+    rd1 = batch.rd_per_image(ss.to_stacks(ss.quantize(out)))[0]
+    return {"image": f"{size}x{size}, {n_prims} prims, seed 0", "tiles": len(im.tiles),
+            "stack_rows": int(p0.shape[0]), "max_prims": ss.max_prims, "cand_gen_s": cand_s,
+            "plain_fit_ms": plain_ms, "adam_steps": steps, "lr": 1e-2,
+            "autograd_ms_per_step": auto_ms / steps, "fused_ms_per_step": fused_ms / steps,
+            "loss_first_last": [hist[0], hist[-1]] if hist else None,
+            "rd_plain": rd0["rd_score"], "rd_refined": rd1["rd_score"], "rd_delta_db": rd1["rd_score"] - rd0["rd_score"],
+            "psnr_plain_db": rd0["psnr_db"], "psnr_refined_db": rd1["psnr_db"]}
+
+
+def image_batch_fit(args, executor, local, stream):
+    """The multi-image workload (``--batch-images``, e.g. "16x256,16x512,16x1024,16x2048"): images
+    of the canonical generator (seeds 0.., primitives scaled with area, 50-2500), all tiles in one
+    plain batched fit and in one refined fit; MPix/s of both and each image's RD."""
+    import torch
+
+    from weft_b200.batch import ImageBatch, prepare_image
+
+    specs = []
+    for part in args.batch_images.split(","):
+        n, side = part.lower().split("x")
+        specs += [int(side)] * int(n)
+    ims = []
+    t0 = time.perf_counter()
+    for seed, side in enumerate(specs):
+        n_prims = int(min(2500, max(50, round(2500 * (side / 2048) ** 2))))
+        ims.append(prepare_image(make_image_u8(side, side, n_prims, seed), QUALITY, executor))
+    cand_s = time.perf_counter() - t0
+    batch = ImageBatch(ims, QUALITY, CAP, device=local)
+    n_px = batch.n_pixels
+
+    def timed(fn, reps=1):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            r = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b) / reps
+
+    fit = batch.plain_fit()
+    fit.run()
+
+    def plain_step():
+        fit.reset()
+        fit.run()
+
+    _, plain_ms = timed(plain_step)
+    ss, p = fit.stack_set()
+    plain_rd = batch.rd_per_image(ss.to_stacks(ss.quantize(p)))
+    rf = batch.refined_fit(steps=args.refine_steps, lr=args.refine_lr)
+    rf.run()
+    rows, ref_ms = timed(rf.run, 3)
+    ref_rd = batch.rd_per_image(rf.ss.to_stacks(rf.ss.quantize(rows)))
+    deltas = [b["rd_score"] - a["rd_score"] for a, b in zip(plain_rd, ref_rd)]
+    return {"images": args.batch_images, "n_images": len(ims), "mpix": n_px / 1e6, "tiles": int(batch.tile_off[-1]),
+            "cand_gen_s": cand_s, "plain_ms": plain_ms, "plain_mpix_per_s": n_px / (plain_ms * 1e-3) / 1e6,
+            "refined_ms": ref_ms, "refined_mpix_per_s": n_px / (ref_ms * 1e-3) / 1e6,
+            "refined": f"{args.refine_pool} init round + {args.refine_steps} fused Adam steps, one CUDA graph",
+            "rd_delta_db_min": min(deltas), "rd_delta_db_mean": float(np.mean(deltas)),
+            "images_within_0.05db": int(sum(d >= -0.05 for d in deltas))}
+
+
 def _hbm_peak() -> tuple[float, str]:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -479,6 +582,10 @@ def main():
                     help="refined fits whose RD is reported, pool:adam_steps[:r] (r: decoded-error loss)")
     ap.add_argument("--refine-reps", type=int, default=5)
     ap.add_argument("--refine-lr", type=float, default=1e-2)
+    ap.add_argument("--diff-steps", type=int, default=200,
+                    help="Adam steps of the 2048^2 differentiable fit (0: skip that workload)")
+    ap.add_argument("--batch-images", default="",
+                    help='multi-image batch, e.g. "16x256,16x512,16x1024,16x2048" (empty: skip)')
     args = ap.parse_args()
 
     # Process pools first: spawned before any CUDA initialisation.
@@ -634,7 +741,8 @@ def run_weft(args, world, rank, local, executor, cores):
     init_tflops = r_work[1] / (r_score_ms * 1e-3) / 1e12 if r_score_ms > 0 else 0.0
     refine_share = args.refine_steps * r_step_ms
     n_cls = sum(1 for k in (8, 16, 32) if fast.n_items[k])
-    ref_launches = 1 + 3 + n_cls + args.refine_steps  # prepare, begin/select/end + scoring, refine steps
+    # reset, prepare, begin, select, end, scoring (one per size class), refine start, refine steps
+    ref_launches = 6 + n_cls + args.refine_steps
 
     def refined_e2e():
         from weft_b200.refine import RefinedFit
@@ -644,6 +752,9 @@ def run_weft(args, world, rank, local, executor, cores):
         return int(pixels.nbytes + frec.nbytes + sizes.nbytes + fcnt.nbytes), int(out_rows.numel() * 4)
 
     ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
+
+    diff = differentiable_fit(args, executor, local, stream) if args.diff_steps > 0 and rank == 0 else None
+    ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -708,6 +819,8 @@ def run_weft(args, world, rank, local, executor, cores):
                              for k, v in (fast.tuning or {}).items()},
         "decode": decode,
         "decode_with_residuals": decode_res,
+        "differentiable_fit": diff,
+        "image_batch": ibatch,
         "rd": rd,
     }
     print(json.dumps(line), flush=True)

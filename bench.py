@@ -626,41 +626,33 @@ def run_weft(args, world, rank, local, executor, cores):
     n_px = int(sum(p.shape[0] ** 2 for p in patches))
     stream = torch.cuda.current_stream()
 
-    def step():
-        fit.reset()
-        fit.run()
-
+    # the whole greedy fit (init, rounds, device re-seeds) replayed from one CUDA graph
+    fit_graph = fit.graph()
     for _ in range(args.warmup):
-        step()
+        fit_graph.replay()
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-    lib.weftk_fit_timing(1, None, None)
     sampler = ClockSampler(local)
     sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    work = []
-    rounds = []
     n_classes = sum(1 for k in (8, 16, 32) if fit.n_items[k])
     torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(args.steps):
-        step()
-        work.append(fit.work_counters())
-        rounds.append(len(fit.stats.per_round))
+        fit_graph.replay()
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    # kernels per step: one prepare at reset and per re-seed, and per round
-    # begin + scoring (one per tile-size class) + select + end
-    launches_per_step = 1 + fit.stats.reseeds + len(fit.stats.per_round) * (3 + n_classes)
+    ctl = fit.control()
+    max_rounds = rate.max_rounds(QUALITY)
+    # kernels per step: reset, prepare; init round: begin, scoring per class, select, end; every
+    # greedy round (run or skipped): begin, scoring per class, select, end, control, re-seed
+    launches_per_step = 2 + (3 + n_classes) + max_rounds * (5 + n_classes)
     import ctypes
 
-    score_ms = ctypes.c_double(0)
-    n_score = ctypes.c_int(0)
-    lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
     ms_total = ev0.elapsed_time(ev1)
     ms_step = ms_total / args.steps
     if world > 1:
@@ -670,16 +662,28 @@ def run_weft(args, world, rank, local, executor, cores):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step = float(t.item())
     value = world * n_px / (ms_step * 1e-3) / 1e6
+    # scoring-kernel time: one host-driven run of the same fit with events around the scoring
+    # launches (the graph cannot host-synchronise); the same kernels and work
+    fit.reset()
+    lib.weftk_fit_timing(1, None, None)
+    fit.run()
+    torch.cuda.synchronize()
+    score_ms = ctypes.c_double(0)
+    n_score = ctypes.c_int(0)
+    lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
+    work = [fit.work_counters()]
+    rounds = [len(fit.stats.per_round)]
+    score_ms.value *= args.steps  # per-step figures below divide by the step count
 
     # roofline of the scoring kernels (FP32-bound): algorithmic ops / scoring device time
-    ops = sum(w[1] for w in work)
+    ops = sum(w[1] for w in work) * args.steps
     score_s = score_ms.value * 1e-3
     achieved_tflops = ops / score_s / 1e12 if score_s > 0 else 0.0
     peak = ctypes.c_double(0)
     _lib.check(lib.weftk_measure_fp32_peak(ctypes.addressof(peak)), "weftk_measure_fp32_peak")
     peak_tflops = peak.value / 1e3
     # bytes the scoring kernels must move per launch: src+bg per pixel per item, prep per candidate
-    cand_px = sum(w[0] for w in work)
+    cand_px = sum(w[0] for w in work) * args.steps
 
     # RD of the fitted primitives (PRIM-only reconstruction)
     sel = fit.selected()
@@ -809,7 +813,8 @@ def run_weft(args, world, rank, local, executor, cores):
                    "plain_bpp": plain_rd["bpp"], "refined_bpp": ref_rd["bpp"], "tolerance_db": 0.05},
         "plain": {"value": plain_value, "ms_per_step": plain_ms, "e2e": plain_e2e_val, "roofline": score_roof,
                   "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
-                  "rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds,
+                  "rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds, "graph_control": ctl,
+                  "fit": "whole greedy (init, rounds, device re-seeds) replayed from one CUDA graph",
                   "reseed_host_s": fit.stats.t_reseed_s, "cand_gen_s": cand_s,
                   "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
                   "prim_payload_bytes": prim_bytes,

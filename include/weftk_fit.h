@@ -103,6 +103,17 @@ typedef struct WeftFitItem {
  * first_new[t] = first pool-local slot to prepare (pass pool_cnt[t] to skip). */
 int weftk_fit_prepare(const WeftFitState* st, const int32_t* d_first_new, void* stream);
 
+/* The whole greedy fit, enqueued without any host synchronisation (so it can be captured in a
+ * CUDA graph): the init round, then max_rounds greedy rounds whose kernels skip their work once
+ * the fit is over, with the host loop's decisions taken on the device after every round
+ * (src/weft/encoder.py:2745-2830: a round that evaluates no tile ends the fit; a round without
+ * improvement is a stall; more than three stalls end it; otherwise a stall re-seeds the complex
+ * tiles on the device).  d_ctl: int32[4] scratch (done, stalls, re-seed pending, rounds run),
+ * readable after the stream completes.  Requires scoring timing off (weftk_fit_timing). */
+int weftk_fit_run(const WeftFitState* st, int max_rounds, double lambda, double complex_threshold,
+                  const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8, const WeftFitItem* d_items16,
+                  int n_items16, const WeftFitItem* d_items32, int n_items32, int32_t* d_ctl, void* stream);
+
 /* Start the fit over: per tile, pool_cnt = d_init_cnt (the initial pools), no selection
  * (n_sel 0, sel -1, sel_bits 8, objective 0, flags 0), every slot dead and n_alive 0 (a
  * following weftk_fit_prepare with zero first_new revives the initial pools), the composite bg

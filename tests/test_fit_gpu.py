@@ -121,3 +121,32 @@ def test_autotune_keeps_the_reference_selection(golden):
     queue = {k: list(v) for k, v in reseeds.items()}
     fit.run(reseed=lambda i, patch, pred: queue[i].pop(0))
     assert fit.selected_indices() == [[int(v) for v in row if v >= 0] for row in g["selected"]]
+
+
+def test_device_driven_fit_equals_host_loop_and_replays():
+    """The whole fit enqueued without host synchronisation (and replayed from a CUDA graph)
+    takes the host loop's decisions: same selections and objectives as run() with device
+    re-seeding, on 8/16/32/64-px tiles at q=92 (re-seeds happen)."""
+    from weft_b200 import candidates, quadtree
+    from weft_b200.fit import BatchedFit
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 64, 3, 3)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    pools = [candidates.tile_candidates(p, 92) for p in patches]
+    fit = BatchedFit(patches, pools, 92, caps=[16] * len(qts))
+    fit.run()
+    want_sel, want_obj, want_rounds = fit.selected_indices(), fit.objectives(), fit.stats.rounds
+    assert fit.stats.reseeds > 0
+    fit.reset()
+    fit.run_device()
+    assert fit.selected_indices() == want_sel
+    np.testing.assert_array_equal(fit.objectives(), want_obj)
+    assert fit.control()["rounds"] == want_rounds
+    g = fit.graph()
+    for _ in range(2):
+        g.replay()
+        assert fit.selected_indices() == want_sel
+        np.testing.assert_array_equal(fit.objectives(), want_obj)

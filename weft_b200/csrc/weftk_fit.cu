@@ -94,12 +94,17 @@ __global__ void fit_prepare_kernel(WeftFitState st, const int* __restrict__ firs
 }
 
 // ------------------------------------------------------------------ round begin / end
-__global__ void fit_begin_kernel(WeftFitState st, int mode) {
+// ctl (device-driven fit, may be NULL): [0] done, [1] stalls, [2] re-seed pending, [3] rounds.
+__global__ void fit_begin_kernel(WeftFitState st, int mode, int* ctl) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= st.n_tiles) return;
+    const bool done = ctl != nullptr && ctl[0] != 0;
+    if (ctl != nullptr && t == 0) ctl[2] = 0;  // the pending re-seed (if any) ran before this launch
     int f = st.flags[t] & ~(WEFTK_TILE_EVAL | WEFTK_TILE_IMPROVED);
     bool ev;
-    if (mode == WEFTK_FIT_INIT)
+    if (done)
+        ev = false;
+    else if (mode == WEFTK_FIT_INIT)
         ev = st.n_alive[t] > 0;
     else
         ev = (f & WEFTK_TILE_COMPLEX) && st.n_alive[t] > 0 && st.n_sel[t] < st.cap[t];
@@ -108,6 +113,27 @@ __global__ void fit_begin_kernel(WeftFitState st, int mode) {
         atomicAdd(&st.status[0], 1);
     }
     st.flags[t] = f;
+}
+
+// The host loop's decisions after a greedy round, on the device (src/weft/encoder.py:2745-2830):
+// no evaluated tile ends the fit; a round without improvement is a stall, more than three
+// stalls end it, otherwise a stall triggers a re-seed; an improving round resets the count.
+__global__ void fit_control_kernel(const int* __restrict__ status, int* ctl) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || ctl[0]) return;
+    if (status[0] == 0) {
+        ctl[0] = 1;
+        return;
+    }
+    ctl[3] += 1;
+    if (status[1] == 0) {
+        ctl[1] += 1;
+        if (ctl[1] > 3)
+            ctl[0] = 1;
+        else
+            ctl[2] = 1;
+    } else {
+        ctl[1] = 0;
+    }
 }
 
 __global__ void fit_end_kernel(WeftFitState st, int mode, double complex_threshold) {
@@ -567,6 +593,35 @@ extern "C" int weftk_fit_variant(int size_class, int variant, int* pixels_per_la
     return WEFTK_OK;
 }
 
+// Control block of the device-driven fit for the round being enqueued (host thread state:
+// set only while weftk_fit_run enqueues its rounds).
+static thread_local int* g_round_ctl = nullptr;
+
+int launch_fit_reseed(const WeftFitState& st, const int* gate, cudaStream_t stream);
+
+extern "C" int weftk_fit_run(const WeftFitState* st, int max_rounds, double lambda, double complex_threshold,
+                             const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
+                             const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
+                             int n_items32, int32_t* d_ctl, void* stream) {
+    WEFTK_REQUIRE(st && d_ctl && max_rounds >= 0, "fit_run: bad arguments");
+    WEFTK_REQUIRE(!g_timing.enabled, "fit_run: scoring timing is host-synchronised; disable it first");
+    cudaStream_t s = (cudaStream_t)stream;
+    WEFTK_CUDA(cudaMemsetAsync(d_ctl, 0, 4 * sizeof(int32_t), s));
+    int rc = weftk_fit_round(st, WEFTK_FIT_INIT, lambda, complex_threshold, d_perm, d_items8, n_items8, d_items16,
+                             n_items16, d_items32, n_items32, stream);
+    for (int r = 0; !rc && r < max_rounds; ++r) {
+        g_round_ctl = d_ctl;
+        rc = weftk_fit_round(st, WEFTK_FIT_ROUND, lambda, complex_threshold, d_perm, d_items8, n_items8, d_items16,
+                             n_items16, d_items32, n_items32, stream);
+        g_round_ctl = nullptr;
+        if (rc) break;
+        fit_control_kernel<<<1, 32, 0, s>>>(st->status, d_ctl);
+        rc = launch_fit_reseed(*st, d_ctl + 2, s);
+    }
+    if (!rc) WEFTK_CUDA(cudaGetLastError());
+    return rc;
+}
+
 extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double complex_threshold,
                                const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
                                const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
@@ -580,7 +635,7 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
     cudaStream_t s = (cudaStream_t)stream;
     const int nt = st->n_tiles;
     WEFTK_CUDA(cudaMemsetAsync(st->status, 0, 4 * sizeof(int32_t), s));
-    fit_begin_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(*st, mode);
+    fit_begin_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(*st, mode, g_round_ctl);
     if (g_timing.enabled) {
         int rc = timing_collect();
         if (rc) return rc;

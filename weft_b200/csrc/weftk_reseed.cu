@@ -93,11 +93,12 @@ __device__ void add_cand(RsShared& s, int kind, const double* g, int ng, const f
     s.n_cand = i + 1;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) fit_reseed_kernel(WeftFitState st) {
+__global__ void __launch_bounds__(RS_THREADS) fit_reseed_kernel(WeftFitState st, const int* gate) {
     extern __shared__ float dyn[];
     __shared__ RsShared s;
     const int t = blockIdx.x;
     if (t >= st.n_tiles) return;
+    if (gate != nullptr && *gate == 0) return;  // device-driven fit: no stall this round
     if (!(st.flags[t] & WEFTK_TILE_COMPLEX) || st.n_sel[t] >= st.cap[t]) return;
     const int ts = st.size[t], n = ts * ts, tid = threadIdx.x;
     const double wf = ts - 1, hf = ts - 1;
@@ -403,17 +404,21 @@ __global__ void __launch_bounds__(RS_THREADS) fit_reseed_kernel(WeftFitState st)
 
 using namespace weftk;
 
-extern "C" int weftk_fit_reseed(const WeftFitState* st, int quality, void* stream) {
-    (void)quality;
-    WEFTK_REQUIRE(st, "fit_reseed: null state");
-    if (st->n_tiles == 0) return WEFTK_OK;
+int launch_fit_reseed(const WeftFitState& st, const int* gate, cudaStream_t stream) {
+    if (st.n_tiles == 0) return WEFTK_OK;
     const int smem = 2 * 64 * 64 * (int)sizeof(float);
     static bool attr_set = false;
     if (!attr_set) {
         WEFTK_CUDA(cudaFuncSetAttribute(fit_reseed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr_set = true;
     }
-    fit_reseed_kernel<<<st->n_tiles, RS_THREADS, smem, (cudaStream_t)stream>>>(*st);
+    fit_reseed_kernel<<<st.n_tiles, RS_THREADS, smem, stream>>>(st, gate);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
+}
+
+extern "C" int weftk_fit_reseed(const WeftFitState* st, int quality, void* stream) {
+    (void)quality;
+    WEFTK_REQUIRE(st, "fit_reseed: null state");
+    return launch_fit_reseed(*st, nullptr, (cudaStream_t)stream);
 }

@@ -359,6 +359,35 @@ class BatchedFit:
                                       _lib.ptr(ti[32]), self.n_items[32], self._stream())
         _lib.check(rc, "weftk_fit_round")
 
+    def run_device(self, max_rounds: int | None = None) -> "BatchedFit":
+        """Reset and run the whole fit with device re-seeding, enqueued without any host
+        synchronisation (``weftk_fit_run``), so it can be captured in a CUDA graph.  Same
+        decisions as ``run()`` with device re-seeding; ``control()`` reads the outcome."""
+        self._device_consts()
+        if not hasattr(self, "t_ctl"):
+            self.t_ctl = torch.zeros(4, dtype=torch.int32, device=self.device)
+        s = self._stream()
+        _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), s), "weftk_fit_reset")
+        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), s),
+                   "weftk_fit_prepare")
+        rounds = rate.max_rounds(self.quality) if max_rounds is None else int(max_rounds)
+        ti = self.t_items
+        rc = self.lib.weftk_fit_run(ctypes_ref(self.st), rounds, self.lam, self.thr, _lib.ptr(self.t_perm),
+                                    _lib.ptr(ti[8]), self.n_items[8], _lib.ptr(ti[16]), self.n_items[16],
+                                    _lib.ptr(ti[32]), self.n_items[32], _lib.ptr(self.t_ctl), s)
+        _lib.check(rc, "weftk_fit_run")
+        self.device_reseeded = True
+        return self
+
+    def control(self) -> dict:
+        """Outcome of the last ``run_device``: rounds run, stall count, whether it ended early."""
+        c = self.t_ctl.cpu().numpy()
+        return {"done": bool(c[0]), "stalls": int(c[1]), "rounds": int(c[3])}
+
+    def graph(self, max_rounds: int | None = None) -> "FitGraph":
+        """The device-driven fit captured once in a CUDA graph (replay() refits from scratch)."""
+        return FitGraph(self, max_rounds)
+
     def init_kinds(self) -> np.ndarray:
         """Primitive kind of every filled slot of the initial pools (host copy)."""
         return self._init_kinds[self._init_kinds < 7].astype(np.int32)
@@ -514,6 +543,26 @@ class BatchedFit:
             a = int(self.px_off[t])
             out.append(bg[a:a + s * s, :3].reshape(s, s, 3))
         return out
+
+
+class FitGraph:
+    """``BatchedFit.run_device`` captured in one CUDA graph: every replay resets the fit and runs
+    the init round, the greedy rounds and the device re-seeds with no host round trip."""
+
+    def __init__(self, fit: BatchedFit, max_rounds: int | None = None):
+        self.fit = fit
+        side = torch.cuda.Stream(fit.device)
+        side.wait_stream(torch.cuda.current_stream(fit.device))
+        with torch.cuda.stream(side):
+            fit.run_device(max_rounds)  # warm-up outside capture (lazy state, kernel attributes)
+        torch.cuda.current_stream(fit.device).wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            fit.run_device(max_rounds)
+
+    def replay(self) -> BatchedFit:
+        self.graph.replay()
+        return self.fit
 
 
 def ctypes_ref(st) -> int:

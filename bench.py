@@ -808,10 +808,12 @@ def run_weft(args, world, rank, local, executor, cores):
         "cpu_baseline": cpu,
         "clocks": clocks2 if iso else clocks,
         "gpu_launches": (ref_launches if iso else launches_per_step) * args.steps,
+        "tiles_per_s": len(tiles) * world / (head_ms * 1e-3),
         "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
                    "plain_psnr_db": plain_rd["psnr_db"], "refined_psnr_db": ref_rd["psnr_db"],
                    "plain_bpp": plain_rd["bpp"], "refined_bpp": ref_rd["bpp"], "tolerance_db": 0.05},
-        "plain": {"value": plain_value, "ms_per_step": plain_ms, "e2e": plain_e2e_val, "roofline": score_roof,
+        "plain": {"value": plain_value, "ms_per_step": plain_ms, "tiles_per_s": len(tiles) * world / (plain_ms * 1e-3),
+                  "e2e": plain_e2e_val, "roofline": score_roof,
                   "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
                   "rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds, "graph_control": ctl,
                   "fit": "whole greedy (init, rounds, device re-seeds) replayed from one CUDA graph",

@@ -228,6 +228,20 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
         b.record(stream)
         torch.cuda.synchronize()
         times.append(a.elapsed_time(b))
+    # reference: a plain streaming write of the same output buffer, timed the same way
+    fill_times = []
+    for _ in range(max(iters, 3)):
+        flush.fill_(1.0)
+        torch.cuda._sleep(100000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out.fill_(0.5)
+        b.record(stream)
+        torch.cuda.synchronize()
+        fill_times.append(a.elapsed_time(b))
+    fill_ms = statistics.median(fill_times)
+    launch()  # the timed output, not the fill, is what the status check follows
+    torch.cuda.synchronize()
     st = ctypes.c_int(0)
     _lib.check(lib.weftk_device_status(ctypes.addressof(st)), "weftk_device_status")
     if st.value:
@@ -239,6 +253,9 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
     return {"target": f"{tw}x{th}", "ms": ms, "mpix_per_s": tw * th / (ms * 1e-3) / 1e6, "bytes": nbytes,
             "achieved_gbs": gbs, "peak_gbs": peak_gbs, "frac": gbs / peak_gbs,
             "peak_source": peak_source,
+            "fill_reference": {"ms": fill_ms, "gbs": 12 * tw * th / (fill_ms * 1e-3) / 1e9,
+                               "what": "torch fill_ of the same output buffer, timed the same way"},
+            "frac_of_fill": (12 * tw * th / (ms * 1e-3)) / (12 * tw * th / (fill_ms * 1e-3)),
             "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims)),
             "residuals": "RES0 + RES1 grids" if n_res1 else "none"}
 

@@ -224,6 +224,86 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
             const int side = max(w, h);
             const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
             const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
+            if (n == 1 && sp[0].kind == K_CONST) {
+                // A lone constant layer is one colour before RES1 (the blend over black and the RES0
+                // add are the general path's operations, done once per item), so the walk only
+                // writes it, or adds the bilinear RES1 grid per pixel.  Each lane steps its group
+                // (row, column) by 32 groups per chunk instead of dividing.
+                const float fr = clamp01(blend(sp[0].cr, sp[0].a, 0.0f) + d.res0_r);
+                const float fg = clamp01(blend(sp[0].cg, sp[0].a, 0.0f) + d.res0_g);
+                const float fb = clamp01(blend(sp[0].cb, sp[0].a, 0.0f) + d.res0_b);
+                const int x0 = d.target_x0, x1 = d.target_x0 + w;
+                const int g0 = item.y * 32 + lane, drow = 32 / G, dcol = 32 - drow * G;
+                int row = g0 / G, col = g0 - row * G;
+                for (int chunk = item.y; chunk < c_end; ++chunk, row += drow, col += dcol) {
+                    if (col >= G) {
+                        col -= G;
+                        ++row;
+                    }
+                    const int gy = d.target_y0 + row;
+                    if (row >= h || gy < 0 || gy >= H) continue;
+                    const int gxs = (a0 + col) * 4;
+                    float* dst = out + ((size_t)gy * W + gxs) * 3;
+                    const bool full = w_aligned && gxs >= x0 && gxs + DEC_PPL <= x1 && gxs >= 0 && gxs + DEC_PPL <= W;
+                    float o[DEC_PPL][3];
+                    if (!has_res1) {
+                        if (full) {
+                            float4* d4 = reinterpret_cast<float4*>(dst);
+                            d4[0] = make_float4(fr, fg, fb, fr);
+                            d4[1] = make_float4(fg, fb, fr, fg);
+                            d4[2] = make_float4(fb, fr, fg, fb);
+                            continue;
+                        }
+#pragma unroll
+                        for (int j = 0; j < DEC_PPL; ++j) {
+                            o[j][0] = fr;
+                            o[j][1] = fg;
+                            o[j][2] = fb;
+                        }
+                    } else {
+                        // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
+                        const float gyf =
+                            fminf(fmaxf(__fsub_rn(__fmul_rn((float)row + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                        const int ry0 = (int)floorf(gyf), ry1 = min(ry0 + 1, 3);
+                        const float wy = __fsub_rn(gyf, (float)ry0);
+#pragma unroll
+                        for (int j = 0; j < DEC_PPL; ++j) {
+                            const int lxc = min(max(gxs + j - x0, 0), w - 1);
+                            const float gx =
+                                fminf(fmaxf(__fsub_rn(__fmul_rn((float)lxc + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                            const int rx0 = (int)floorf(gx), rx1 = min(rx0 + 1, 3);
+                            const float wx = __fsub_rn(gx, (float)rx0);
+                            const float base[3] = {fr, fg, fb};
+#pragma unroll
+                            for (int ch = 0; ch < 3; ++ch) {
+                                const float c00 = grid[(ry0 * 4 + rx0) * 3 + ch], c01 = grid[(ry0 * 4 + rx1) * 3 + ch];
+                                const float c10 = grid[(ry1 * 4 + rx0) * 3 + ch], c11 = grid[(ry1 * 4 + rx1) * 3 + ch];
+                                const float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
+                                const float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
+                                o[j][ch] = clamp01(base[ch] + __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)),
+                                                                        __fmul_rn(bot, wy)));
+                            }
+                        }
+                        if (full) {
+                            float4* d4 = reinterpret_cast<float4*>(dst);
+                            d4[0] = make_float4(o[0][0], o[0][1], o[0][2], o[1][0]);
+                            d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
+                            d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
+                            continue;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < DEC_PPL; ++j) {
+                        const int gxp = gxs + j;
+                        if (gxp >= x0 && gxp < x1 && gxp >= 0 && gxp < W) {
+                            dst[3 * j] = o[j][0];
+                            dst[3 * j + 1] = o[j][1];
+                            dst[3 * j + 2] = o[j][2];
+                        }
+                    }
+                }
+                continue;
+            }
             for (int chunk = item.y; chunk < c_end; ++chunk) {
                 const int g = chunk * 32 + lane;
                 const bool g_ok = g < n_groups;
@@ -236,7 +316,7 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
                 float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
                 int lx[DEC_PPL];
                 bool valid[DEC_PPL];
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < DEC_PPL; ++j) {
                     lx[j] = gxs + j - d.target_x0;
                     valid[j] = g_ok && lx[j] >= 0 && lx[j] < w;
@@ -260,7 +340,7 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
                         if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
                         float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
                         prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
-    #pragma unroll
+#pragma unroll
                         for (int j = 0; j < DEC_PPL; ++j) {
                             cr[j] = blend(sr[j], a[j], cr[j]);
                             cg[j] = blend(sg[j], a[j], cg[j]);
@@ -269,7 +349,7 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
                     }
                 }
                 float o[DEC_PPL][3];
-    #pragma unroll
+#pragma unroll
                 for (int j = 0; j < DEC_PPL; ++j) {
                     float r = clamp01(cr[j] + d.res0_r), gg = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
                     if (has_res1) {
@@ -280,7 +360,7 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
                         float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
                         int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
                         float v[3];
-    #pragma unroll
+#pragma unroll
                         for (int ch = 0; ch < 3; ++ch) {
                             float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
                             float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
@@ -305,7 +385,7 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
                     d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
                     d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
                 } else {
-    #pragma unroll
+#pragma unroll
                     for (int j = 0; j < DEC_PPL; ++j) {
                         const int gxp = gxs + j;
                         if (valid[j] && gxp >= 0 && gxp < W) {

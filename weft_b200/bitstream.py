@@ -267,7 +267,46 @@ def encode_weft(width: int, height: int, quality: int, tiles, stacks, residuals=
     return bytes(header + directory + payload)
 
 
-def decode_weft(blob: bytes) -> WeftFile:
+def decode_prim_chunks_gpu(prim: bytes, entries, out_len: int, device: int = 0) -> bytes:
+    """The PRIM payload's chunks decoded on the GPU (``weftk_rans_decode_chunks``, one warp per
+    chunk); ``entries`` are CIDX rows (start_tile, tile_count, raw_off, raw_len, coded_off, coded_len)."""
+    import torch
+
+    from . import _lib
+
+    lib = _lib.lib_for_device(device)
+    d = torch.device("cuda", device)
+    ent = np.array([(e[4], e[5], e[2], e[3]) for e in entries], np.int64).reshape(-1, 4)
+    t_pay = torch.from_numpy(np.frombuffer(prim, np.uint8).copy()).to(d) if len(prim) else \
+        torch.zeros(1, dtype=torch.uint8, device=d)
+    t_ent = torch.from_numpy(ent).to(d)
+    t_out = torch.zeros(max(out_len, 1), dtype=torch.uint8, device=d)
+    status = ctypes_int()
+    lib.weftk_device_status(ctypes_addr_of(status))  # clear any earlier report
+    rc = lib.weftk_rans_decode_chunks(_lib.ptr(t_pay), len(prim), _lib.ptr(t_ent), len(ent), _lib.ptr(t_out),
+                                      out_len, torch.cuda.current_stream(d).cuda_stream)
+    _lib.check(rc, "weftk_rans_decode_chunks")
+    out = t_out[:out_len].cpu().numpy().tobytes()
+    _lib.check(lib.weftk_device_status(ctypes_addr_of(status)), "weftk_device_status")
+    if status.value:
+        raise ValueError("a PRIM chunk does not parse")
+    return out
+
+
+def ctypes_int():
+    import ctypes
+
+    return ctypes.c_int(0)
+
+
+def ctypes_addr_of(v) -> int:
+    import ctypes
+
+    return ctypes.addressof(v)
+
+
+def decode_weft(blob: bytes, device: int | None = None) -> WeftFile:
+    """Parse a WEFT file; with ``device`` the PRIM chunks are entropy-decoded on that GPU."""
     magic, major, minor, n_blocks, _ = struct.unpack_from("<4sBBHI", blob, 0)
     if magic != MAGIC or major != MAJOR:
         raise ValueError("not a WEFT v1 file")
@@ -286,7 +325,11 @@ def decode_weft(blob: bytes) -> WeftFile:
     n_toc = struct.unpack_from("<I", blocks[b"TOC "], 0)[0]
     toc = list(np.frombuffer(blocks[b"TOC "], "<u4", n_toc, 4).astype(np.int64))
     prim = blocks[b"PRIM"]
-    if b"CIDX" in blocks:
+    if b"CIDX" in blocks and device is not None:
+        nc = struct.unpack_from("<I", blocks[b"CIDX"], 0)[0]
+        entries = [struct.unpack_from("<IIIIII", blocks[b"CIDX"], 4 + 24 * i) for i in range(nc)]
+        prim_raw = decode_prim_chunks_gpu(prim, entries, int(toc[-1]) if toc else 0, device)
+    elif b"CIDX" in blocks:
         nc = struct.unpack_from("<I", blocks[b"CIDX"], 0)[0]
         raw = bytearray(toc[-1] if toc else 0)
         for i in range(nc):

@@ -86,6 +86,14 @@ int weftk_refine_step(const WeftStackSet* set, float* d_params, float* d_m, floa
                       float* d_loss, float* d_grad_params, float lr, float beta1, float beta2, float eps, int flags,
                       void* stream);
 
+/* `steps` refinement steps in one launch: each tile group repeats weftk_refine_step's work on
+ * its own rows (tiles never interact), keeping the rows and moments in shared memory between
+ * steps.  The same results as `steps` calls of weftk_refine_step; d_loss receives the last
+ * step's loss and d_grad_params (may be NULL) its gradient. */
+int weftk_refine_steps(const WeftStackSet* set, int steps, float* d_params, float* d_m, float* d_v,
+                       const float* d_grad_loss, float* d_loss, float* d_grad_params, float lr, float beta1,
+                       float beta2, float eps, int flags, void* stream);
+
 /* Start a refinement from a fit: row r = the first selected primitive of tile d_tiles[r] of the
  * fit state (weftk_fit.h), as a parameter row projected onto the wire box, its kind in
  * d_kind[r], and zero Adam moments and step count (d_m, d_v rows).  A tile without a selection

@@ -126,3 +126,21 @@ def test_single_layer_register_path_matches_general_path(residual):
         two.step()
         l1, l2 = float((one.loss * w).sum()), float((two.loss * w).sum())
         assert l1 == pytest.approx(l2, rel=1e-4)
+
+
+@pytest.mark.parametrize("residual", [False, True])
+def test_multi_step_launch_equals_single_steps(residual):
+    """weftk_refine_steps (all steps in one launch) = the same number of one-step launches."""
+    from weft_b200.refine import FusedRefiner
+
+    fit = _fit().run()
+    ss, params = fit.stack_set()
+    one = FusedRefiner(ss, params, lr=1e-2, residual=residual)
+    many = FusedRefiner(ss, params, lr=1e-2, residual=residual)
+    for _ in range(7):
+        one.step()
+    many.run(7)
+    assert torch.equal(one.p[:, :14], many.p[:, :14])
+    assert torch.equal(one.m[:, :14], many.m[:, :14]) and torch.equal(one.v[:, :14], many.v[:, :14])
+    assert torch.equal(one.m[:, 15], many.m[:, 15])
+    assert torch.equal(one.loss, many.loss)

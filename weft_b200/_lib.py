@@ -98,6 +98,8 @@ SIGNATURES: dict[str, list] = {
     "weftk_stack_loss_backward": [_P, _P, _P, _P, _P, _I, _P],
     "weftk_adam_step": [_P, _P, _P, _P, _P, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P,
                         _P],
+    "weftk_refine_steps": [_P, _I, _P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                           ctypes.c_float, _I, _P],
     "weftk_refine_step": [_P, _P, _P, _P, _P, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                           ctypes.c_float, _I, _P],
     "weftk_measure_fp32_peak": [_P],

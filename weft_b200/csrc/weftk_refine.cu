@@ -258,7 +258,7 @@ __device__ void layer_grad(const Layers& s, int k, float px, float py, bool soft
 // Byte offsets for L staged layers; every region starts on a 16-byte boundary
 // except the trailing doubles (8-byte aligned).
 struct GroupLayout {
-    int prep, seg, raw, msum, quad, hnode, hist, gacc, lacc, lred, bytes;
+    int prep, seg, raw, madam, vadam, msum, quad, hnode, hist, gacc, lacc, lred, bytes;
 };
 
 // Stacks of at most this many layers accumulate gradients per lane (one slot per
@@ -271,7 +271,9 @@ __host__ __device__ __forceinline__ GroupLayout group_layout(int L, int wpt, boo
     g.prep = 0;
     g.seg = g.prep + L * 64;
     g.raw = g.seg + L * 992;
-    g.msum = g.raw + L * 64;
+    g.madam = g.raw + L * 64;   // Adam moments of the rows (RF_STEP)
+    g.vadam = g.madam + L * 64;
+    g.msum = g.vadam + L * 64;
     g.quad = g.msum + (resid ? 48 * 4 : 0);
     g.hnode = g.quad + (resid ? 768 * 4 : 0);
     g.hist = g.hnode + (resid ? 48 * 4 : 0);
@@ -285,15 +287,27 @@ __host__ __device__ __forceinline__ GroupLayout group_layout(int L, int wpt, boo
 // Adam (PyTorch's update rule, FP32) for one value at step t (1-based), then the
 // projection onto what the wire format carries: colours and alpha in [0, 1],
 // coordinates in [0, 15], thickness in [0, 4] (src/weft/primitives.py:102-177).
-__device__ __forceinline__ float adam_update(float p, float g, float& m, float& v, float t, float lr, float b1,
-                                             float b2, float eps, int kind, int col) {
+__device__ __forceinline__ float adam_update_bc(float p, float g, float& m, float& v, float bc1, float bc2, float lr,
+                                                float b1, float b2, float eps, int kind, int col) {
     m = fmaf(b1, m, (1.0f - b1) * g);
     v = fmaf(b2, v, (1.0f - b2) * g * g);
-    const float bc1 = 1.0f - powf(b1, t), bc2 = 1.0f - powf(b2, t);
     float x = p - lr * (m / bc1) / (sqrtf(v / bc2) + eps);
     if (col >= 7) return fminf(fmaxf(x, 0.0f), 1.0f);
     const bool thick = (kind == K_LINE && col == 4) || (kind == K_CURVE && col == 6);
     return fminf(fmaxf(x, 0.0f), thick ? 4.0f : 15.0f);
+}
+
+// Bias corrections 1 - beta^t of step t (1-based).
+__device__ __forceinline__ void adam_bias(float b1, float b2, float t, float& bc1, float& bc2) {
+    bc1 = 1.0f - powf(b1, t);
+    bc2 = 1.0f - powf(b2, t);
+}
+
+__device__ __forceinline__ float adam_update(float p, float g, float& m, float& v, float t, float lr, float b1,
+                                             float b2, float eps, int kind, int col) {
+    float bc1, bc2;
+    adam_bias(b1, b2, t, bc1, bc2);
+    return adam_update_bc(p, g, m, v, bc1, bc2, lr, b1, b2, eps, kind, col);
 }
 
 // Optimiser state of the fused refine step; the per-row step count lives in m[row * 16 + 15].
@@ -445,7 +459,7 @@ template <int MODE, bool CL1>
 __global__ void __launch_bounds__(RF_THREADS, 3)
     refine_tiles_kernel(WeftStackSet set, float* __restrict__ params, const float* __restrict__ grad_loss,
                         float* __restrict__ grad, float* __restrict__ loss, int flags, RefinePlan plan, int L,
-                        AdamArgs adam) {
+                        AdamArgs adam, int n_steps) {
     constexpr bool BWD = MODE != RF_LOSS;
     extern __shared__ __align__(16) unsigned char rf_smem[];
     const int bx = blockIdx.x;
@@ -467,6 +481,8 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     Prep* prep = reinterpret_cast<Prep*>(base + lay.prep);
     float4(*seg)[31][2] = reinterpret_cast<float4(*)[31][2]>(base + lay.seg);
     float(*raw)[16] = reinterpret_cast<float(*)[16]>(base + lay.raw);
+    float* madam = reinterpret_cast<float*>(base + lay.madam);
+    float* vadam = reinterpret_cast<float*>(base + lay.vadam);
     float* msum = reinterpret_cast<float*>(base + lay.msum);
     float* quad = reinterpret_cast<float*>(base + lay.quad);
     float* hnode = reinterpret_cast<float*>(base + lay.hnode);
@@ -490,40 +506,16 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     }
     const int gt = wig * 32 + lane, GT = wpt * 32;
 
-    // ---- stage the layers
-    for (int i = gt; i < K * 16; i += GT) raw[i >> 4][i & 15] = params[(size_t)p0 * 16 + i];
-    group_sync(wpt, grp);
-    for (int k = gt; k < K; k += GT) {
-        Prep P = prep_prim(row_to_prim(raw[k], set.kind[p0 + k]));
-        if (P.kind == K_BICUBIC) P.kind = K_SKIP;
-        prep[k] = P;
-    }
-    group_sync(wpt, grp);
-    for (int i = gt; i < K * 31; i += GT) {
-        const int k = i / 31, j = i - k * 31;
-        if (prep[k].kind == K_CURVE) {
-            const Seg g = lane_segment(prep[k], j);
-            seg[k][j][0] = make_float4(g.ax, g.ay, g.vx, g.vy);
-            seg[k][j][1] = make_float4(g.ux, g.uy, 0.0f, 0.0f);
+    // ---- stage the layers (rows, and for STEP the Adam moments, stay in shared memory
+    //      across the launch's steps; everything else is re-derived every step)
+    for (int i = gt; i < K * 16; i += GT) {
+        raw[i >> 4][i & 15] = params[(size_t)p0 * 16 + i];
+        if (MODE == RF_STEP) {
+            madam[i] = adam.m[(size_t)p0 * 16 + i];
+            vadam[i] = adam.v[(size_t)p0 * 16 + i];
         }
     }
-    if (BWD) {
-        for (int i = lane; i < K * 14; i += 32) gacc[i] = 0.0f;
-        if (lane_acc)
-            for (int i = lane; i < K * 14 * 32; i += 32) lacc[i] = 0.0f;
-    }
-    if (resid)
-        for (int i = gt; i < 48 + 768; i += GT) {
-            if (i < 48)
-                msum[i] = 0.0f;
-            else
-                quad[i - 48] = 0.0f;
-        }
-    group_sync(wpt, grp);
     const Layers S{prep, raw, seg};
-    if (CL1 && K == 1 && gt == 0 && prep[0].kind != K_CONST && prep[0].kind != K_LINEAR && prep[0].kind != K_SKIP)
-        atomicCAS(&g_device_status, 0, WEFTK_E_ARG);  // not a constant/linear layer: treated as absent
-
     const float4* src = reinterpret_cast<const float4*>(set.src) + set.px_off[t];
     const int n = ts * ts;
     const int chunks = (n + 31) >> 5;
@@ -596,6 +588,39 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     };
 
     double sse = 0.0;
+    for (int step = 0; step < n_steps; ++step) {
+    sse = 0.0;
+    group_sync(wpt, grp);
+    for (int k = gt; k < K; k += GT) {
+        Prep P = prep_prim(row_to_prim(raw[k], set.kind[p0 + k]));
+        if (P.kind == K_BICUBIC) P.kind = K_SKIP;
+        prep[k] = P;
+    }
+    group_sync(wpt, grp);
+    for (int i = gt; !CL1 && i < K * 31; i += GT) {
+        const int k = i / 31, j = i - k * 31;
+        if (prep[k].kind == K_CURVE) {
+            const Seg g = lane_segment(prep[k], j);
+            seg[k][j][0] = make_float4(g.ax, g.ay, g.vx, g.vy);
+            seg[k][j][1] = make_float4(g.ux, g.uy, 0.0f, 0.0f);
+        }
+    }
+    if (BWD) {
+        for (int i = lane; i < K * 14; i += 32) gacc[i] = 0.0f;
+        if (!CL1 && lane_acc)
+            for (int i = lane; i < K * 14 * 32; i += 32) lacc[i] = 0.0f;
+    }
+    if (resid)
+        for (int i = gt; i < 48 + 768; i += GT) {
+            if (i < 48)
+                msum[i] = 0.0f;
+            else
+                quad[i - 48] = 0.0f;
+        }
+    group_sync(wpt, grp);
+    if (CL1 && K == 1 && gt == 0 && prep[0].kind != K_CONST && prep[0].kind != K_LINEAR && prep[0].kind != K_SKIP)
+        atomicCAS(&g_device_status, 0, WEFTK_E_ARG);  // not a constant/linear layer: treated as absent
+
     if (resid) {
         // ---- pass 1: block sums of e (segments of bb visits; one owner per block)
         float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -789,6 +814,9 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
                 gacc[j] = s;
             }
         }
+        if (MODE == RF_STEP)  // each row's bias corrections for this step, once (column 14 is free)
+            for (int k = gt; k < K; k += GT) adam_bias(adam.b1, adam.b2, madam[k * 16 + 15] + 1.0f,
+                                                       madam[k * 16 + 14], vadam[k * 16 + 14]);
         group_sync(wpt, grp);
         for (int i = gt; i < K * 16; i += GT) {
             const int k = i >> 4, j = i & 15;
@@ -796,19 +824,18 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
             if (j < 14)
                 for (int w = 0; w < wpt; ++w) s += gacc_all[((size_t)w * L + k) * 14 + j];
             const size_t at = (size_t)(p0 + k) * 16 + j;
-            if (grad) grad[at] = s;
+            if (grad && step == n_steps - 1) grad[at] = s;
             if (MODE == RF_STEP && j < 14) {
-                const float tstep = adam.m[(size_t)(p0 + k) * 16 + 15] + 1.0f;
-                float m = adam.m[at], v = adam.v[at];
-                params[at] = adam_update(raw[k][j], s, m, v, tstep, adam.lr, adam.b1, adam.b2, adam.eps,
-                                         set.kind[p0 + k], j);
-                adam.m[at] = m;
-                adam.v[at] = v;
+                float m = madam[k * 16 + j], v = vadam[k * 16 + j];
+                raw[k][j] = adam_update_bc(raw[k][j], s, m, v, madam[k * 16 + 14], vadam[k * 16 + 14], adam.lr,
+                                           adam.b1, adam.b2, adam.eps, set.kind[p0 + k], j);
+                madam[k * 16 + j] = m;
+                vadam[k * 16 + j] = v;
             }
         }
         if (MODE == RF_STEP) {
             group_sync(wpt, grp);  // every column of a row has read its step count
-            for (int k = gt; k < K; k += GT) adam.m[(size_t)(p0 + k) * 16 + 15] += 1.0f;
+            for (int k = gt; k < K; k += GT) madam[k * 16 + 15] += 1.0f;
         }
     } else if (!resid) {
         float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -823,6 +850,16 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
             composite((float)x + 0.5f, (float)y + 0.5f, c, nullptr);
             const float dr = clamp01(c[0]) - v.x, dg = clamp01(c[1]) - v.y, db = clamp01(c[2]) - v.z;
             sse += (double)fmaf(dr, dr, fmaf(dg, dg, db * db));
+        }
+    }
+    }  // steps
+    if (MODE == RF_STEP) {
+        group_sync(wpt, grp);
+        for (int i = gt; i < K * 16; i += GT) {
+            const bool scratch = (i & 15) == 14;  // bias-correction scratch, not state
+            params[(size_t)p0 * 16 + i] = raw[i >> 4][i & 15];
+            adam.m[(size_t)p0 * 16 + i] = scratch ? 0.0f : madam[i];
+            adam.v[(size_t)p0 * 16 + i] = scratch ? 0.0f : vadam[i];
         }
     }
     if (loss != nullptr) {
@@ -840,7 +877,8 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
 
 template <int MODE>
 static int launch_refine(const WeftStackSet& set, float* params, const float* grad_loss, float* grad, float* loss,
-                         int flags, AdamArgs adam, cudaStream_t stream, const char* what) {
+                         int flags, AdamArgs adam, cudaStream_t stream, const char* what, int n_steps = 1) {
+    if (n_steps < 1 || (MODE != RF_STEP && n_steps != 1)) return fail(WEFTK_E_ARG, std::string(what) + ": bad step count");
     if (set.n_tiles == 0) return WEFTK_OK;
     if (set.max_prims < 0 || set.max_prims > MAXL) return fail(WEFTK_E_RANGE, std::string(what) + ": stack too long");
     if (!params || !set.src || !set.px_off || !set.size || !set.prim_off || (set.max_prims > 0 && !set.kind))
@@ -886,10 +924,10 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
     }
     if (cl1)
         refine_tiles_kernel<MODE, true><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags,
-                                                                            plan, L, adam);
+                                                                            plan, L, adam, n_steps);
     else
         refine_tiles_kernel<MODE, false><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss,
-                                                                             flags, plan, L, adam);
+                                                                             flags, plan, L, adam, n_steps);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }
@@ -990,4 +1028,13 @@ extern "C" int weftk_refine_step(const WeftStackSet* set, float* d_params, float
     WEFTK_REQUIRE(set && d_params && d_m && d_v && d_grad_loss, "refine_step: null argument");
     return launch_refine<RF_STEP>(*set, d_params, d_grad_loss, d_grad_params, d_loss, flags,
                                   AdamArgs{d_m, d_v, lr, beta1, beta2, eps}, (cudaStream_t)stream, "refine_step");
+}
+
+extern "C" int weftk_refine_steps(const WeftStackSet* set, int steps, float* d_params, float* d_m, float* d_v,
+                                  const float* d_grad_loss, float* d_loss, float* d_grad_params, float lr, float beta1,
+                                  float beta2, float eps, int flags, void* stream) {
+    WEFTK_REQUIRE(set && d_params && d_m && d_v && d_grad_loss && steps >= 1, "refine_steps: bad argument");
+    return launch_refine<RF_STEP>(*set, d_params, d_grad_loss, d_grad_params, d_loss, flags,
+                                  AdamArgs{d_m, d_v, lr, beta1, beta2, eps}, (cudaStream_t)stream, "refine_steps",
+                                  steps);
 }

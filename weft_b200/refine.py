@@ -264,8 +264,19 @@ class FusedRefiner:
                                        _lib.ptr(self.step_ctr), s), "weftk_adam_step")
 
     def run(self, steps: int) -> torch.Tensor:
-        for _ in range(int(steps)):
-            self.step()
+        """``steps`` steps; with ``single_launch`` all of them in ONE launch
+        (``weftk_refine_steps``: each tile group loops over the steps on its own rows)."""
+        steps = int(steps)
+        if steps <= 0:
+            return self.p
+        if not self.single_launch:
+            for _ in range(steps):
+                self.step()
+            return self.p
+        lib, ss = self.ss.lib, self.ss
+        _lib.check(lib.weftk_refine_steps(ctypes_addr(ss.st), steps, _lib.ptr(self.p), _lib.ptr(self.m),
+                                          _lib.ptr(self.v), _lib.ptr(self.w), _lib.ptr(self.loss), 0, self.lr,
+                                          self.b1, self.b2, self.eps, self.flags, ss._stream()), "weftk_refine_steps")
         return self.p
 
     def restart(self, params: torch.Tensor) -> None:
@@ -308,8 +319,7 @@ class RefinedFit:
         _lib.check(self.ss.lib.weftk_refine_start(ctypes_addr(f.st), _lib.ptr(self.rows32), int(self.rows32.numel()),
                                                   _lib.ptr(fr.p), _lib.ptr(fr.m), _lib.ptr(fr.v),
                                                   _lib.ptr(self.kinds), self.ss._stream()), "weftk_refine_start")
-        for _ in range(self.steps):
-            fr.step()
+        fr.run(self.steps)
 
     @property
     def start(self) -> torch.Tensor:

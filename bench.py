@@ -377,6 +377,7 @@ def refined_headline(args, local, pixels, sizes, pools, stream, world):
     rec = np.concatenate(fast_pools)
     cnt = np.array([len(p) for p in fast_pools], np.int64)
     fast = BatchedFit.from_arrays(pixels, sizes, rec, cnt, QUALITY, caps=[CAP] * len(sizes), device=local, reserve=0)
+    fast.use_closed_form_init(True)
     fast.autotune()
     rf = RefinedFit(fast, steps=args.refine_steps, lr=args.refine_lr, use_graph=True)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")

@@ -80,7 +80,16 @@ typedef struct WeftFitState {
      * pixels per lane x warps per candidate x CTAs per SM.  Chosen by the autotuner. */
     int32_t variant[3];
     int32_t _pad;
+    /* Optional (NULL: off): per-tile pixel moments, double[n_tiles * 6] = sum of src r, g, b and
+     * of their squares (weftk_fit_moments).  When set, the init round scores a constant
+     * candidate in closed form — over an empty stack its render is one colour q per channel,
+     * so its squared error is n q^2 - 2 q S1 + S2 — instead of per pixel (equal up to
+     * rounding; a near tie may then pick differently from the per-pixel sum). */
+    const double* moments;
 } WeftFitState;
+
+/* Fill d_moments (double[n_tiles * 6]) from the fit's tile pixels. */
+int weftk_fit_moments(const WeftFitState* st, double* d_moments, void* stream);
 
 #define WEFTK_FIT_VARIANTS 3
 

@@ -150,3 +150,26 @@ def test_device_driven_fit_equals_host_loop_and_replays():
         g.replay()
         assert fit.selected_indices() == want_sel
         np.testing.assert_array_equal(fit.objectives(), want_obj)
+
+
+def test_closed_form_init_matches_per_pixel_objectives():
+    """Init-round objectives with constant candidates scored from tile moments agree with the
+    per-pixel scores to float rounding; selections agree except on near ties."""
+    from weft_b200 import candidates, quadtree
+    from weft_b200.fit import BatchedFit
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 64, 3, 3)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    pools = [[c for c in candidates.tile_candidates(p, 75) if c.kind in (0, 1)] for p in patches]
+    fit = BatchedFit(patches, pools, 75, caps=[16] * len(qts))
+    fit.run(max_rounds=0)
+    want_sel, want_obj = fit.selected_indices(), fit.objectives()
+    fit.use_closed_form_init(True)
+    fit.reset()
+    fit.run(max_rounds=0)
+    np.testing.assert_allclose(fit.objectives(), want_obj, rtol=1e-5)
+    same = sum(a == b for a, b in zip(fit.selected_indices(), want_sel))
+    assert same >= 0.95 * len(want_sel)

@@ -43,7 +43,7 @@ class WeftFitState(ctypes.Structure):
         (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "pool_cap", "n_alive",
                                        "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive", "kind",
                                        "partial", "status", "work")] + [
-        ("variant", ctypes.c_int32 * 3), ("_pad", ctypes.c_int32)]
+        ("variant", ctypes.c_int32 * 3), ("_pad", ctypes.c_int32), ("moments", ctypes.c_void_p)]
 
 FIT_VARIANTS = 3
 
@@ -69,7 +69,7 @@ assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
 assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
 FIT_ITEM_DTYPE = np.dtype([("tile", np.int32), ("block", np.int32), ("first", np.int32), ("count", np.int32)])
 assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
-assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8 + 16
+assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8 + 16 + 8
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -87,6 +87,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_render_tiles_host": [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I],
     "weftk_fit_prepare": [_P, _P, _P],
     "weftk_fit_reset": [_P, _P, _P],
+    "weftk_fit_moments": [_P, _P, _P],
     "weftk_rans_decode_chunks": [_P, ctypes.c_int64, _P, _I, _P, ctypes.c_int64, _P],
     "weftk_fit_run": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P, _P],
     "weftk_refine_start": [_P, _P, _I, _P, _P, _P, _P, _P],

@@ -89,6 +89,7 @@ class ImageBatch:
         pixels, sizes, recs, cnt = self.arrays(kinds)
         fit = BatchedFit.from_arrays(pixels, sizes, recs, cnt, self.quality, caps=[self.cap] * len(sizes),
                                      device=self.device, reserve=0)
+        fit.use_closed_form_init(True)
         if autotune:
             fit.autotune()
         return RefinedFit(fit, steps=steps, lr=lr, use_graph=use_graph, residual=residual)

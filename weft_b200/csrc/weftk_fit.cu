@@ -159,7 +159,7 @@ constexpr int MAX_ITEM = 128;
 template <int PPL, int WPC, int MINB>
 __global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
                                                         const WeftFitItem* __restrict__ items, int n_items,
-                                                        int expect_min, int expect_max) {
+                                                        int expect_min, int expect_max, bool mode_init) {
     constexpr int GROUPS = 4 / WPC;
     __shared__ float4 s_prep[MAX_ITEM][4];
     __shared__ int s_slot[MAX_ITEM];
@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, c
     }
     if (!(st.flags[t] & WEFTK_TILE_EVAL)) return;
     const int ts = st.size[t];
+    const bool closed_form = mode_init && st.moments != nullptr;
     if (ts < expect_min || ts > expect_max || w.count > MAX_ITEM || w.block * 1024 >= ts * ts || w.first < 0 ||
         w.first + w.count > st.pool_cap[t]) {
         if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
@@ -192,6 +193,23 @@ __global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, c
     if ((int)threadIdx.x < count) {
         my_slot = off + perm[off + w.first + threadIdx.x];
         live = st.alive[my_slot] != 0;
+        if (live && closed_form && st.kind[my_slot] == K_CONST) {
+            // Init round over an empty stack: a constant layer renders one colour q per channel,
+            // so sum over pixels and channels of (q - s)^2 = sum_ch n q^2 - 2 q S1 + S2.
+            const float4 head = __ldg(reinterpret_cast<const float4*>(st.prep) + my_slot * 4);
+            const float4 head2 = __ldg(reinterpret_cast<const float4*>(st.prep) + my_slot * 4 + 1);
+            const float a = head.y, col[3] = {head.z, head.w, head2.x};
+            const double* mo = st.moments + (size_t)t * 6;
+            const double npx = (double)(ts * ts);
+            double e = 0.0;
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                const double q = (double)clamp01(blend(col[ch], a, 0.0f));
+                e += npx * q * q - 2.0 * q * mo[ch] + mo[3 + ch];
+            }
+            st.partial[my_slot * 4 + w.block] = w.block == 0 ? (float)e : 0.0f;
+            live = false;  // not evaluated per pixel
+        }
     }
     const unsigned bal = __ballot_sync(FULL, live);
     if (lane == 0) s_wcount[warp] = __popc(bal);
@@ -506,6 +524,41 @@ __global__ void fit_reset_kernel(WeftFitState st, const int* __restrict__ init_c
     for (int i = threadIdx.x; i < ts * ts; i += blockDim.x) bg[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
+__global__ void fit_moments_kernel(WeftFitState st, double* __restrict__ out) {
+    __shared__ double red[6][4];
+    const int t = blockIdx.x;
+    if (t >= st.n_tiles) return;
+    const int ts = st.size[t], n = ts * ts, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float4* src = reinterpret_cast<const float4*>(st.src) + st.px_off[t];
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 v = src[i];
+        a[0] += v.x;
+        a[1] += v.y;
+        a[2] += v.z;
+        a[3] += (double)v.x * v.x;
+        a[4] += (double)v.y * v.y;
+        a[5] += (double)v.z * v.z;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], o);
+        if (lane == 0) red[k][warp] = a[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) out[(size_t)t * 6 + threadIdx.x] = red[threadIdx.x][0] + red[threadIdx.x][1] +
+                                                             red[threadIdx.x][2] + red[threadIdx.x][3];
+}
+
+extern "C" int weftk_fit_moments(const WeftFitState* st, double* d_moments, void* stream) {
+    WEFTK_REQUIRE(st && d_moments, "fit_moments: null argument");
+    if (st->n_tiles == 0) return WEFTK_OK;
+    fit_moments_kernel<<<st->n_tiles, 128, 0, (cudaStream_t)stream>>>(*st, d_moments);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_fit_reset(const WeftFitState* st, const int32_t* d_init_cnt, void* stream) {
     WEFTK_REQUIRE(st && d_init_cnt, "fit_reset: null argument");
     if (st->n_tiles == 0) return WEFTK_OK;
@@ -545,7 +598,7 @@ extern "C" int weftk_fit_round_static(const WeftFitState* st, int mode, double l
 // Scoring variants per size class.  A class's variants cover the same pixels per candidate pass
 // (64 for 8-px tiles, 256 for 16-px tiles, one 1024-pixel block for 32/64-px tiles) with a
 // different split over lanes and warps, or a different register budget.
-static_assert(sizeof(WeftFitState) == 200, "WeftFitState layout is part of the C ABI");
+static_assert(sizeof(WeftFitState) == 208, "WeftFitState layout is part of the C ABI");
 
 struct ScoreShape {
     int ppl, wpc, minb;
@@ -556,10 +609,13 @@ static const ScoreShape kShapes[3][WEFTK_FIT_VARIANTS] = {
     {{8, 4, 4}, {8, 4, 3}, {8, 4, 5}},
 };
 
+// mode of the round being enqueued (the class launchers' extra argument)
+static thread_local bool g_mode_init = false;
+
 template <int PPL, int WPC, int MINB>
 static void launch_score(const WeftFitState& st, const int* perm, const WeftFitItem* items, int n, int lo, int hi,
                          cudaStream_t s) {
-    fit_score_kernel<PPL, WPC, MINB><<<n, 128, 0, s>>>(st, perm, items, n, lo, hi);
+    fit_score_kernel<PPL, WPC, MINB><<<n, 128, 0, s>>>(st, perm, items, n, lo, hi, g_mode_init);
 }
 
 static void launch_score_class8(int v, const WeftFitState& st, const int* perm, const WeftFitItem* it, int n,
@@ -641,6 +697,7 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
         if (rc) return rc;
         WEFTK_CUDA(cudaEventRecord(g_timing.start, s));
     }
+    g_mode_init = mode == WEFTK_FIT_INIT;
     if (n_items8) launch_score_class8(st->variant[0], *st, d_perm, d_items8, n_items8, s);
     if (n_items16) launch_score_class16(st->variant[1], *st, d_perm, d_items16, n_items16, s);
     if (n_items32) launch_score_class32(st->variant[2], *st, d_perm, d_items32, n_items32, s);

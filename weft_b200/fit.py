@@ -388,6 +388,20 @@ class BatchedFit:
         """The device-driven fit captured once in a CUDA graph (replay() refits from scratch)."""
         return FitGraph(self, max_rounds)
 
+    def use_closed_form_init(self, on: bool = True) -> "BatchedFit":
+        """Score constant candidates of the init round in closed form from per-tile pixel
+        moments (``WeftFitState.moments``) instead of per pixel; equal up to rounding, so a near
+        tie may pick differently from the reference's per-pixel sum (off for the plain fit)."""
+        if on:
+            if not hasattr(self, "t_moments"):
+                self.t_moments = torch.zeros(max(self.n, 1) * 6, dtype=torch.float64, device=self.device)
+                _lib.check(self.lib.weftk_fit_moments(ctypes_ref(self.st), _lib.ptr(self.t_moments), self._stream()),
+                           "weftk_fit_moments")
+            self.st.moments = _lib.ptr(self.t_moments)
+        else:
+            self.st.moments = None
+        return self
+
     def init_kinds(self) -> np.ndarray:
         """Primitive kind of every filled slot of the initial pools (host copy)."""
         return self._init_kinds[self._init_kinds < 7].astype(np.int32)

@@ -293,8 +293,10 @@ class RefinedFit:
     fit's (possibly kind-filtered) pools, gather of each tile's selected primitive, and
     ``steps`` fused Adam steps.  Every launch is device work on torch's current stream."""
 
-    def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True, residual: bool = False):
+    def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True, residual: bool = False,
+                 closed_form_init: bool = True):
         self.fit = fit
+        fit.use_closed_form_init(closed_form_init)
         dev = fit.device
         has = fit.init_cnt > 0
         self.rows = torch.from_numpy(np.nonzero(has)[0]).to(dev)

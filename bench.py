@@ -537,6 +537,19 @@ def _hbm_peak() -> tuple[float, str]:
         return 6650.0, "fallback 6.65 TB/s (earlier measurement on this pool)"
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """The slowest rank's time (every rank calls this at the same point)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup(n_gpus: int):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -673,12 +686,7 @@ def run_weft(args, world, rank, local, executor, cores):
 
     ms_total = ev0.elapsed_time(ev1)
     ms_step = ms_total / args.steps
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = max_over_ranks(ms_step, world)
     value = world * n_px / (ms_step * 1e-3) / 1e6
     # scoring-kernel time: one host-driven run of the same fit with events around the scoring
     # launches (the graph cannot host-synchronise); the same kernels and work
@@ -746,12 +754,7 @@ def run_weft(args, world, rank, local, executor, cores):
     sampler2.start()
     rf, fast, frec, fcnt, ref_ms = refined_headline(args, local, pixels, sizes, pools, stream, world)
     clocks2 = sampler2.stop()
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ref_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ref_ms = float(t.item())
+    ref_ms = max_over_ranks(ref_ms, world)
     ref_value = world * n_px / (ref_ms * 1e-3) / 1e6
     plain_rd = rd["plain"] if rd else rd_of_params(*fit.stack_set(), tiles, patches, img, args.size)
     ref_rd = rd_of_params(rf.ss, rf.refiner.p, tiles, patches, img, args.size)

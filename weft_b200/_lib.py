@@ -87,6 +87,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_render_tiles_host": [_P, _I, _P, _I, _P, _I, _P, _I, _P, _I, _I, _I],
     "weftk_fit_prepare": [_P, _P, _P],
     "weftk_fit_reset": [_P, _P, _P],
+    "weftk_build_residuals": [_P, _P, _I, _P, _P, _I, _P, _P, _P],
     "weftk_fit_moments": [_P, _P, _P],
     "weftk_rans_decode_chunks": [_P, ctypes.c_int64, _P, _I, _P, ctypes.c_int64, _P],
     "weftk_fit_run": [_P, _I, ctypes.c_double, ctypes.c_double, _P, _P, _I, _P, _I, _P, _I, _P, _P],

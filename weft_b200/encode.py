@@ -42,6 +42,24 @@ def residuals_from_recon(patches, recon):
     return res0, res1
 
 
+def residuals_from_fit_gpu(fit):
+    """RES0 and RES1 of a ``BatchedFit``'s current selection, built on the GPU from its resident
+    tile pixels and composite (``weftk_build_residuals``); the same bytes as
+    ``residuals_from_recon(patches, fit.recon_tiles())``."""
+    import torch
+
+    from . import _lib
+
+    d = fit.device
+    r0 = torch.zeros((fit.n, 3), dtype=torch.int8, device=d)
+    r1 = torch.zeros((fit.n, 4, 4, 3), dtype=torch.int8, device=d)
+    _lib.check(fit.lib.weftk_build_residuals(_lib.ptr(fit.t_src), _lib.ptr(fit.t_bg), 1, _lib.ptr(fit.t_px_off),
+                                             _lib.ptr(fit.t_size), fit.n, _lib.ptr(r0), _lib.ptr(r1),
+                                             torch.cuda.current_stream(d).cuda_stream), "weftk_build_residuals")
+    res0 = [tuple(int(v) for v in row) for row in r0.cpu().numpy()]
+    return res0, list(r1.cpu().numpy())
+
+
 def encode_fit(width, height, quality, tiles, patches, stacks, recon, with_res0=True, with_res1=True):
     """File bytes for fitted ``stacks`` (per-tile primitives) whose clipped renders are ``recon``."""
     res0, res1 = residuals_from_recon(patches, recon)

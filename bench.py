@@ -767,7 +767,7 @@ def run_weft(args, world, rank, local, executor, cores):
     refine_share = args.refine_steps * r_step_ms
     n_cls = sum(1 for k in (8, 16, 32) if fast.n_items[k])
     # reset, prepare, begin, select, end, scoring (one per size class), refine start, refine steps
-    ref_launches = 6 + n_cls + args.refine_steps
+    ref_launches = 7 + n_cls  # ... and one launch for all refine steps
 
     def refined_e2e():
         from weft_b200.refine import RefinedFit
@@ -798,10 +798,10 @@ def run_weft(args, world, rank, local, executor, cores):
                   "candidate_pixels_per_step": cand_px // args.steps}
     refine_roof = {"bound": "fp32", "achieved": refine_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
                    "frac": refine_tflops / peak_tflops if peak_tflops else None, "traffic": None,
-                   "kernel": "refine_tiles_kernel (loss + gradient + Adam, one launch per step)",
+                   "kernel": "refine_tiles_kernel (loss + gradient + Adam; all steps of a fit in one launch)",
                    "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
-                   "ms_per_launch": r_step_ms, "launches_per_step": args.refine_steps,
-                   "flops_per_launch": r_flops}
+                   "ms_per_adam_step": r_step_ms, "adam_steps_per_launch": args.refine_steps,
+                   "flops_per_adam_step": r_flops}
     init_roof = {"bound": "fp32", "achieved": init_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
                  "frac": init_tflops / peak_tflops if peak_tflops else None, "traffic": None,
                  "kernel": "fit_score_kernel, init round of the refined fit", "ms_per_step": r_score_ms,

@@ -52,3 +52,35 @@ def test_reader_parses_reference_file_and_writer_reproduces_its_payloads(golden)
     wb = bitstream.decode_weft(blob)
     assert wb.prim_raw == wf.prim_raw and wb.toc == wf.toc and wb.residuals == wf.residuals
     assert all(np.array_equal(x, y) for x, y in zip(wb.res1_maps, wf.res1_maps))
+
+
+def test_edge_cases_round_trip():
+    """Empty stacks, empty files, one tile, the longest stacks and values at the wire grid's
+    limits write and read back (host coder)."""
+    class QT:
+        def __init__(self, x, y, s):
+            self.x, self.y, self.size = x, y, s
+
+    rng = np.random.default_rng(5)
+    # every tile empty
+    tiles = [QT(0, 0, 64), QT(64, 0, 64)]
+    blob = bitstream.encode_weft(128, 64, 75, tiles, [[], []])
+    wf = bitstream.decode_weft(blob)
+    assert [len(t) for t in bitstream.decode_tiles(wf.prim_raw, wf.toc)] == [0, 0]
+    # one tile with a long stack of every kind, geometry and colours at the grid's limits
+    kinds = [0, 1, 2, 3, 4] * 9
+    stack = []
+    for k in kinds:
+        glen = {0: 0, 1: 4, 2: 5, 3: 7, 4: 6}[k]
+        g = tuple(float(v) for v in rng.choice([0.0, 15.0, 7.5], glen))
+        if k in (2, 3):
+            g = g[:-1] + (float(rng.choice([0.0, 4.0])),)
+        c1 = (1.0, 0.0, 1.0) if k == 1 else None
+        stack.append(Cand(k, g, (0.0, 1.0, 0.5), c1, float(rng.choice([0.0, 1.0]))))
+    blob = bitstream.encode_weft(64, 64, 92, [QT(0, 0, 64)], [stack])
+    wf = bitstream.decode_weft(blob)
+    back = bitstream.decode_tiles(wf.prim_raw, wf.toc)[0]
+    assert [b[0] for b in back] == kinds
+    for b, c in zip(back, stack):
+        assert np.allclose(b[1], c.geom, atol=1e-3) and np.allclose(b[2], c.color0, atol=1 / 255)
+        assert abs(b[4] - c.alpha) < 1e-4

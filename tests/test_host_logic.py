@@ -40,3 +40,11 @@ def test_refine_flop_count_follows_the_per_kind_table():
     per = {k: 2 * bench.REFINE_EVAL[k] + 9 + bench.REFINE_CHAIN[k] for k in (0, 1, 4)}
     want = 64 * (per[0] + per[1] + 9) + 256 * 9 + 1024 * (per[0] + per[4] + 9)
     assert bench.refine_flops(ss) == want
+
+
+def test_kinds_mask():
+    from weft_b200.refine import kinds_mask_of
+
+    assert kinds_mask_of(np.array([0, 1, 1, 0], np.int8)) == 3
+    assert kinds_mask_of(np.zeros(0, np.int32)) == 0
+    assert kinds_mask_of(np.array([4, 2, -1, 7], np.int32)) == (1 << 4) | (1 << 2) | (1 << 7)

@@ -73,8 +73,7 @@ class StackSet:
             self.kinds_np = np.asarray(kinds, np.int32)
             self.t_kind = torch.from_numpy(self.kinds_np).to(self.device)
             if kinds_mask is None:
-                kinds_mask = int(np.bitwise_or.reduce(1 << np.unique(self.kinds_np).astype(np.int64))) \
-                    if self.kinds_np.size else 0
+                kinds_mask = kinds_mask_of(self.kinds_np)
         self.t_prim_off = torch.from_numpy(self.prim_off_np.astype(np.int32)).to(self.device)
         # work split by tile side (largest first): > 32 px eight warps, 17-32 four, 9-16 two, <= 8 one
         sz = sizes.cpu().numpy()
@@ -176,6 +175,16 @@ class StackSet:
         cands = unpack_cands(recs)
         off = self.prim_off_np
         return [cands[off[t]:off[t + 1]] for t in range(self.n)]
+
+
+def kinds_mask_of(kinds: np.ndarray) -> int:
+    """Bit k set when kind k occurs (kinds outside 0..30 are ignored)."""
+    k = np.asarray(kinds).astype(np.int64, copy=False).ravel()
+    k = k[(k >= 0) & (k < 31)]
+    if k.size == 0:
+        return 0
+    present = np.nonzero(np.bincount(k, minlength=1))[0]
+    return int(np.bitwise_or.reduce(np.left_shift(1, present)))
 
 
 def loss_flags(soft: bool = False, residual: bool = False) -> int:
@@ -304,8 +313,7 @@ class RefinedFit:
         prim_off = np.concatenate([[0], np.cumsum(has.astype(np.int64))])
         n_rows = int(has.sum())
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
-        pool_kinds = np.unique(fit.init_kinds())
-        mask = int(np.bitwise_or.reduce(1 << pool_kinds.astype(np.int64))) if pool_kinds.size else 0
+        mask = kinds_mask_of(fit.init_kinds())
         self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask)
         self.refiner = FusedRefiner(self.ss, torch.zeros((n_rows, 16), dtype=torch.float32, device=dev), lr=lr,
                                     residual=residual)

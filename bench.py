@@ -711,7 +711,7 @@ def run_weft(args, world, rank, local, executor, cores):
     # bytes the scoring kernels must move per launch: src+bg per pixel per item, prep per candidate
     cand_px = sum(w[0] for w in work) * args.steps
 
-    # RD of the fitted primitives (PRIM-only reconstruction)
+    # PSNR and payload of the fitted primitives alone (no residual grids)
     sel = fit.selected()
     recon = fit.recon_tiles()
     mse = float(np.mean([np.mean((p - r) ** 2) for p, r in zip(patches, recon)]))

@@ -3,10 +3,11 @@
 This package restates, in plain numpy, the reference's CPU algorithms for the
 path the CUDA library implements: the per-tile renderer, the per-tile
 objective and rate model, the greedy candidate-scoring fit, the decoder's
-scene walk, primitive quantization/serialization, the quadtree and the
+scene walk and its raster branch (DCT residual layer, Pillow-compatible
+BILINEAR resize), primitive quantization/serialization, the quadtree and the
 order-0 rANS coder.  Every function cites the reference file:line it follows.
 
-Parity is pinned: ``tests/test_oracle_golden.py`` checks every function here
+Parity is pinned: ``tests/test_oracle_golden.py`` and ``tests/test_dct_cpu.py`` check every function here
 against golden vectors produced by running the reference itself
 (``tests/golden/make_golden.py``).
 

@@ -33,6 +33,15 @@ What is captured (reference function -> fixture):
     ``render_tile`` at pixel centres (the reference GPU launcher
     ``gpu_render.gpu_batch_score_prepacked`` needs a GPU)
                                -> fit_small.npz (q=75), fit_hq.npz (q=92)
+  * ``dct_residual.encode_tile_residuals`` / ``permute_tile_to_band`` /
+    ``bitstream.pack_dct`` payloads (block versions 2-5, every chroma mode and
+    layout, presence masks, per-tile scales) applied by the reference decoder's
+    steps ``unpack_dct`` -> ``permute_band_to_tile`` -> ``apply_residual_to_image``
+    (src/weft/decoder.py:477-507), and Pillow ``Image.resize(BILINEAR)`` of u8
+    images (src/weft/decoder.py:514-518)                    -> dct.npz
+  * ``encoder.encode_image`` with the DCT residual layer, decoded by
+    ``decoder.decode_to_array`` at the encoded size and at up/down-scaled
+    targets (the raster branch)                             -> container_dct.npz
 
 Every primitive parameter handed to the reference is first rounded to float32,
 so the fixtures are exact for kernels that consume float32 records.
@@ -41,6 +50,7 @@ so the fixtures are exact for kernels that consume float32 records.
 from __future__ import annotations
 
 import os
+import struct
 import sys
 import tempfile
 
@@ -550,10 +560,113 @@ def gen_container(ref) -> None:
           file_b=np.frombuffer(blob_b, np.uint8), decoded_b=dec_b.astype(np.float32))
 
 
+DCT_TILES = [(0, 0, 64), (64, 0, 32), (96, 0, 32), (64, 32, 16), (80, 32, 16), (64, 48, 8), (72, 48, 8),
+             (64, 56, 8), (72, 56, 8), (80, 48, 16), (96, 32, 32), (0, 64, 32), (32, 64, 32), (0, 96, 32),
+             (32, 96, 32), (64, 64, 64)]
+
+
+def gen_dct(ref) -> None:
+    """BLOCK_DCT payloads from the reference's encoder helpers, applied to a random recon by
+    the reference decoder's own steps (src/weft/decoder.py:477-507); Pillow BILINEAR resizes."""
+    from PIL import Image
+
+    R = ref["dct_residual"]
+    B = ref["bitstream"]
+
+    class QT:
+        def __init__(self, x, y, size):
+            self.x, self.y, self.size = x, y, size
+
+    rng = np.random.default_rng(20260416)
+    H, W = 72, 100   # tiles cover 128 x 128: some cross the image edge, two lie outside it
+    recon = rng.uniform(-0.05, 1.05, (H, W, 3)).astype(np.float32)
+    # (chroma mode, freq alpha, per-tile scales, layout, block version, presence probability)
+    cases = [(0, 0.0, False, 0, 5, 0.8), (1, 4.0, False, 1, 5, 0.8), (2, 4.0, True, 1, 5, 0.8),
+             (2, 0.0, True, 0, 5, 1.0), (2, 4.0, False, 1, 4, 0.7), (1, 0.0, False, 0, 3, 0.7),
+             (2, 4.0, False, 0, 2, 1.0), (0, 4.0, False, 1, 5, 0.0)]
+    out = {"recon": recon, "tiles": np.array(DCT_TILES, np.int32)}
+    for i, (chroma, alpha, scales, layout, version, p_present) in enumerate(cases):
+        present = [bool(rng.random() < p_present) for _ in DCT_TILES]
+        res = [rng.normal(0.0, 0.06, (s, s, 3)).astype(np.float32) for (_, _, s), p in zip(DCT_TILES, present) if p]
+        sizes = [s for (_, _, s), p in zip(DCT_TILES, present) if p]
+        su8 = bytes(int(v) for v in rng.integers(40, 220, len(res))) if scales else b""
+        sc = [R.decode_tile_scale_u8(b) for b in su8] if scales else None
+        coeffs, _ = R.encode_tile_residuals(res, quant_step=0.0135, freq_alpha=alpha, chroma_mode=chroma,
+                                            per_tile_scales=sc)
+        payload = R.permute_tile_to_band(coeffs, sizes, chroma) if layout else coeffs
+        mask = R._present_indices_to_bitmask(present)
+        if version == 5:
+            blob = B.pack_dct(payload, 0.0135, 3, freq_alpha=alpha, chroma_mode=chroma, presence_bitmask=mask,
+                              n_tiles=len(DCT_TILES), layout=layout, per_tile_scales_u8=su8)
+        elif version == 4:
+            blob = struct.pack("<BBBBffHII", 4, chroma, layout, 0, 0.0135, alpha, 3, len(DCT_TILES),
+                               payload.size) + mask + payload.astype("<i2").tobytes()
+        elif version == 3:
+            blob = struct.pack("<BBffHII", 3, chroma, 0.0135, alpha, 3, len(DCT_TILES),
+                               payload.size) + mask + payload.astype("<i2").tobytes()
+        else:
+            blob = struct.pack("<BBffHI", 2, chroma, 0.0135, alpha, 3, payload.size) + payload.astype("<i2").tobytes()
+        c, step, channels, falpha, cmode, pmask, n_hdr, lay, su = B.unpack_dct(blob)
+        if lay == 1:
+            pr = R._bitmask_to_present_indices(pmask, n_hdr) if (n_hdr > 0 and len(pmask) > 0) else [True] * 16
+            c = R.permute_band_to_tile(c, [s for (_, _, s), p in zip(DCT_TILES, pr) if p], cmode)
+        pts = [R.decode_tile_scale_u8(b) for b in su] if su else None
+        want = R.apply_residual_to_image(recon, c, [QT(*t) for t in DCT_TILES], quant_step=step, channels=channels,
+                                         freq_alpha=falpha, chroma_mode=cmode, presence_bitmask=pmask,
+                                         per_tile_scales=pts)
+        out[f"blob_{i}"] = np.frombuffer(blob, np.uint8)
+        out[f"out_{i}"] = want.astype(np.float32)
+    for j, ((h, w), (ow, oh)) in enumerate((((48, 64), (240, 135)), ((64, 96), (96, 200)), ((80, 100), (37, 29)),
+                                            ((17, 33), (200, 100)), ((50, 70), (70, 50)), ((31, 29), (300, 7)))):
+        u8 = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+        out[f"rs_in_{j}"] = u8
+        out[f"rs_out_{j}"] = np.asarray(Image.fromarray(u8).resize((ow, oh), Image.BILINEAR))
+    _save("dct.npz", **out)
+
+
+def gen_container_dct(ref) -> None:
+    """Reference encodes with the DCT residual layer (default flags, and with per-tile adaptive
+    quantization), decoded by the reference at the encoded size and at an up- and a
+    down-scaled target (the raster branch, src/weft/decoder.py:446-518)."""
+    from PIL import Image
+
+    from weft_b200.synth import make_image_u8
+
+    enc = ref["encoder"]
+    gr = ref["gpu_render"]
+    dec_mod = ref["decoder"]
+    prim_chunks = ref["prim_chunks"]
+    score, _ = _cpu_score_prepacked(ref)
+    saved = (gr.gpu_batch_score_prepacked, enc._get_persistent_worker_pool, dec_mod._decode_prim_payload)
+    gr.gpu_batch_score_prepacked = score
+    enc._get_persistent_worker_pool = lambda: None
+    dec_mod._decode_prim_payload = lambda weft: (
+        prim_chunks.decode_prim_payload(weft.prim_payload, weft.toc, weft.chunk_index), "cpu")
+    out = {}
+    try:
+        img_u8 = make_image_u8(96, 80, 10, 33)
+        out["image_u8"] = img_u8
+        for name, flags in (("a", {"dct_residual": True}),
+                            ("b", {"dct_residual": True, "dct_residual_adaptive_quant": True})):
+            with tempfile.TemporaryDirectory() as td:
+                src = os.path.join(td, "in.png")
+                Image.fromarray(img_u8).save(src)
+                fa = os.path.join(td, "a.weft")
+                enc.encode_image(src, fa, ref["EncodeConfig"](quality=75, feature_flags=flags))
+                out[f"file_{name}"] = np.frombuffer(open(fa, "rb").read(), np.uint8)
+                out[f"native_{name}"] = dec_mod.decode_to_array(fa).astype(np.float32)
+                out[f"up_{name}"] = dec_mod.decode_to_array(fa, 200, 150).astype(np.float32)
+                out[f"down_{name}"] = dec_mod.decode_to_array(fa, 50, 37).astype(np.float32)
+    finally:
+        gr.gpu_batch_score_prepacked, enc._get_persistent_worker_pool, dec_mod._decode_prim_payload = saved
+    _save("container_dct.npz", **out)
+
+
 def main() -> None:
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
     sys.path.insert(0, src)
     import weft.bitstream as bitstream_mod
+    import weft.dct_residual as dct_residual
     import weft.decoder as decoder
     import weft.encoder as encoder
     import weft.entropy as entropy
@@ -568,13 +681,14 @@ def main() -> None:
         "encoder": encoder, "entropy": entropy, "gpu_render": gpu_render, "prim_chunks": prim_chunks,
         "primitives": primitives, "quadtree": quadtree, "render": render,
         "Primitive": primitives.Primitive, "TileRecord": primitives.TileRecord, "EncodeConfig": EncodeConfig,
-        "decoder": decoder, "bitstream": bitstream_mod,
+        "decoder": decoder, "bitstream": bitstream_mod, "dct_residual": dct_residual,
     }
     which = set(sys.argv[2:]) if len(sys.argv) > 2 else None
     for name, fn in (("render_tiles", gen_render_tiles), ("render_scene", gen_render_scene), ("rate", gen_rate),
                      ("entropy", gen_entropy), ("quant", gen_quant), ("quadtree", gen_quadtree),
                      ("candidates", gen_candidates), ("fit", gen_fit),
-                     ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("container", gen_container)):
+                     ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("container", gen_container),
+                     ("dct", gen_dct), ("container_dct", gen_container_dct)):
         if which is None or name in which:
             fn(ref)
 

@@ -1,0 +1,59 @@
+"""The decoder's raster branch on the GPU: ``weftk_dct_apply`` and ``weftk_raster_resize`` against
+the reference's outputs (golden fixtures made by the reference and Pillow), and whole-file decodes
+of reference-written files that carry the DCT residual layer."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RESIZE_TARGETS = [(240, 135), (96, 200), (37, 29), (200, 100), (70, 50), (300, 7)]
+# float64 transform with fused multiply-adds against scipy's FFT: the float32 results may differ
+# in the last place
+APPLY_TOL = 2.5e-7
+
+
+@pytest.mark.parametrize("i", range(8))
+def test_dct_apply_matches_reference(golden, i):
+    import torch
+
+    from weft_b200 import raster
+
+    g = golden("dct.npz")
+    tiles = [tuple(int(v) for v in t) for t in g["tiles"]]
+    img = torch.from_numpy(g["recon"].copy()).cuda()
+    out = raster.apply_dct(img, g[f"blob_{i}"].tobytes(), tiles).cpu().numpy()
+    want = g[f"out_{i}"]
+    assert float(np.max(np.abs(out - want))) <= APPLY_TOL
+    assert float(out.min()) >= 0.0 and float(out.max()) <= 1.0
+
+
+@pytest.mark.parametrize("j", range(len(RESIZE_TARGETS)))
+def test_raster_resize_matches_pillow(golden, j):
+    import torch
+
+    from weft_b200 import raster
+
+    g = golden("dct.npz")
+    u8 = g[f"rs_in_{j}"]
+    src = torch.from_numpy((u8.astype(np.float32) + np.float32(0.5)) / np.float32(255.0)).cuda()
+    tw, th = RESIZE_TARGETS[j]
+    out = raster.resize(src, tw, th).cpu().numpy()
+    np.testing.assert_array_equal(out, g[f"rs_out_{j}"].astype(np.float32) / np.float32(255.0))
+
+
+@pytest.mark.parametrize("which", ["a", "b"])
+def test_decode_file_raster_branch_matches_reference_decoder(golden, which):
+    from weft_b200.encode import decode_file
+
+    g = golden("container_dct.npz")
+    blob = g[f"file_{which}"].tobytes()
+    for key, size in (("native", (None, None)), ("up", (200, 150)), ("down", (50, 37))):
+        got = decode_file(blob, *size)
+        want = g[f"{key}_{which}"]
+        assert got.shape == want.shape, key
+        # primitive walk parity is 1/255; after u8 truncation a walk difference moves a value by at
+        # most one step, and the resize keeps that bound
+        assert float(np.max(np.abs(got - want))) <= 1.0 / 255.0 + 1e-6, key

@@ -69,6 +69,11 @@ assert PRIM_DTYPE.itemsize == ctypes.sizeof(WeftPrim) == 60
 assert EVAL_DTYPE.itemsize == ctypes.sizeof(WeftEval) == 16
 FIT_ITEM_DTYPE = np.dtype([("tile", np.int32), ("block", np.int32), ("first", np.int32), ("count", np.int32)])
 assert TILE_DECODE_DTYPE.itemsize == ctypes.sizeof(WeftTileDecodeDesc) == 48
+# WeftDctTile (include/weftk_dct.h)
+DCT_TILE_DTYPE = np.dtype([("x", np.int32), ("y", np.int32), ("size", np.int32), ("_pad", np.int32),
+                           ("step_scale", np.float64), ("coef_base", np.int64, 3), ("coef_stride", np.int32, 3),
+                           ("_pad2", np.int32)])
+assert DCT_TILE_DTYPE.itemsize == 64
 assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8 + 16 + 8
 
 _P = ctypes.c_void_p
@@ -106,6 +111,8 @@ SIGNATURES: dict[str, list] = {
                           ctypes.c_float, _I, _P],
     "weftk_measure_fp32_peak": [_P],
     "weftk_fit_variant": [_I, _I, _P, _P, _P],
+    "weftk_dct_apply": [_P, _I, _P, _I64, _I, _I, ctypes.c_float, ctypes.c_float, _I, _P, _I, _I, _I, _P],
+    "weftk_raster_resize": [_P, _I, _I, _P, _I, _I, _P, _P],
 }
 
 _lock = threading.Lock()

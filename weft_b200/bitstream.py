@@ -28,6 +28,7 @@ import numpy as np
 MAGIC = b"WEFT"
 MAJOR, MINOR = 1, 4
 FLAG_DETERMINISTIC, FLAG_HAS_RES0, FLAG_HAS_RES1, FLAG_CHUNKED_PRIM = 1, 2, 4, 8
+FLAG_HAS_DCT = 1 << 9
 PROB_BITS = 12
 TOTFREQ = 1 << PROB_BITS
 RANS_L = 1 << 23
@@ -196,6 +197,7 @@ class WeftFile:
     res1_maps: list | None       # per tile (4, 4, 3) int8
     qtree: list                  # (x, y, size)
     meta: dict = field(default_factory=dict)
+    dct_payload: bytes | None = None   # BLOCK_DCT body (per-tile DCT residual layer)
 
 
 def _align(v: int, a: int) -> int:
@@ -352,7 +354,9 @@ def decode_weft(blob: bytes, device: int | None = None) -> WeftFile:
     qn = struct.unpack_from("<I", blocks[b"QTRE"], 0)[0]
     qtree = [struct.unpack_from("<HHB", blocks[b"QTRE"], 4 + 5 * i) for i in range(qn)]
     meta = json.loads(blocks[b"META"][4:].decode())
-    return WeftFile(w, h, quality, toc, prim_raw, residuals, res1, qtree, meta)
+    if (flags & FLAG_HAS_DCT) and b"DCT " not in blocks:
+        raise ValueError("HEAD indicates DCT but DCT block is missing")
+    return WeftFile(w, h, quality, toc, prim_raw, residuals, res1, qtree, meta, blocks.get(b"DCT "))
 
 
 def decode_tiles(prim_raw: bytes, toc) -> list[list[tuple]]:

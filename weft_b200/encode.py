@@ -68,7 +68,9 @@ def encode_fit(width, height, quality, tiles, patches, stacks, recon, with_res0=
 
 
 def decode_file(blob: bytes, target_width=None, target_height=None) -> np.ndarray:
-    """Decode a primitive-stack WEFT file with the GPU decoder walk (linear float32 RGB)."""
+    """Decode a primitive-stack WEFT file with the GPU decoder walk (linear float32 RGB); the target
+    defaults to the file's width and height.  A file with a DCT residual block takes the raster
+    branch: walk at the encoded size, DCT residual, u8 BILINEAR resize to the target."""
     wf = bitstream.decode_weft(blob)
     tiles = [type("QT", (), {"x": x, "y": y, "size": s})() for x, y, s in wf.qtree]
     stacks = bitstream.decode_tiles(wf.prim_raw, wf.toc)
@@ -79,7 +81,16 @@ def decode_file(blob: bytes, target_width=None, target_height=None) -> np.ndarra
     maps = [m.astype(np.float32) / 255.0 for m in wf.res1_maps] if wf.res1_maps is not None else None
     ew = int(wf.meta.get("encode_width", wf.width))
     eh = int(wf.meta.get("encode_height", wf.height))
-    return render.render_scene_adaptive(recs, tiles, ew, eh, maps, 4, target_width or ew, target_height or eh)
+    tw, th = int(target_width or wf.width), int(target_height or wf.height)
+    if wf.dct_payload is None:
+        return render.render_scene_adaptive(recs, tiles, ew, eh, maps, 4, tw, th)
+    # raster branch (src/weft/decoder.py:446-518): walk at the encoded size, add the DCT
+    # residual, then u8 + BILINEAR resize when the target differs
+    from . import raster
+
+    img = render.render_scene_device(recs, tiles, ew, eh, maps)
+    img = raster.apply_dct(img, wf.dct_payload, wf.qtree)
+    return raster.resize(img, tw, th).cpu().numpy()
 
 
 def rd_score(image: np.ndarray, blob: bytes, quality: int) -> dict:

@@ -142,6 +142,30 @@ def render_scene_adaptive(records, quad_tiles, width: int, height: int, residual
     return _launch(descs, prims, cp48, res1, th, tw)
 
 
+def render_scene_device(records, quad_tiles, width: int, height: int, residual_maps=None, device: int = 0):
+    """``render_scene_adaptive`` at the encoded size into a float32 CUDA tensor (h, w, 3), for the
+    raster branch that keeps working on the image on the device."""
+    import torch
+
+    descs, prims, cp48, res1, th, tw = build_scene(records, quad_tiles, width, height, residual_maps)
+    dev = torch.device("cuda", device)
+    out = torch.zeros((th, tw, 3), dtype=torch.float32, device=dev)
+    if len(descs) == 0:
+        return out
+    items = decode_items(descs)
+    t_d = torch.from_numpy(np.ascontiguousarray(descs, TILE_DECODE_DTYPE).view(np.uint8)).to(dev)
+    t_i = torch.from_numpy(items).to(dev)
+    t_p = torch.from_numpy(np.ascontiguousarray(prims, PRIM_DTYPE).view(np.uint8)).to(dev)
+    t_c = torch.from_numpy(np.ascontiguousarray(cp48, np.float32)).to(dev) if len(cp48) else None
+    n_res1 = 0 if res1 is None else len(res1)
+    t_r = torch.from_numpy(np.ascontiguousarray(res1, np.float32)).to(dev) if n_res1 else None
+    lib = _lib.lib_for_device(device)
+    _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_i), len(items), _lib.ptr(t_p),
+                                      _lib.ptr(t_c), len(cp48), _lib.ptr(t_r), n_res1, _lib.ptr(out), th, tw, 0,
+                                      torch.cuda.current_stream(dev).cuda_stream), "weftk_render_tiles")
+    return out
+
+
 def render_tile(prims, tile_size: int, residual_rgb=None, source_size: int | None = None) -> np.ndarray:
     """GPU render of one stack as a single tile (clipped, with optional RES0)."""
     ts = int(tile_size)

@@ -12,7 +12,8 @@ primitives per tile.  Pixels and candidate records are resident in HBM when a ti
 * ``plain``: the reference's greedy (init, rounds, device re-seeds) for all tiles at once, replayed
   from one CUDA graph;
 * also: e2e through the public API from host buffers, the FP32 rooflines of the scoring and refine
-  kernels, the decoder walk at 3840x2160, the 2048^2 differentiable-fit workload, an RD table of
+  kernels, the decoder walk at 3840x2160, the decoder's raster branch (DCT residual layer + u8
+  BILINEAR resize to 3840x2160), the 2048^2 differentiable-fit workload, an RD table of
   refined-fit variants, clocks during the timed region, and the CPU baseline (the numpy oracle of the
   reference's greedy on a bounded sample of the same tiles, all host cores).
 
@@ -261,6 +262,122 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
             "frac_of_fill": (12 * tw * th / (ms * 1e-3)) / (12 * tw * th / (fill_ms * 1e-3)),
             "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims)),
             "residuals": "RES0 + RES1 grids" if n_res1 else "none"}
+
+
+def synthetic_dct_block(tiles, quality: int, seed: int = 0) -> bytes:
+    """A BLOCK_DCT (format v5) covering every tile, in the reference encoder's default configuration
+    (YCbCr 4:2:0, frequency-weight alpha 4.0, tile-major layout, the quality's quant step): seeded
+    Laplacian coefficients whose scale falls with frequency, 6 / (1 + u + v), as a residual's do."""
+    import struct
+
+    rng = np.random.default_rng(seed)
+    parts = []
+    for t in tiles:
+        for n in (t.size, t.size // 2, t.size // 2):
+            f = np.arange(n, dtype=np.float64)
+            scale = 6.0 / (1.0 + f[:, None] + f[None, :])
+            parts.append(np.clip(np.round(rng.laplace(0.0, scale)), -32768, 32767).astype("<i2").reshape(-1))
+    coeffs = np.concatenate(parts)
+    q = max(10, min(99, int(quality)))
+    step = float(max(0.003, min(0.20, ((101 - q) / 100.0) ** 2 * 0.20)))
+    n = len(tiles)
+    mask = np.packbits(np.ones(n, np.uint8), bitorder="little").tobytes()
+    head = struct.pack("<BBBBffHIII", 5, 2, 0, 0, step, 4.0, 3, n, coeffs.size, 0)
+    return head + mask + coeffs.tobytes()
+
+
+def raster_bench(fit, tiles, patches, size, out_w, out_h, iters, peak):
+    """The decoder's raster branch (a file with a DCT residual layer, decoded at another size): walk at
+    the encoded size, DCT layer, u8 + BILINEAR resize, on a synthetic DCT block over every tile."""
+    import ctypes
+
+    import torch
+
+    from weft_b200 import _lib, raster
+    from weft_b200.encode import residuals_from_recon
+    from weft_b200.render import build_scene, decode_items
+
+    class _Rec:
+        __slots__ = ("primitives", "residual_rgb")
+
+        def __init__(self, p, r):
+            self.primitives, self.residual_rgb = p, r
+
+    res0, res1 = residuals_from_recon(patches, fit.recon_tiles())
+    recs = [_Rec(st, r) for st, r in zip(fit.selected(), res0)]
+    maps = [g.astype(np.float32) / np.float32(255.0) for g in res1]
+    descs, prims, cp48, res1_tab, th, tw = build_scene(recs, tiles, size, size, maps)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = _lib.lib_for_device(dev.index)
+    stream = torch.cuda.current_stream()
+    t_d = torch.from_numpy(descs.view(np.uint8)).to(dev)
+    t_p = torch.from_numpy(prims.view(np.uint8)).to(dev)
+    t_c = torch.from_numpy(np.ascontiguousarray(cp48)).to(dev) if len(cp48) else None
+    t_r = torch.from_numpy(np.ascontiguousarray(res1_tab)).to(dev)
+    items = decode_items(descs)
+    t_i = torch.from_numpy(items).to(dev)
+    img = torch.zeros((th, tw, 3), dtype=torch.float32, device=dev)
+    base = torch.empty_like(img)
+    out = torch.empty((out_h, out_w, 3), dtype=torch.float32, device=dev)
+    tmp = torch.empty(th * out_w * 3, dtype=torch.uint8, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    layer = raster.DctLaunch(synthetic_dct_block(tiles, QUALITY), [(t.x, t.y, t.size) for t in tiles], tw, th,
+                             dev.index)
+
+    def walk():
+        _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_i), len(items), _lib.ptr(t_p),
+                                          _lib.ptr(t_c), len(cp48), _lib.ptr(t_r), len(res1_tab), _lib.ptr(img),
+                                          th, tw, 0, stream.cuda_stream), "weftk_render_tiles")
+
+    def timed(fn, prep=None):
+        for _ in range(3):
+            if prep:
+                prep()
+            fn()
+        times = []
+        for _ in range(iters):
+            if prep:
+                prep()
+            flush.fill_(1.0)
+            torch.cuda._sleep(100000)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        return statistics.median(times)
+
+    st = ctypes.c_int(0)
+    lib.weftk_device_status(ctypes.addressof(st))
+    walk()
+    base.copy_(img)
+    apply_ms = timed(lambda: layer.run(img, stream.cuda_stream), prep=lambda: img.copy_(base))
+    resize_ms = timed(lambda: raster.resize_into(img, out, tmp, stream.cuda_stream))
+
+    def whole():
+        walk()
+        layer.run(img, stream.cuda_stream)
+        raster.resize_into(img, out, tmp, stream.cuda_stream)
+
+    whole_ms = timed(whole)
+    torch.cuda.synchronize()
+    _lib.check(lib.weftk_device_status(ctypes.addressof(st)), "weftk_device_status")
+    if st.value:
+        raise RuntimeError("the raster branch reported a bad descriptor")
+    rbytes = 12 * tw * th + 2 * 3 * th * out_w + 12 * out_w * out_h
+    gbs = rbytes / (resize_ms * 1e-3) / 1e9
+    peak_gbs, peak_source = peak
+    return {"encoded": f"{tw}x{th}", "target": f"{out_w}x{out_h}", "ms": whole_ms,
+            "mpix_per_s": out_w * out_h / (whole_ms * 1e-3) / 1e6,
+            "launches": 1 + layer.launches + 2,
+            "dct_apply": {"ms": apply_ms, "tiles": len(layer.descs), "coefficients": int(layer.block.coeffs.size),
+                          "fp64_flops": layer.flops(), "fp64_tflops": layer.flops() / (apply_ms * 1e-3) / 1e12,
+                          "launches": layer.launches},
+            "resize": {"ms": resize_ms, "bytes": rbytes, "achieved_gbs": gbs, "peak_gbs": peak_gbs,
+                       "frac": gbs / peak_gbs, "peak_source": peak_source},
+            "payload": "synthetic BLOCK_DCT v5 over every tile (4:2:0, alpha 4, q75 step, Laplacian coefficients)",
+            "l2": "256 MiB written between timed launches"}
 
 
 def _recon_of(stack_set, params, tiles, size):
@@ -800,6 +917,13 @@ def run_weft(args, world, rank, local, executor, cores):
                          f"{wall:.1f} s wall on {cores} processes"}
     if rank != 0:
         return
+    # the raster branch is timed last, so that a failure in it leaves every number above intact
+    raster_line = None
+    if args.decode_iters > 0:
+        try:
+            raster_line = raster_bench(fit, tiles, patches, args.size, 3840, 2160, args.decode_iters, _hbm_peak())
+        except Exception as e:  # reported in the line instead of ending the run
+            raster_line = {"error": f"{type(e).__name__}: {e}"}
     score_roof = {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
                   "frac": achieved_tflops / peak_tflops if peak_tflops else None, "traffic": None,
                   "kernel": "fit_score_kernel (3 tile-size classes), plain fit",
@@ -856,6 +980,7 @@ def run_weft(args, world, rank, local, executor, cores):
                              for k, v in (fast.tuning or {}).items()},
         "decode": decode,
         "decode_with_residuals": decode_res,
+        "decode_raster": raster_line,
         "differentiable_fit": diff,
         "image_batch": ibatch,
         "rd": rd,

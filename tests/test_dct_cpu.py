@@ -206,3 +206,99 @@ def test_legacy_block_versions_parse():
     v3 = struct.pack("<BBffHII", 3, 2, 0.02, 0.0, 3, 9, coeffs.size) + b"\xff\x01" + coeffs.tobytes()
     b = raster.unpack_dct(v3)
     assert (b.chroma_mode, b.layout, b.n_tiles, b.presence_bitmask) == (2, 0, 9, b"\xff\x01")
+
+
+class _RecordingLib:
+    """Stands in for libweftk: checks each call against the bound signature and records it."""
+
+    def __init__(self):
+        self.calls = []
+
+    def __getattr__(self, name):
+        def call(*args):
+            sig = _lib.SIGNATURES[name]
+            assert len(args) == len(sig), name
+            for a, t in zip(args, sig):
+                t.from_param(a)  # raises on a type ctypes would reject
+            self.calls.append((name, args))
+            return 0
+        return call
+
+
+def test_dct_launch_enqueues_one_launch_per_tile_side(golden):
+    """Host marshalling of ``DctLaunch.run`` with host arrays in place of device buffers."""
+    g = golden("dct.npz")
+    tiles = [tuple(int(v) for v in t) for t in g["tiles"]]
+    layer = object.__new__(raster.DctLaunch)
+    layer.block = raster.unpack_dct(_blob(g, 1))
+    layer.descs = raster.tile_table(layer.block, tiles, 100, 72)
+    layer.width, layer.height = 100, 72
+    layer.lib = _RecordingLib()
+    layer.t_coeffs = layer.block.coeffs
+    layer.t_descs = layer.descs.view(np.uint8)
+    sizes = layer.descs["size"]
+    layer.groups = [(int(v), int(np.searchsorted(sizes, v, "left")), int(np.searchsorted(sizes, v, "right")))
+                    for v in np.unique(sizes)]
+    img = np.zeros((72, 100, 3), np.float32)
+    layer.run(img, 0)
+    calls = layer.lib.calls
+    assert len(calls) == layer.launches == len(np.unique(sizes)) + 1
+    base = layer.t_descs.ctypes.data
+    seen = 0
+    for (name, a), (s, lo, hi) in zip(calls, layer.groups):
+        assert name == "weftk_dct_apply"
+        assert a[0] == base + 64 * lo and a[1] == hi - lo and a[8] == s and a[12] == 0
+        assert np.all(layer.descs["size"][lo:hi] == s)
+        seen += hi - lo
+    assert seen == len(layer.descs)
+    name, a = calls[-1]
+    assert name == "weftk_dct_apply" and a[1] == 0 and a[12] == 1 and a[9] == img.ctypes.data
+    n = raster._channel_sides(layer.descs["size"].astype(np.int64), layer.block.chroma_mode)
+    assert layer.flops() == pytest.approx(float(np.sum(4.0 * n.astype(np.float64) ** 3)))
+
+
+def test_resize_into_checks_scratch_and_marshals(monkeypatch):
+    rec = _RecordingLib()
+    monkeypatch.setattr(_lib, "lib_for_device", lambda device=0: rec)
+
+    class _T:
+        """Minimal tensor stand-in: shape, numel, device index and a data pointer."""
+
+        def __init__(self, shape, n):
+            self.shape, self._n = shape, n
+            self.device = type("D", (), {"index": 0})()
+            self.buf = np.zeros(max(n, 1), np.uint8)
+
+        def numel(self):
+            return self._n
+
+        def data_ptr(self):
+            return self.buf.ctypes.data
+
+    src, out = _T((48, 64, 3), 48 * 64 * 3), _T((135, 240, 3), 135 * 240 * 3)
+    with pytest.raises(ValueError, match="scratch"):
+        raster.resize_into(src, out, _T((1,), 48 * 240 * 3 - 1), 0)
+    raster.resize_into(src, out, _T((1,), 48 * 240 * 3), 0)
+    name, a = rec.calls[-1]
+    assert name == "weftk_raster_resize" and a[1:3] == (64, 48) and a[4:6] == (240, 135)
+
+
+def test_bench_synthetic_dct_block_is_a_valid_block():
+    """The bench's raster-branch payload parses, covers every tile and decodes with the oracle."""
+    import bench
+    from weft_b200 import quadtree
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 128, 30, 3)
+    img = srgb_u8_to_linear(u8)
+    tiles = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    blob = bench.synthetic_dct_block(tiles, 75)
+    block = raster.unpack_dct(blob)
+    assert (block.chroma_mode, block.layout, block.freq_alpha, block.n_tiles) == (2, 0, 4.0, len(tiles))
+    assert block.quant_step == pytest.approx(0.01352, rel=1e-6)
+    qt = [(t.x, t.y, t.size) for t in tiles]
+    descs = raster.tile_table(block, qt, 128, 128)
+    assert len(descs) == len(tiles)
+    out = odct.apply_dct_block(img, blob, qt)
+    assert out.shape == img.shape and 0.0 <= out.min() and out.max() <= 1.0
+    assert 0.0 < float(np.sqrt(np.mean((out - np.clip(img, 0, 1)) ** 2))) < 0.2

@@ -156,6 +156,48 @@ def tile_table(block: DctBlock, quad_tiles, width: int, height: int) -> np.ndarr
     return d[np.argsort(d["size"], kind="stable")]
 
 
+class DctLaunch:
+    """A BLOCK_DCT bound to a tile list and an image size, with its descriptors and coefficients
+    resident on the device; ``run`` enqueues the layer (one ``weftk_dct_apply`` launch per tile
+    side, then the whole-image clip) without host synchronisation."""
+
+    def __init__(self, payload: bytes, quad_tiles, width: int, height: int, device: int = 0):
+        import torch
+
+        self.block = unpack_dct(payload)
+        self.descs = tile_table(self.block, quad_tiles, width, height)
+        self.width, self.height = int(width), int(height)
+        self.device = torch.device("cuda", device)
+        self.lib = _lib.lib_for_device(device)
+        c = self.block.coeffs if self.block.coeffs.size else np.zeros(1, np.int16)
+        self.t_coeffs = torch.from_numpy(c).to(self.device)
+        self.t_descs = torch.from_numpy(self.descs.view(np.uint8)).to(self.device) if len(self.descs) else None
+        sizes = self.descs["size"]
+        self.groups = [(int(v), int(np.searchsorted(sizes, v, "left")), int(np.searchsorted(sizes, v, "right")))
+                       for v in np.unique(sizes)]
+
+    @property
+    def launches(self) -> int:
+        return len(self.groups) + 1
+
+    def flops(self) -> float:
+        """Float64 operations of the two transform passes: 2 n^3 multiply-adds per n x n block."""
+        n = _channel_sides(self.descs["size"].astype(np.int64), self.block.chroma_mode).astype(np.float64)
+        return float(np.sum(4.0 * n ** 3))
+
+    def run(self, image, stream: int, clip_all: bool = True) -> None:
+        b = self.block
+        for s, lo, hi in self.groups:
+            _lib.check(self.lib.weftk_dct_apply(_lib.ptr(self.t_descs) + lo * DCT_TILE_DTYPE.itemsize, hi - lo,
+                                                _lib.ptr(self.t_coeffs), int(b.coeffs.size), b.chroma_mode, b.layout,
+                                                b.quant_step, b.freq_alpha, s, _lib.ptr(image), self.width,
+                                                self.height, 0, stream), "weftk_dct_apply")
+        if clip_all:
+            _lib.check(self.lib.weftk_dct_apply(0, 0, 0, 0, b.chroma_mode, b.layout, b.quant_step, b.freq_alpha, 4,
+                                                _lib.ptr(image), self.width, self.height, 1, stream),
+                       "weftk_dct_apply")
+
+
 def apply_dct(image, payload: bytes, quad_tiles, clip_all: bool = True):
     """Add a BLOCK_DCT's residual to ``image`` (torch float32 CUDA tensor, (h, w, 3)) in place and
     return it; ``clip_all`` clips the whole image to [0, 1] as the reference does."""
@@ -165,32 +207,27 @@ def apply_dct(image, payload: bytes, quad_tiles, clip_all: bool = True):
         raise ValueError("image must be a float32 (h, w, 3) CUDA tensor")
     image = image.contiguous() if not image.is_contiguous() else image
     h, w = int(image.shape[0]), int(image.shape[1])
-    block = unpack_dct(payload)
-    descs = tile_table(block, quad_tiles, w, h)
-    dev = image.device
-    lib = _lib.lib_for_device(dev.index)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    t_c = torch.from_numpy(block.coeffs if block.coeffs.size else np.zeros(1, np.int16)).to(dev)
+    layer = DctLaunch(payload, quad_tiles, w, h, image.device.index)
     status = ctypes.c_int(0)
-    lib.weftk_device_status(ctypes.addressof(status))  # clear any earlier report
-    if len(descs):
-        t_d = torch.from_numpy(descs.view(np.uint8)).to(dev)
-        sizes = descs["size"]
-        for s in np.unique(sizes):
-            lo = int(np.searchsorted(sizes, s, "left"))
-            hi = int(np.searchsorted(sizes, s, "right"))
-            _lib.check(lib.weftk_dct_apply(_lib.ptr(t_d) + lo * DCT_TILE_DTYPE.itemsize, hi - lo, _lib.ptr(t_c),
-                                           int(block.coeffs.size), block.chroma_mode, block.layout,
-                                           block.quant_step, block.freq_alpha, int(s), _lib.ptr(image), w, h, 0,
-                                           stream), "weftk_dct_apply")
-    if clip_all:
-        _lib.check(lib.weftk_dct_apply(0, 0, 0, 0, block.chroma_mode, block.layout, block.quant_step,
-                                       block.freq_alpha, 4, _lib.ptr(image), w, h, 1, stream), "weftk_dct_apply")
-    if len(descs):
-        _lib.check(lib.weftk_device_status(ctypes.addressof(status)), "weftk_device_status")
+    layer.lib.weftk_device_status(ctypes.addressof(status))  # clear any earlier report
+    layer.run(image, torch.cuda.current_stream(image.device).cuda_stream, clip_all)
+    if len(layer.descs):
+        _lib.check(layer.lib.weftk_device_status(ctypes.addressof(status)), "weftk_device_status")
         if status.value:
             raise ValueError("a DCT tile reads past its coefficient stream or has an unsupported side")
     return image
+
+
+def resize_into(image, out, tmp, stream: int) -> None:
+    """Enqueue ``weftk_raster_resize`` from ``image`` (h, w, 3) into ``out`` (H, W, 3) with the caller's
+    u8 scratch ``tmp`` of h * W * 3 bytes."""
+    h, w = int(image.shape[0]), int(image.shape[1])
+    th, tw = int(out.shape[0]), int(out.shape[1])
+    if tmp.numel() < h * tw * 3:
+        raise ValueError("resize scratch too small")
+    lib = _lib.lib_for_device(image.device.index)
+    _lib.check(lib.weftk_raster_resize(_lib.ptr(image), w, h, _lib.ptr(out), tw, th, _lib.ptr(tmp), stream),
+               "weftk_raster_resize")
 
 
 def resize(image, target_w: int, target_h: int):
@@ -201,10 +238,7 @@ def resize(image, target_w: int, target_h: int):
     if (target_w, target_h) == (w, h):
         return image
     image = image.contiguous()
-    dev = image.device
-    out = torch.empty((target_h, target_w, 3), dtype=torch.float32, device=dev)
-    tmp = torch.empty(h * target_w * 3, dtype=torch.uint8, device=dev)
-    lib = _lib.lib_for_device(dev.index)
-    _lib.check(lib.weftk_raster_resize(_lib.ptr(image), w, h, _lib.ptr(out), target_w, target_h, _lib.ptr(tmp),
-                                       torch.cuda.current_stream(dev).cuda_stream), "weftk_raster_resize")
+    out = torch.empty((target_h, target_w, 3), dtype=torch.float32, device=image.device)
+    tmp = torch.empty(h * target_w * 3, dtype=torch.uint8, device=image.device)
+    resize_into(image, out, tmp, torch.cuda.current_stream(image.device).cuda_stream)
     return out

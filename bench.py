@@ -14,8 +14,9 @@ primitives per tile.  Pixels and candidate records are resident in HBM when a ti
 * also: e2e through the public API from host buffers, the FP32 rooflines of the scoring and refine
   kernels, the decoder walk at 3840x2160, the decoder's raster branch (DCT residual layer + u8
   BILINEAR resize to 3840x2160), the 2048^2 differentiable-fit workload, an RD table of
-  refined-fit variants, clocks during the timed region, and the CPU baseline (the numpy oracle of the
-  reference's greedy on a bounded sample of the same tiles, all host cores).
+  refined-fit variants, clocks during the timed region, and the CPU baselines (the numpy oracle of the
+  reference's greedy on a bounded sample of the same tiles, all host cores; the oracle decoder walk and
+  raster branch on one core).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl weft|reference]
 
@@ -378,6 +379,45 @@ def raster_bench(fit, tiles, patches, size, out_w, out_h, iters, peak):
                        "frac": gbs / peak_gbs, "peak_source": peak_source},
             "payload": "synthetic BLOCK_DCT v5 over every tile (4:2:0, alpha 4, q75 step, Laplacian coefficients)",
             "l2": "256 MiB written between timed launches"}
+
+
+def cpu_decode_baselines(fit, tiles, patches, size, out_w, out_h) -> tuple[dict, dict]:
+    """CPU baselines of the two decode lines, one process each (the reference decoder is single
+    threaded numpy): the oracle's analytic walk at the output size (no residual grids, like the
+    ``decode`` line), and the raster branch of ``decode_raster`` -- oracle walk at the encoded size with
+    RES0/RES1, oracle DCT layer on the same synthetic block, then u8 and Pillow's own BILINEAR resize."""
+    from PIL import Image
+
+    from oracle import dct as odct
+    from oracle import render as orender
+    from weft_b200.encode import residuals_from_recon
+
+    class _Rec:
+        __slots__ = ("primitives", "residual_rgb")
+
+        def __init__(self, p, r):
+            self.primitives, self.residual_rgb = p, r
+
+    sel = fit.selected()
+    t0 = time.perf_counter()
+    orender.render_scene_adaptive([_Rec(st, (0, 0, 0)) for st in sel], tiles, size, size, None, 4, out_w, out_h)
+    walk_s = time.perf_counter() - t0
+    res0, res1 = residuals_from_recon(patches, fit.recon_tiles())
+    maps = [g.astype(np.float32) / np.float32(255.0) for g in res1]
+    payload = synthetic_dct_block(tiles, QUALITY)
+    t0 = time.perf_counter()
+    img = orender.render_scene_adaptive([_Rec(st, r) for st, r in zip(sel, res0)], tiles, size, size, maps, 4)
+    img = odct.apply_dct_block(img, payload, [(t.x, t.y, t.size) for t in tiles])
+    u8 = np.clip(img * np.float32(255.0), 0.0, 255.0).astype(np.uint8)
+    np.asarray(Image.fromarray(u8).resize((out_w, out_h), Image.BILINEAR), dtype=np.float32) / np.float32(255.0)
+    raster_s = time.perf_counter() - t0
+    px = out_w * out_h
+    walk = {"value": px / walk_s / 1e6, "unit": "MPix/s", "ms": walk_s * 1e3, "cores": 1, "kind": "port",
+            "sample": f"oracle render_scene_adaptive of the whole scene at {out_w}x{out_h}, one process"}
+    raster = {"value": px / raster_s / 1e6, "unit": "MPix/s", "ms": raster_s * 1e3, "cores": 1, "kind": "port",
+              "sample": f"oracle walk at {size}x{size} with RES0/RES1 + oracle DCT layer + Pillow BILINEAR to "
+                        f"{out_w}x{out_h}, one process"}
+    return walk, raster
 
 
 def _recon_of(stack_set, params, tiles, size):
@@ -909,7 +949,10 @@ def run_weft(args, world, rank, local, executor, cores):
     ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None
 
     cpu = None
+    dec_cpu = ras_cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        if args.decode_iters > 0:
+            dec_cpu, ras_cpu = cpu_decode_baselines(fit, tiles, patches, args.size, 3840, 2160)
         pick = cpu_sample(patches, pools, args.cpu_budget_s, executor)
         v, wall, px = run_cpu(patches, pools, pick, executor, cores)
         cpu = {"value": v, "unit": "MPix/s", "cores": cores, "kind": "port",
@@ -924,6 +967,10 @@ def run_weft(args, world, rank, local, executor, cores):
             raster_line = raster_bench(fit, tiles, patches, args.size, 3840, 2160, args.decode_iters, _hbm_peak())
         except Exception as e:  # reported in the line instead of ending the run
             raster_line = {"error": f"{type(e).__name__}: {e}"}
+        if ras_cpu is not None:
+            raster_line["cpu_baseline"] = ras_cpu
+    if decode is not None and dec_cpu is not None:
+        decode["cpu_baseline"] = dec_cpu
     score_roof = {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
                   "frac": achieved_tflops / peak_tflops if peak_tflops else None, "traffic": None,
                   "kernel": "fit_score_kernel (3 tile-size classes), plain fit",

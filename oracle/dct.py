@@ -146,40 +146,51 @@ def idct_matrix(n: int) -> np.ndarray:
     return a
 
 
-def dequant_idct(q: np.ndarray, step: float, alpha: float, scale: float | None) -> np.ndarray:
-    """Dequantize one (n, n) int16 block and inverse-DCT it to float32
-    (src/weft/dct_residual.py:513-547)."""
-    n = q.shape[0]
+def dequant_idct(q: np.ndarray, step: float, alpha: float, scales) -> np.ndarray:
+    """Dequantize a stack of (n, n) int16 blocks and inverse-DCT them to float32; ``scales`` is
+    None or one per-tile factor per block (src/weft/dct_residual.py:513-547)."""
+    n = q.shape[-1]
     grid = step * freq_weights(n, alpha) if alpha > 0 else np.full((n, n), step)
-    if scale is not None:
-        grid = grid * scale
+    grid = grid[None] if scales is None else grid[None] * np.asarray(scales, np.float64)[:, None, None]
     a = idct_matrix(n)
     return (a.T @ (q.astype(np.float64) * grid) @ a).astype(np.float32)
 
 
 def decode_tile_residuals(coeffs, sizes, quant_step, channels=3, freq_alpha=0.0, chroma_mode=0,
                           per_tile_scales=None) -> list[np.ndarray]:
-    """Per-tile (size, size, 3) float32 RGB residuals (src/weft/dct_residual.py:550-701)."""
+    """Per-tile (size, size, 3) float32 RGB residuals, tiles bucketed by size and each bucket
+    transformed as one stack (src/weft/dct_residual.py:550-701)."""
     if chroma_mode not in (0, 1, 2):
         raise ValueError(f"bad chroma_mode: {chroma_mode}")
-    out, cur = [], 0
+    sizes = [int(s) for s in sizes]
+    if per_tile_scales is not None and len(per_tile_scales) != len(sizes):
+        raise ValueError("per_tile_scales length does not match tile_sizes length")
+    buckets: dict[int, tuple[list[int], list[list[np.ndarray]]]] = {}
+    cur = 0
     for t, s in enumerate(sizes):
-        sc = None if per_tile_scales is None else float(per_tile_scales[t])
-        blocks = []
+        idx, blocks = buckets.setdefault(s, ([], [[], [], []]))
+        idx.append(t)
         for c, n in enumerate(channel_sizes(s, chroma_mode)):
-            q = coeffs[cur:cur + n * n].reshape(n, n)
+            blocks[c].append(coeffs[cur:cur + n * n].reshape(n, n))
             cur += n * n
+    out: list[np.ndarray] = [None] * len(sizes)  # type: ignore[list-item]
+    for s, (idx, blocks) in buckets.items():
+        sc = None if per_tile_scales is None else [float(per_tile_scales[t]) for t in idx]
+        chans = []
+        for c in range(3):
             st = quant_step if (chroma_mode == 0 or c == 0) else quant_step * CHROMA_QUANT_SCALE
-            blocks.append(dequant_idct(q, st, freq_alpha, sc))
+            chans.append(dequant_idct(np.stack(blocks[c]), st, freq_alpha, sc))
         if chroma_mode == 0:
-            out.append(np.stack(blocks, axis=-1))
-            continue
-        y, cb, cr = blocks
-        if chroma_mode == 2:
-            cb = np.repeat(np.repeat(cb, 2, axis=0), 2, axis=1)
-            cr = np.repeat(np.repeat(cr, 2, axis=0), 2, axis=1)
-        ycc = np.stack([y, cb, cr], axis=-1).astype(np.float64)
-        out.append((ycc @ YCBCR_TO_RGB.T).astype(np.float32))
+            rgb = np.stack(chans, axis=-1)
+        else:
+            y, cb, cr = chans
+            if chroma_mode == 2:
+                cb = np.repeat(np.repeat(cb, 2, axis=-2), 2, axis=-1)
+                cr = np.repeat(np.repeat(cr, 2, axis=-2), 2, axis=-1)
+            ycc = np.stack([y, cb, cr], axis=-1).astype(np.float64)
+            rgb = (ycc @ YCBCR_TO_RGB.T).astype(np.float32)
+        for j, t in enumerate(idx):
+            out[t] = rgb[j]
     return out
 
 

@@ -302,3 +302,28 @@ def test_bench_synthetic_dct_block_is_a_valid_block():
     out = odct.apply_dct_block(img, blob, qt)
     assert out.shape == img.shape and 0.0 <= out.min() and out.max() <= 1.0
     assert 0.0 < float(np.sqrt(np.mean((out - np.clip(img, 0, 1)) ** 2))) < 0.2
+
+
+def test_bench_cpu_decode_baselines_run_on_a_small_scene():
+    """The bench's CPU decode baselines on a 128² scene with a stand-in fit (tile-mean constants)."""
+    import bench
+    from oracle import render as orender
+    from weft_b200 import quadtree
+    from weft_b200.candidates import Cand
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 128, 30, 4)
+    img = srgb_u8_to_linear(u8)
+    tiles = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, tiles, 64)
+
+    class Fit:
+        def selected(self):
+            return [[Cand(0, (), tuple(float(v) for v in p.reshape(-1, 3).mean(0)), None, 1.0)] for p in patches]
+
+        def recon_tiles(self):
+            return [orender.render_tile(s, p.shape[0]) for s, p in zip(self.selected(), patches)]
+
+    walk, ras = bench.cpu_decode_baselines(Fit(), tiles, patches, 128, 480, 270)
+    for d in (walk, ras):
+        assert d["value"] > 0 and d["unit"] == "MPix/s" and d["cores"] == 1 and d["kind"] == "port"

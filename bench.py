@@ -322,8 +322,8 @@ def raster_bench(fit, tiles, patches, size, out_w, out_h, iters, peak):
     out = torch.empty((out_h, out_w, 3), dtype=torch.float32, device=dev)
     tmp = torch.empty(th * out_w * 3, dtype=torch.uint8, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    layer = raster.DctLaunch(synthetic_dct_block(tiles, QUALITY), [(t.x, t.y, t.size) for t in tiles], tw, th,
-                             dev.index)
+    layer = raster.DctLaunch.from_payload(synthetic_dct_block(tiles, QUALITY), [(t.x, t.y, t.size) for t in tiles],
+                                          tw, th, dev.index)
 
     def walk():
         _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_i), len(items), _lib.ptr(t_p),

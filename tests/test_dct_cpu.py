@@ -327,3 +327,28 @@ def test_bench_cpu_decode_baselines_run_on_a_small_scene():
     walk, ras = bench.cpu_decode_baselines(Fit(), tiles, patches, 128, 480, 270)
     for d in (walk, ras):
         assert d["value"] > 0 and d["unit"] == "MPix/s" and d["cores"] == 1 and d["kind"] == "port"
+
+
+def test_tile_table_with_float_scales_matches_u8_scales(golden):
+    """The drop-in path passes the reference's float ``per_tile_scales``; the descriptors equal those
+    built from the block's u8 scales."""
+    g = golden("dct.npz")
+    tiles = [tuple(int(v) for v in t) for t in g["tiles"]]
+    block = raster.unpack_dct(_blob(g, 2))
+    assert block.scales_u8
+    a = raster.tile_table(block, tiles, 100, 72)
+    b = raster.tile_table(raster.DctBlock(**{**block.__dict__, "scales_u8": b""}), tiles, 100, 72,
+                          scales=[odct.tile_scale(u) for u in block.scales_u8])
+    np.testing.assert_array_equal(a, b)
+    with pytest.raises(ValueError, match="per_tile_scales"):
+        raster.tile_table(block, tiles, 100, 72, scales=[1.0])
+
+
+def test_install_raster_into_swaps_the_reference_entry():
+    import types
+
+    import weft_b200
+
+    mod = types.SimpleNamespace(apply_residual_to_image=None)
+    weft_b200.install_raster_into(mod)
+    assert mod.apply_residual_to_image is raster.apply_residual_to_image

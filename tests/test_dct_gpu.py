@@ -60,3 +60,31 @@ def test_decode_file_raster_branch_matches_reference_decoder(golden, which):
         # primitive walk parity is 1/255; after u8 truncation a walk difference moves a value by at
         # most one step, and the resize keeps that bound
         assert float(np.max(np.abs(got - want))) <= 1.0 / 255.0 + 1e-6, key
+
+
+@pytest.mark.parametrize("i", range(8))
+def test_drop_in_apply_residual_to_image(golden, i):
+    """The reference decoder's own steps (unpack, undo the band layout, decode the u8 scales) feeding
+    the drop-in ``apply_residual_to_image``."""
+    from oracle import dct as odct
+    from weft_b200 import raster
+
+    g = golden("dct.npz")
+    tiles = [tuple(int(v) for v in t) for t in g["tiles"]]
+    d = odct.unpack_dct(g[f"blob_{i}"].tobytes())
+    coeffs = d["coeffs"]
+    if d["layout"] == 1:
+        pres = odct.presence(d["mask"], d["n_tiles"]) if (d["n_tiles"] and d["mask"]) else [True] * len(tiles)
+        coeffs = odct.permute_band_to_tile(coeffs, [s for (_, _, s), p in zip(tiles, pres) if p], d["chroma_mode"])
+    scales = [odct.tile_scale(u) for u in d["scales_u8"]] if d["scales_u8"] else None
+
+    class QT:
+        def __init__(self, x, y, size):
+            self.x, self.y, self.size = x, y, size
+
+    out = raster.apply_residual_to_image(g["recon"], coeffs, [QT(*t) for t in tiles], quant_step=d["quant_step"],
+                                         channels=d["channels"], freq_alpha=d["freq_alpha"],
+                                         chroma_mode=d["chroma_mode"], presence_bitmask=d["mask"],
+                                         per_tile_scales=scales)
+    assert out.dtype == np.float32
+    assert float(np.max(np.abs(out - g[f"out_{i}"]))) <= APPLY_TOL

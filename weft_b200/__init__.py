@@ -5,11 +5,12 @@ Modules:
   fit         batched, device-resident greedy candidate-scoring fit
   refine      hand-written backward + Adam refinement of fitted stacks
   render      the decoder's primitive walk on the GPU
+  raster      the decoder's raster branch: DCT residual layer and u8 BILINEAR resize on the GPU
   candidates  the reference's candidate generators (host, numpy)
   quadtree    tile layout; rate: lambda / bits / RD score; synth: test images
 """
 
-__all__ = ["install_into"]
+__all__ = ["install_into", "install_raster_into"]
 
 
 def install_into(gpu_render_module) -> None:
@@ -22,3 +23,12 @@ def install_into(gpu_render_module) -> None:
 
     for name in ("gpu_batch_score_prepacked", "gpu_batch_objectives", "gpu_render_tiles_to_image"):
         setattr(gpu_render_module, name, getattr(g, name))
+
+
+def install_raster_into(dct_residual_module) -> None:
+    """Replace ``apply_residual_to_image`` in ``dct_residual_module`` (``weft.dct_residual``) with the
+    GPU layer.  The reference decoder imports it inside its DCT branch (src/weft/decoder.py:477-486),
+    so the swap takes effect on the next decode."""
+    from . import raster
+
+    dct_residual_module.apply_residual_to_image = raster.apply_residual_to_image

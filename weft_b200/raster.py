@@ -94,12 +94,13 @@ def _channel_sides(size: np.ndarray, chroma_mode: int) -> np.ndarray:
     return np.stack([size, half, half], axis=1)
 
 
-def tile_table(block: DctBlock, quad_tiles, width: int, height: int) -> np.ndarray:
+def tile_table(block: DctBlock, quad_tiles, width: int, height: int, scales=None) -> np.ndarray:
     """Descriptors (``DCT_TILE_DTYPE``) of the tiles that carry coefficients and touch the image,
     sorted by tile side.
 
     ``quad_tiles``: (x, y, size) per tile in quadtree order, the order the coefficient stream
-    follows."""
+    follows.  ``scales``: per-present-tile quant-step factors as floats, instead of the block's u8
+    scales (the reference's ``per_tile_scales`` argument)."""
     if block.chroma_mode not in (0, 1, 2):
         raise ValueError(f"bad chroma_mode: {block.chroma_mode}")
     if block.layout not in (0, 1):
@@ -119,10 +120,12 @@ def tile_table(block: DctBlock, quad_tiles, width: int, height: int) -> np.ndarr
     m = len(tiles)
     if m and (np.any(sizes < 4) or np.any(sizes > 64) or np.any(sizes & (sizes - 1))):
         raise ValueError("DCT tiles must have a power-of-two side in 4..64")
-    if block.scales_u8:
-        if len(block.scales_u8) != m:
-            raise ValueError(f"per_tile_scales length {len(block.scales_u8)} does not match tile_sizes length {m}")
-        scale = np.array([tile_scale(u) for u in block.scales_u8], np.float64)
+    if scales is None and block.scales_u8:
+        scales = [tile_scale(u) for u in block.scales_u8]
+    if scales is not None:
+        if len(scales) != m:
+            raise ValueError(f"per_tile_scales length {len(scales)} does not match tile_sizes length {m}")
+        scale = np.asarray(scales, np.float64).reshape(m)
     else:
         scale = np.ones(m, np.float64)
     sides = _channel_sides(sizes, block.chroma_mode)           # (m, 3)
@@ -161,11 +164,11 @@ class DctLaunch:
     resident on the device; ``run`` enqueues the layer (one ``weftk_dct_apply`` launch per tile
     side, then the whole-image clip) without host synchronisation."""
 
-    def __init__(self, payload: bytes, quad_tiles, width: int, height: int, device: int = 0):
+    def __init__(self, block: DctBlock, quad_tiles, width: int, height: int, device: int = 0, scales=None):
         import torch
 
-        self.block = unpack_dct(payload)
-        self.descs = tile_table(self.block, quad_tiles, width, height)
+        self.block = block
+        self.descs = tile_table(block, quad_tiles, width, height, scales)
         self.width, self.height = int(width), int(height)
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
@@ -175,6 +178,10 @@ class DctLaunch:
         sizes = self.descs["size"]
         self.groups = [(int(v), int(np.searchsorted(sizes, v, "left")), int(np.searchsorted(sizes, v, "right")))
                        for v in np.unique(sizes)]
+
+    @classmethod
+    def from_payload(cls, payload: bytes, quad_tiles, width: int, height: int, device: int = 0) -> "DctLaunch":
+        return cls(unpack_dct(payload), quad_tiles, width, height, device)
 
     @property
     def launches(self) -> int:
@@ -207,7 +214,13 @@ def apply_dct(image, payload: bytes, quad_tiles, clip_all: bool = True):
         raise ValueError("image must be a float32 (h, w, 3) CUDA tensor")
     image = image.contiguous() if not image.is_contiguous() else image
     h, w = int(image.shape[0]), int(image.shape[1])
-    layer = DctLaunch(payload, quad_tiles, w, h, image.device.index)
+    _run_checked(DctLaunch.from_payload(payload, quad_tiles, w, h, image.device.index), image, clip_all)
+    return image
+
+
+def _run_checked(layer: DctLaunch, image, clip_all: bool = True) -> None:
+    import torch
+
     status = ctypes.c_int(0)
     layer.lib.weftk_device_status(ctypes.addressof(status))  # clear any earlier report
     layer.run(image, torch.cuda.current_stream(image.device).cuda_stream, clip_all)
@@ -215,7 +228,27 @@ def apply_dct(image, payload: bytes, quad_tiles, clip_all: bool = True):
         _lib.check(layer.lib.weftk_device_status(ctypes.addressof(status)), "weftk_device_status")
         if status.value:
             raise ValueError("a DCT tile reads past its coefficient stream or has an unsupported side")
-    return image
+
+
+def apply_residual_to_image(recon, coeffs, quad_tiles, *, quant_step: float, channels: int = 3,
+                            freq_alpha: float = 0.0, chroma_mode: int = 0, presence_bitmask: bytes | None = None,
+                            per_tile_scales=None) -> np.ndarray:
+    """Drop-in for the reference's ``apply_residual_to_image`` (src/weft/dct_residual.py:727-783), same
+    arguments: ``recon`` (h, w, 3) host image, ``coeffs`` the tile-major int16 stream (the decoder has
+    already undone a band layout), ``quad_tiles`` objects with ``x``, ``y``, ``size``.  Returns the
+    float32 image with the residual added and clipped to [0, 1], computed on the current GPU."""
+    import torch
+
+    qt = [(int(q.x), int(q.y), int(q.size)) for q in quad_tiles]
+    mask = bytes(presence_bitmask) if presence_bitmask else b""
+    block = DctBlock(np.ascontiguousarray(coeffs, np.int16).reshape(-1), float(quant_step), int(channels),
+                     float(freq_alpha), int(chroma_mode), mask, len(qt) if mask else 0, 0, b"")
+    img = torch.from_numpy(np.ascontiguousarray(recon, np.float32)).cuda()
+    if img.dim() != 3 or img.shape[2] != 3:
+        raise ValueError("recon must be (h, w, 3)")
+    h, w = int(img.shape[0]), int(img.shape[1])
+    _run_checked(DctLaunch(block, qt, w, h, img.device.index, per_tile_scales), img)
+    return img.cpu().numpy()
 
 
 def resize_into(image, out, tmp, stream: int) -> None:

@@ -265,6 +265,17 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
             "residuals": "RES0 + RES1 grids" if n_res1 else "none"}
 
 
+def pinned_copy(a: np.ndarray, keep: list) -> np.ndarray:
+    """A copy of ``a`` in page-locked host memory (its torch buffer is appended to ``keep``)."""
+    import torch
+
+    buf = torch.empty(max(a.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+    keep.append(buf)
+    out = buf.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
+    out[...] = a
+    return out
+
+
 def synthetic_dct_block(tiles, quality: int, seed: int = 0) -> bytes:
     """A BLOCK_DCT (format v5) covering every tile, in the reference encoder's default configuration
     (YCbCr 4:2:0, frequency-weight alpha 4.0, tile-major layout, the quality's quant step): seeded
@@ -894,9 +905,13 @@ def run_weft(args, world, rank, local, executor, cores):
     rd = rd_compare(args, fit, tiles, patches, pools, img, stream) if args.refine_variants else None
     plain_value, plain_ms = value, ms_step
 
-    # e2e of the plain fit through the public API from host buffers
+    # e2e of the plain fit through the public API from host buffers (pinned, as a caller that
+    # streams images would keep them)
+    pin_keep = []
+    pixels_h, records_h = pinned_copy(pixels, pin_keep), pinned_copy(records, pin_keep)
+
     def plain_e2e():
-        f2 = BatchedFit.from_arrays(pixels, sizes, records, counts, QUALITY, caps=caps, device=local)
+        f2 = BatchedFit.from_arrays(pixels_h, sizes, records_h, counts, QUALITY, caps=caps, device=local)
         f2.run()
         f2.selected_indices()
         return (int(pixels.nbytes + records.nbytes + 4 * 6 * f2.n),
@@ -936,10 +951,12 @@ def run_weft(args, world, rank, local, executor, cores):
     # reset, prepare, begin, select, end, scoring (one per size class), refine start, refine steps
     ref_launches = 7 + n_cls  # ... and one launch for all refine steps
 
+    frec_h = pinned_copy(frec, pin_keep)
+
     def refined_e2e():
         from weft_b200.refine import RefinedFit
 
-        f2 = BatchedFit.from_arrays(pixels, sizes, frec, fcnt, QUALITY, caps=caps, device=local, reserve=0)
+        f2 = BatchedFit.from_arrays(pixels_h, sizes, frec_h, fcnt, QUALITY, caps=caps, device=local, reserve=0)
         out_rows = RefinedFit(f2, steps=args.refine_steps, lr=args.refine_lr, use_graph=False).run().cpu()
         return int(pixels.nbytes + frec.nbytes + sizes.nbytes + fcnt.nbytes), int(out_rows.numel() * 4)
 

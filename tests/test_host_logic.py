@@ -48,3 +48,41 @@ def test_kinds_mask():
     assert kinds_mask_of(np.array([0, 1, 1, 0], np.int8)) == 3
     assert kinds_mask_of(np.zeros(0, np.int32)) == 0
     assert kinds_mask_of(np.array([4, 2, -1, 7], np.int32)) == (1 << 4) | (1 << 2) | (1 << 7)
+
+
+def test_slot_layout_matches_the_scatter_formula():
+    """Slots and kinds of the packed records, with and without reserved slots, against the direct
+    formula (pool_off of the tile + index in its pool)."""
+    from weft_b200._lib import PRIM_DTYPE
+    from weft_b200.fit import slot_layout
+
+    rng = np.random.default_rng(7)
+    for reserve in (0, 3, 384):
+        cnt = rng.integers(0, 9, 40).astype(np.int64)
+        recs = np.zeros(int(cnt.sum()), PRIM_DTYPE)
+        recs["kind"] = rng.integers(0, 9, len(recs))
+        cap = cnt + reserve
+        pool_off = np.concatenate([[0], np.cumsum(cap)[:-1]]).astype(np.int64)
+        n_slots = int(cap.sum())
+        kinds, slots = slot_layout(recs, cnt, pool_off, n_slots)
+        want_slots = np.concatenate([pool_off[t] + np.arange(cnt[t]) for t in range(len(cnt))]).astype(np.int64)
+        want_kinds = np.full(n_slots, 7, np.int8)
+        want_kinds[want_slots] = np.where(recs["kind"] < 7, recs["kind"], 7)
+        np.testing.assert_array_equal(kinds, want_kinds)
+        if reserve == 0:
+            assert slots is None and np.array_equal(want_slots, np.arange(len(recs)))
+        else:
+            np.testing.assert_array_equal(slots, want_slots)
+
+
+def test_init_kinds_mask_matches_kinds_mask_of():
+    from weft_b200.fit import BatchedFit
+    from weft_b200.refine import kinds_mask_of
+
+    rng = np.random.default_rng(3)
+    cases = [rng.integers(0, 8, 5000).astype(np.int8), np.full(10, 7, np.int8), np.zeros(0, np.int8),
+             np.array([0, 1, 1, 7, 7], np.int8), np.array([-3, 2, 7, 5], np.int8), np.array([4, 4, 6], np.int8)]
+    for k in cases:
+        f = BatchedFit.__new__(BatchedFit)
+        f._init_kinds = k
+        assert f.init_kinds_mask() == kinds_mask_of(f.init_kinds()), k

@@ -63,6 +63,21 @@ def unpack_cands(arr: np.ndarray) -> list:
     return out
 
 
+def slot_layout(records: np.ndarray, counts: np.ndarray, pool_off: np.ndarray, n_slots: int):
+    """Kind of every slot (int8; 7 = empty or unknown kind) and the slot of every packed record
+    (``pool_off`` of its tile + its index in the tile's pool), or ``None`` for the slots when that is
+    the record's own index (no slots reserved for re-seeding), so the records are the slot array."""
+    rec_kind = np.minimum(records["kind"], 7).astype(np.int8)
+    if len(records) == n_slots:
+        return rec_kind, None
+    n = len(counts)
+    first = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
+    slots = np.repeat(pool_off - first, counts) + np.arange(int(counts.sum()))
+    kinds = np.full(n_slots, 7, np.int8)
+    kinds[slots] = rec_kind
+    return kinds, slots
+
+
 def _dev(a: np.ndarray, device) -> torch.Tensor:
     return torch.from_numpy(np.ascontiguousarray(a)).to(device, non_blocking=False)
 
@@ -157,16 +172,17 @@ class BatchedFit:
         self.t_flags = torch.zeros(n, dtype=torch.int32, device=d)
         self.t_cur_obj = torch.zeros(n, dtype=torch.float64, device=d)
         self.t_sel = torch.full((n * self.cap_max,), -1, dtype=torch.int32, device=d)
-        # slot of every packed record: pool_off of its tile + its index in the pool
-        first = np.concatenate([[0], np.cumsum(cnt)[:-1]]).astype(np.int64) if n else np.zeros(0, np.int64)
-        slots = np.repeat(self.pool_off - first, cnt) + np.arange(int(cnt.sum()))
-        self.kinds = np.full(self.n_slots, 7, np.int8)
-        self.kinds[slots] = np.where(records["kind"] < 7, records["kind"], 7)
+        self.kinds, slots = slot_layout(records, cnt, self.pool_off, self.n_slots)
+        rec_bytes = np.ascontiguousarray(records).view(np.uint8).reshape(-1, PRIM_DTYPE.itemsize)
+        if slots is None:
+            self.t_cand = _dev(rec_bytes, d).view(-1) if len(records) else \
+                torch.zeros(0, dtype=torch.uint8, device=d)
+        else:
+            self.t_cand = torch.zeros((self.n_slots, PRIM_DTYPE.itemsize), dtype=torch.uint8, device=d)
+            if len(records):
+                self.t_cand[_dev(slots, d)] = _dev(rec_bytes, d)
+            self.t_cand = self.t_cand.view(-1)
         self._init_kinds = self.kinds.copy()
-        self.t_cand = torch.zeros((self.n_slots, PRIM_DTYPE.itemsize), dtype=torch.uint8, device=d)
-        if len(records):
-            self.t_cand[_dev(slots, d)] = _dev(np.ascontiguousarray(records).view(np.uint8).reshape(-1, PRIM_DTYPE.itemsize), d)
-        self.t_cand = self.t_cand.view(-1)
         self.t_prep = torch.empty(self.n_slots * 16, dtype=torch.float32, device=d)
         self.t_alive = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
         self.t_kind = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
@@ -211,7 +227,7 @@ class BatchedFit:
         cap = torch.from_numpy(self.pool_cap).to(d)
         cnt = torch.from_numpy(self.init_cnt.astype(np.int64)).to(d)
         off = torch.from_numpy(self.pool_off).to(d)
-        kinds = torch.from_numpy(self._init_kinds.astype(np.int64)).to(d)
+        kinds = torch.from_numpy(self._init_kinds).to(d).to(torch.int64)
         tile_of = torch.repeat_interleave(torch.arange(n, device=d), cap)
         local = torch.arange(self.n_slots, device=d) - torch.repeat_interleave(off, cap)
         filled = local < cnt[tile_of]
@@ -405,6 +421,19 @@ class BatchedFit:
     def init_kinds(self) -> np.ndarray:
         """Primitive kind of every filled slot of the initial pools (host copy)."""
         return self._init_kinds[self._init_kinds < 7].astype(np.int32)
+
+    def init_kinds_mask(self) -> int:
+        """Bit k set when kind k (0..6) occurs in the initial pools: ``kinds_mask_of(init_kinds())``
+        from one count over the slot kinds."""
+        k = self._init_kinds
+        if k.size == 0:
+            return 0
+        if int(k.min()) < 0:
+            from .refine import kinds_mask_of
+
+            return kinds_mask_of(self.init_kinds())
+        c = np.bincount(k, minlength=8)[:7]
+        return int(sum(1 << j for j in range(7) if c[j]))
 
     # ------------------------------------------------------------------ autotuner
     def configure(self, variants=None, chunks=None) -> "BatchedFit":

@@ -313,7 +313,7 @@ class RefinedFit:
         prim_off = np.concatenate([[0], np.cumsum(has.astype(np.int64))])
         n_rows = int(has.sum())
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
-        mask = kinds_mask_of(fit.init_kinds())
+        mask = fit.init_kinds_mask()
         self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask)
         self.refiner = FusedRefiner(self.ss, torch.zeros((n_rows, 16), dtype=torch.float32, device=dev), lr=lr,
                                     residual=residual)

@@ -919,6 +919,9 @@ def run_weft(args, world, rank, local, executor, cores):
 
     def timed_e2e(fn):
         ms, io = [], (0, 0)
+        if args.e2e_steps > 0:
+            for _ in range(args.warmup):  # untimed, like the device-timed steps
+                fn()
         for _ in range(args.e2e_steps):
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -927,7 +930,9 @@ def run_weft(args, world, rank, local, executor, cores):
             b.record(stream)
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
-        return (world * n_px / (statistics.mean(ms) * 1e-3) / 1e6 if ms else None), io
+        if not ms:
+            return None, io
+        return world * n_px / (max_over_ranks(statistics.mean(ms), world) * 1e-3) / 1e6, io
 
     plain_e2e_val, (p_h2d, p_d2h) = timed_e2e(plain_e2e)
 

@@ -51,10 +51,22 @@ CAP = 16
 
 
 def _pool_cands(args):
-    patch, q = args
+    patch, q = args[:2]
+    kinds = args[2] if len(args) > 2 else None
     from weft_b200.fit import pack_cands
 
-    return pack_cands(candidates.tile_candidates(patch, q))
+    return pack_cands(candidates.tile_candidates(patch, q, kinds=kinds))
+
+
+def restricted_pools(patches, pools, kinds, executor):
+    """Pools of the given kinds generated directly (host, ``executor`` processes), timed, and checked
+    against the full pools filtered to those kinds."""
+    t0 = time.perf_counter()
+    got = list(executor.map(_pool_cands, [(p, QUALITY, tuple(kinds)) for p in patches], chunksize=32))
+    gen_s = time.perf_counter() - t0
+    same = all(np.array_equal(g.view(np.uint8), f[np.isin(f["kind"], kinds)].view(np.uint8))
+               for g, f in zip(got, pools))
+    return got, gen_s, same
 
 
 def _oracle_shard(args):
@@ -940,6 +952,8 @@ def run_weft(args, world, rank, local, executor, cores):
     sampler2 = ClockSampler(local)
     sampler2.start()
     rf, fast, frec, fcnt, ref_ms = refined_headline(args, local, pixels, sizes, pools, stream, world)
+    _, cl_gen_s, cl_same = restricted_pools(patches, pools, REFINE_POOLS[args.refine_pool], executor)
+    cl_gen_s, gen_s = max_over_ranks(cl_gen_s, world), max_over_ranks(cand_s, world)
     clocks2 = sampler2.stop()
     ref_ms = max_over_ranks(ref_ms, world)
     ref_value = world * n_px / (ref_ms * 1e-3) / 1e6
@@ -1032,6 +1046,15 @@ def run_weft(args, world, rank, local, executor, cores):
         "clocks": clocks2 if iso else clocks,
         "gpu_launches": (ref_launches if iso else launches_per_step) * args.steps,
         "tiles_per_s": len(tiles) * world / (head_ms * 1e-3),
+        "fit_total": {
+            "what": "candidate generation on the host included: pools generated on all host processes, "
+                    "then the device fit (value and plain.value exclude the generation)",
+            "cores": cores,
+            "refined": {"mpix_per_s": world * n_px / (cl_gen_s + ref_ms * 1e-3) / 1e6, "cand_gen_s": cl_gen_s,
+                        "fit_ms": ref_ms, "kinds": list(REFINE_POOLS[args.refine_pool]),
+                        "pools_equal_filtered_full": bool(cl_same)},
+            "plain": {"mpix_per_s": world * n_px / (gen_s + plain_ms * 1e-3) / 1e6, "cand_gen_s": gen_s,
+                      "fit_ms": plain_ms}},
         "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
                    "plain_psnr_db": plain_rd["psnr_db"], "refined_psnr_db": ref_rd["psnr_db"],
                    "plain_bpp": plain_rd["bpp"], "refined_bpp": ref_rd["bpp"], "tolerance_db": 0.05},

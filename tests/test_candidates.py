@@ -43,3 +43,37 @@ def test_fit_golden_pools_match_reference(golden):
         for i, p in enumerate(patches):
             _same(candidates.tile_candidates(p, int(g["quality"])),
                   prims_from_pack(pool, int(pool["offsets"][i]), int(pool["offsets"][i + 1])))
+
+
+def test_kind_restricted_pools_are_the_filtered_full_pools(golden):
+    """``tile_candidates(..., kinds=...)`` generates only those kinds and equals the full pool
+    filtered to them, in order (the refined fit's constant + linear pools)."""
+    g = golden("candidates.npz")
+    for i, ts in enumerate(g["sizes"]):
+        a, b = int(g["px_offsets"][i]), int(g["px_offsets"][i + 1])
+        patch = g["patch"][a:b].reshape(ts, ts, 3)
+        for q in (40, 75, 92):
+            full = candidates.tile_candidates(patch, q)
+            for kinds in ((0, 1), (0, 1, 2), (1, 4)):
+                assert candidates.tile_candidates(patch, q, kinds=kinds) == [c for c in full if c.kind in kinds]
+
+
+def test_bench_restricted_pools_match_filtered_full_pools():
+    """The bench's directly generated constant + linear pools (worker processes) equal the full
+    pools filtered to those kinds."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    import bench
+    from weft_b200 import quadtree
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 128, 25, 9)
+    img = srgb_u8_to_linear(u8)
+    tiles = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, tiles, 64)
+    pools = [bench._pool_cands((p, 75)) for p in patches]
+    with ProcessPoolExecutor(max_workers=2, mp_context=mp.get_context("spawn")) as ex:
+        got, gen_s, same = bench.restricted_pools(patches, pools, (0, 1), ex)
+    assert same and gen_s > 0 and len(got) == len(patches)
+    assert all(set(np.unique(g["kind"])) <= {0, 1} for g in got)

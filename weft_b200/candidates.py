@@ -118,13 +118,16 @@ def _q(v: float, s: float) -> int:
 
 
 def dedup(cands: list[Cand]) -> list[Cand]:
-    """Keep the first candidate of each coarse key: geometry x4, colours x64, alpha x32."""
+    """Keep the first candidate of each coarse key: geometry x4, colours x64, alpha x32 (each
+    ``int(v * s + 0.5)`` as ``_q``, written out inline: this loop runs over every candidate)."""
     seen, out = set(), []
     for c in cands:
-        key = (c.kind, tuple(_q(g, 4) for g in c.geom), _q(c.color0[0], 64), _q(c.color0[1], 64),
-               _q(c.color0[2], 64), _q(c.alpha, 32))
+        c0 = c.color0
+        key = (c.kind, tuple([int(g * 4 + 0.5) for g in c.geom]), int(c0[0] * 64 + 0.5), int(c0[1] * 64 + 0.5),
+               int(c0[2] * 64 + 0.5), int(c.alpha * 32 + 0.5))
         if c.kind == 1:
-            key += tuple(_q(v, 64) for v in c.color1)
+            c1 = c.color1
+            key += (int(c1[0] * 64 + 0.5), int(c1[1] * 64 + 0.5), int(c1[2] * 64 + 0.5))
         if key not in seen:
             seen.add(key)
             out.append(c)
@@ -227,7 +230,14 @@ def _kmeans3_triangles(tile, pixels, wf, hf, alphas, clamp_geom):
     return out
 
 
-def edge_candidates(tile: np.ndarray, quality: int = 75) -> list[Cand]:
+def edge_candidates(tile: np.ndarray, quality: int = 75, kinds=None) -> list[Cand]:
+    """The edge-driven pool; ``kinds`` (a set) skips the generators of other kinds, which leaves the
+    remaining candidates, their values and their order unchanged."""
+    return dedup(_edge_raw(tile, quality, kinds))
+
+
+def _edge_raw(tile: np.ndarray, quality: int, kinds) -> list[Cand]:
+    want = (lambda k: True) if kinds is None else (lambda k: k in kinds)
     h, w = tile.shape[:2]
     hf, wf = float(h - 1), float(w - 1)
     mag, angle, _ = sobel(tile)
@@ -257,7 +267,7 @@ def edge_candidates(tile: np.ndarray, quality: int = 75) -> list[Cand]:
             out.append(Cand(1, (ox - nx * wf * 0.4, oy - ny * hf * 0.4, ox + nx * wf * 0.4, oy + ny * hf * 0.4),
                             c0, c1, 0.5))
 
-    pts = edge_points(mag, 60.0)
+    pts = edge_points(mag, 60.0) if (want(2) or want(3)) else []
     if pts:
         groups = cluster_points(pts, min(6, max(2, len(pts) // 4)))
         base_alpha = min(1.0, 0.25 + float(np.mean(mag)) * 3.0)
@@ -291,13 +301,19 @@ def edge_candidates(tile: np.ndarray, quality: int = 75) -> list[Cand]:
                 col = clamp_rgb(tile[int(max(0, min(h - 1, round(float(mid[1]))))),
                                      int(max(0, min(w - 1, round(float(mid[0])))))])
                 out += [Cand(3, g + (t,), col, None, base_alpha) for t in (0.5, 1.0, 2.0)]
-    if quality >= 60:
+    if quality >= 60 and want(4):
         out += _kmeans3_triangles(tile, pixels, wf, hf, (0.6, 0.3), clamp_geom=True)
-    return dedup(out)
+    return out if kinds is None else [c for c in out if c.kind in kinds]
 
 
 # ----------------------------------------------------------------------------- template pool
-def template_candidates(tile: np.ndarray, quality: int = 75) -> list[Cand]:
+def template_candidates(tile: np.ndarray, quality: int = 75, kinds=None) -> list[Cand]:
+    """The template pool; ``kinds`` as for ``edge_candidates``."""
+    return dedup(_template_raw(tile, quality, kinds))
+
+
+def _template_raw(tile: np.ndarray, quality: int, kinds) -> list[Cand]:
+    want = (lambda k: True) if kinds is None else (lambda k: k in kinds)
     h, w, _ = tile.shape
     hf, wf = float(h - 1), float(w - 1)
     lum = luminance(tile)
@@ -347,62 +363,69 @@ def template_candidates(tile: np.ndarray, quality: int = 75) -> list[Cand]:
             cx, cy = wf * ox, hf * oy
             specs.append((cx - vx * wf * 0.4, cy - vy * hf * 0.4, cx + vx * wf * 0.4, cy + vy * hf * 0.4, False))
     cols = side_means(tile, np.array([s[:4] for s in specs], dtype=np.float32))
-    for (x0, y0, x1, y1, centre), pair in zip(specs, cols):
-        c0 = tuple(float(v) for v in pair[0])
-        c1 = tuple(float(v) for v in pair[1])
+    for (x0, y0, x1, y1, centre), (c0, c1) in zip(specs, cols.tolist()):
+        c0, c1 = tuple(c0), tuple(c1)  # float32 -> Python float, exact
         for a in ((1.0, 0.7, 0.4) if centre else (0.5,)):
             out.append(Cand(1, (x0, y0, x1, y1), c0, c1, a))
 
     thicks = (0.4, 0.8, 1.2, 2.0, 3.0)
-    for t in thicks:
-        for f in (0.0, 0.25, 0.5, 0.75, 1.0):
-            out.append(Cand(2, (wf * f, 0, wf * f, hf, t), edge_col, None, base_alpha))
-            out.append(Cand(2, (0, hf * f, wf, hf * f, t), edge_col, None, base_alpha))
-        for col in (edge_col, bright, dark):
-            out.append(Cand(2, (0, 0, wf, hf, t), col, None, base_alpha))
-            out.append(Cand(2, (0, hf, wf, 0, t), col, None, base_alpha))
-    if gnorm > 1e-4:
-        lx, ly = -gmy / (gnorm + 1e-8), gmx / (gnorm + 1e-8)
-        cx, cy = wf * 0.5, hf * 0.5
-        g = (cx - lx * wf * 0.7, cy - ly * hf * 0.7, cx + lx * wf * 0.7, cy + ly * hf * 0.7)
+    if want(2):
         for t in thicks:
-            out += [Cand(2, g + (t,), col, None, base_alpha) for col in (edge_col, bright)]
+            for f in (0.0, 0.25, 0.5, 0.75, 1.0):
+                out.append(Cand(2, (wf * f, 0, wf * f, hf, t), edge_col, None, base_alpha))
+                out.append(Cand(2, (0, hf * f, wf, hf * f, t), edge_col, None, base_alpha))
+            for col in (edge_col, bright, dark):
+                out.append(Cand(2, (0, 0, wf, hf, t), col, None, base_alpha))
+                out.append(Cand(2, (0, hf, wf, 0, t), col, None, base_alpha))
+        if gnorm > 1e-4:
+            lx, ly = -gmy / (gnorm + 1e-8), gmx / (gnorm + 1e-8)
+            cx, cy = wf * 0.5, hf * 0.5
+            g = (cx - lx * wf * 0.7, cy - ly * hf * 0.7, cx + lx * wf * 0.7, cy + ly * hf * 0.7)
+            for t in thicks:
+                out += [Cand(2, g + (t,), col, None, base_alpha) for col in (edge_col, bright)]
 
     fr = (0.25, 0.5, 0.75)
-    for fy in fr:
-        for fx in fr:
-            out += [Cand(3, (0, hf * 0.5, wf * fx, hf * fy, wf, hf * 0.5, t), edge_col, None, base_alpha)
-                    for t in (0.5, 1.0, 2.0)]
-    for fx in fr:
+    if want(3):
         for fy in fr:
-            out += [Cand(3, (wf * 0.5, 0, wf * fx, hf * fy, wf * 0.5, hf, t), edge_col, None, base_alpha)
-                    for t in (0.5, 1.0)]
+            for fx in fr:
+                out += [Cand(3, (0, hf * 0.5, wf * fx, hf * fy, wf, hf * 0.5, t), edge_col, None, base_alpha)
+                        for t in (0.5, 1.0, 2.0)]
+        for fx in fr:
+            for fy in fr:
+                out += [Cand(3, (wf * 0.5, 0, wf * fx, hf * fy, wf * 0.5, hf, t), edge_col, None, base_alpha)
+                        for t in (0.5, 1.0)]
 
-    corners = [(0.0, 0.0), (wf, 0.0), (wf, hf), (0.0, hf)]
-    for i in range(4):
-        v0, v1 = corners[i], corners[(i + 1) % 4]
-        g = (v0[0], v0[1], v1[0], v1[1], wf * 0.5, hf * 0.5)
-        for col in pal[:3]:
-            out += [Cand(4, g, col, None, a) for a in (0.6, 0.3)]
-    for gv in ((0, 0, wf, 0, wf, hf), (0, 0, wf, hf, 0, hf), (0, 0, wf, 0, 0, hf), (wf, 0, wf, hf, 0, hf)):
-        out += [Cand(4, tuple(float(v) for v in gv), avg, None, a) for a in (0.5, 0.3)]
-    flat = lum.reshape(-1)
-    n_pk = min(6, len(flat))
-    for idx in (np.argpartition(flat, -n_pk)[-n_pk:], np.argpartition(flat, n_pk)[:n_pk]):
-        py, px = np.unravel_index(idx, lum.shape)
-        if n_pk >= 3:
-            for i in range(min(n_pk - 2, 4)):
-                g = (float(px[i]), float(py[i]), float(px[i + 1]), float(py[i + 1]), float(px[i + 2]),
-                     float(py[i + 2]))
-                out.append(Cand(4, g, clamp_rgb(tile[py[i:i + 3], px[i:i + 3]].mean(axis=0)), None, 0.5))
-    if quality >= 80:
-        out += _kmeans3_triangles(tile, pixels, wf, hf, (0.5, 0.3), clamp_geom=False)
-    return dedup(out)
+    if want(4):
+        corners = [(0.0, 0.0), (wf, 0.0), (wf, hf), (0.0, hf)]
+        for i in range(4):
+            v0, v1 = corners[i], corners[(i + 1) % 4]
+            g = (v0[0], v0[1], v1[0], v1[1], wf * 0.5, hf * 0.5)
+            for col in pal[:3]:
+                out += [Cand(4, g, col, None, a) for a in (0.6, 0.3)]
+        for gv in ((0, 0, wf, 0, wf, hf), (0, 0, wf, hf, 0, hf), (0, 0, wf, 0, 0, hf), (wf, 0, wf, hf, 0, hf)):
+            out += [Cand(4, tuple(float(v) for v in gv), avg, None, a) for a in (0.5, 0.3)]
+        flat = lum.reshape(-1)
+        n_pk = min(6, len(flat))
+        for idx in (np.argpartition(flat, -n_pk)[-n_pk:], np.argpartition(flat, n_pk)[:n_pk]):
+            py, px = np.unravel_index(idx, lum.shape)
+            if n_pk >= 3:
+                for i in range(min(n_pk - 2, 4)):
+                    g = (float(px[i]), float(py[i]), float(px[i + 1]), float(py[i + 1]), float(px[i + 2]),
+                         float(py[i + 2]))
+                    out.append(Cand(4, g, clamp_rgb(tile[py[i:i + 3], px[i:i + 3]].mean(axis=0)), None, 0.5))
+        if quality >= 80:
+            out += _kmeans3_triangles(tile, pixels, wf, hf, (0.5, 0.3), clamp_geom=False)
+    return out if kinds is None else [c for c in out if c.kind in kinds]
 
 
-def tile_candidates(tile: np.ndarray, quality: int = 75) -> list[Cand]:
-    """The tile's initial pool: edge-driven then template candidates, de-duplicated."""
-    return dedup(edge_candidates(tile, quality) + template_candidates(tile, quality))
+def tile_candidates(tile: np.ndarray, quality: int = 75, kinds=None) -> list[Cand]:
+    """The tile's initial pool: edge-driven then template candidates, de-duplicated.  With ``kinds``
+    only those kinds are generated: the result is the full pool filtered to them, in pool order
+    (the de-duplication key starts with the kind, so other kinds never shadow a candidate)."""
+    kinds = None if kinds is None else frozenset(int(k) for k in kinds)
+    # one de-duplication of the concatenation keeps the same first occurrences as de-duplicating
+    # each pool first
+    return dedup(_edge_raw(tile, quality, kinds) + _template_raw(tile, quality, kinds))
 
 
 # ----------------------------------------------------------------------------- re-seeding

@@ -36,7 +36,8 @@ What is captured (reference function -> fixture):
   * ``dct_residual.encode_tile_residuals`` / ``permute_tile_to_band`` /
     ``bitstream.pack_dct`` payloads (block versions 2-5, every chroma mode and
     layout, presence masks, per-tile scales) applied by the reference decoder's
-    steps ``unpack_dct`` -> ``permute_band_to_tile`` -> ``apply_residual_to_image``
+    steps ``unpack_dct`` -> ``permute_band_to_tile`` -> ``apply_residual_to_image``, plus
+    extremes (u8 scales 0 and 255, coefficients in the thousands, most pixels clipped)
     (src/weft/decoder.py:477-507), and Pillow ``Image.resize(BILINEAR)`` of u8
     images (src/weft/decoder.py:514-518)                    -> dct.npz
   * ``encoder.encode_image`` with the DCT residual layer, decoded by
@@ -580,17 +581,18 @@ def gen_dct(ref) -> None:
     rng = np.random.default_rng(20260416)
     H, W = 72, 100   # tiles cover 128 x 128: some cross the image edge, two lie outside it
     recon = rng.uniform(-0.05, 1.05, (H, W, 3)).astype(np.float32)
-    # (chroma mode, freq alpha, per-tile scales, layout, block version, presence probability)
-    cases = [(0, 0.0, False, 0, 5, 0.8), (1, 4.0, False, 1, 5, 0.8), (2, 4.0, True, 1, 5, 0.8),
-             (2, 0.0, True, 0, 5, 1.0), (2, 4.0, False, 1, 4, 0.7), (1, 0.0, False, 0, 3, 0.7),
-             (2, 4.0, False, 0, 2, 1.0), (0, 4.0, False, 1, 5, 0.0)]
     out = {"recon": recon, "tiles": np.array(DCT_TILES, np.int32)}
-    for i, (chroma, alpha, scales, layout, version, p_present) in enumerate(cases):
+
+    def case(i, chroma, alpha, scales, layout, version, p_present, std=0.06):
+        """One block: ``scales`` None (uniform), "rng" (u8 scales drawn from 40..219) or u8 bytes."""
         present = [bool(rng.random() < p_present) for _ in DCT_TILES]
-        res = [rng.normal(0.0, 0.06, (s, s, 3)).astype(np.float32) for (_, _, s), p in zip(DCT_TILES, present) if p]
+        res = [rng.normal(0.0, std, (s, s, 3)).astype(np.float32) for (_, _, s), p in zip(DCT_TILES, present) if p]
         sizes = [s for (_, _, s), p in zip(DCT_TILES, present) if p]
-        su8 = bytes(int(v) for v in rng.integers(40, 220, len(res))) if scales else b""
-        sc = [R.decode_tile_scale_u8(b) for b in su8] if scales else None
+        if scales == "rng":
+            su8 = bytes(int(v) for v in rng.integers(40, 220, len(res)))
+        else:
+            su8 = bytes(scales[:len(res)]) if scales else b""
+        sc = [R.decode_tile_scale_u8(b) for b in su8] if su8 else None
         coeffs, _ = R.encode_tile_residuals(res, quant_step=0.0135, freq_alpha=alpha, chroma_mode=chroma,
                                             per_tile_scales=sc)
         payload = R.permute_tile_to_band(coeffs, sizes, chroma) if layout else coeffs
@@ -616,11 +618,23 @@ def gen_dct(ref) -> None:
                                          per_tile_scales=pts)
         out[f"blob_{i}"] = np.frombuffer(blob, np.uint8)
         out[f"out_{i}"] = want.astype(np.float32)
+
+    # (chroma mode, freq alpha, per-tile scales, layout, block version, presence probability)
+    cases = [(0, 0.0, None, 0, 5, 0.8), (1, 4.0, None, 1, 5, 0.8), (2, 4.0, "rng", 1, 5, 0.8),
+             (2, 0.0, "rng", 0, 5, 1.0), (2, 4.0, None, 1, 4, 0.7), (1, 0.0, None, 0, 3, 0.7),
+             (2, 4.0, None, 0, 2, 1.0), (0, 4.0, None, 1, 5, 0.0)]
+    for i, cfg in enumerate(cases):
+        case(i, *cfg)
     for j, ((h, w), (ow, oh)) in enumerate((((48, 64), (240, 135)), ((64, 96), (96, 200)), ((80, 100), (37, 29)),
                                             ((17, 33), (200, 100)), ((50, 70), (70, 50)), ((31, 29), (300, 7)))):
         u8 = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
         out[f"rs_in_{j}"] = u8
         out[f"rs_out_{j}"] = np.asarray(Image.fromarray(u8).resize((ow, oh), Image.BILINEAR))
+    # extremes: the ends of the u8 scale range, and residuals large enough for coefficients in the
+    # thousands with most pixels clipped
+    case(8, 2, 4.0, bytes([0, 255] * 8), 1, 5, 1.0)
+    case(9, 0, 0.0, None, 0, 5, 0.9, std=0.6)
+    case(10, 1, 4.0, bytes([255, 0, 128] * 6), 0, 5, 0.9, std=0.3)
     _save("dct.npz", **out)
 
 

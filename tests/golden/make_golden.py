@@ -37,7 +37,8 @@ What is captured (reference function -> fixture):
     ``bitstream.pack_dct`` payloads (block versions 2-5, every chroma mode and
     layout, presence masks, per-tile scales) applied by the reference decoder's
     steps ``unpack_dct`` -> ``permute_band_to_tile`` -> ``apply_residual_to_image``, plus
-    extremes (u8 scales 0 and 255; noise residuals up to std 0.6, ~40 % of pixels clipped)
+    extremes (u8 scales 0 and 255; noise residuals up to std 0.6, ~40 % of pixels clipped;
+    smooth residuals whose low-frequency coefficients reach ~800)
     (src/weft/decoder.py:477-507), and Pillow ``Image.resize(BILINEAR)`` of u8
     images (src/weft/decoder.py:514-518)                    -> dct.npz
   * ``encoder.encode_image`` with the DCT residual layer, decoded by
@@ -583,10 +584,16 @@ def gen_dct(ref) -> None:
     recon = rng.uniform(-0.05, 1.05, (H, W, 3)).astype(np.float32)
     out = {"recon": recon, "tiles": np.array(DCT_TILES, np.int32)}
 
-    def case(i, chroma, alpha, scales, layout, version, p_present, std=0.06):
-        """One block: ``scales`` None (uniform), "rng" (u8 scales drawn from 40..219) or u8 bytes."""
+    def case(i, chroma, alpha, scales, layout, version, p_present, std=0.06, smooth=False):
+        """One block: ``scales`` None (uniform), "rng" (u8 scales drawn from 40..219) or u8 bytes;
+        ``smooth`` adds a per-tile offset and ramp (large low-frequency coefficients)."""
         present = [bool(rng.random() < p_present) for _ in DCT_TILES]
         res = [rng.normal(0.0, std, (s, s, 3)).astype(np.float32) for (_, _, s), p in zip(DCT_TILES, present) if p]
+        if smooth:
+            for r in res:
+                s = r.shape[0]
+                ramp = np.linspace(-0.3, 0.3, s, dtype=np.float32)
+                r += (ramp[:, None, None] + np.array([0.45, -0.35, 0.2], np.float32)).astype(np.float32)
         sizes = [s for (_, _, s), p in zip(DCT_TILES, present) if p]
         if scales == "rng":
             su8 = bytes(int(v) for v in rng.integers(40, 220, len(res)))
@@ -634,6 +641,7 @@ def gen_dct(ref) -> None:
     case(8, 2, 4.0, bytes([0, 255] * 8), 1, 5, 1.0)
     case(9, 0, 0.0, None, 0, 5, 0.9, std=0.6)
     case(10, 1, 4.0, bytes([255, 0, 128] * 6), 0, 5, 0.9, std=0.3)
+    case(11, 2, 4.0, None, 1, 5, 1.0, std=0.02, smooth=True)
     _save("dct.npz", **out)
 
 

@@ -12,7 +12,7 @@ import pytest
 from oracle import dct as odct
 from weft_b200 import _lib, raster
 
-N_CASES = 11
+N_CASES = 12
 N_RESIZE = 6
 RESIZE_TARGETS = [(240, 135), (96, 200), (37, 29), (200, 100), (70, 50), (300, 7)]
 

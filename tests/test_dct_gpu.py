@@ -15,7 +15,7 @@ RESIZE_TARGETS = [(240, 135), (96, 200), (37, 29), (200, 100), (70, 50), (300, 7
 APPLY_TOL = 2.5e-7
 
 
-@pytest.mark.parametrize("i", range(11))
+@pytest.mark.parametrize("i", range(12))
 def test_dct_apply_matches_reference(golden, i):
     import torch
 
@@ -62,7 +62,7 @@ def test_decode_file_raster_branch_matches_reference_decoder(golden, which):
         assert float(np.max(np.abs(got - want))) <= 1.0 / 255.0 + 1e-6, key
 
 
-@pytest.mark.parametrize("i", range(11))
+@pytest.mark.parametrize("i", range(12))
 def test_drop_in_apply_residual_to_image(golden, i):
     """The reference decoder's own steps (unpack, undo the band layout, decode the u8 scales) feeding
     the drop-in ``apply_residual_to_image``."""

@@ -952,9 +952,10 @@ def run_weft(args, world, rank, local, executor, cores):
     sampler2 = ClockSampler(local)
     sampler2.start()
     rf, fast, frec, fcnt, ref_ms = refined_headline(args, local, pixels, sizes, pools, stream, world)
+    clocks2 = sampler2.stop()
+    # host generation of the refined fit's pools alone (outside the clock window: no GPU work)
     _, cl_gen_s, cl_same = restricted_pools(patches, pools, REFINE_POOLS[args.refine_pool], executor)
     cl_gen_s, gen_s = max_over_ranks(cl_gen_s, world), max_over_ranks(cand_s, world)
-    clocks2 = sampler2.stop()
     ref_ms = max_over_ranks(ref_ms, world)
     ref_value = world * n_px / (ref_ms * 1e-3) / 1e6
     plain_rd = rd["plain"] if rd else rd_of_params(*fit.stack_set(), tiles, patches, img, args.size)

@@ -70,15 +70,16 @@ def restricted_pools(patches, pools, kinds, executor):
 
 
 def _oracle_shard(args):
-    """CPU baseline worker: the oracle greedy over a shard of tiles."""
-    patches, pools, q = args
+    """CPU baseline worker: the oracle greedy over a shard of tiles (with ``schedule``, the round
+    decisions of the whole fit those tiles belong to); returns (seconds, selections, objectives)."""
+    patches, pools, q, schedule = args
     from oracle import fit as ofit
 
     t0 = time.perf_counter()
-    ofit.greedy_fit(patches, [p.shape[0] for p in patches], pools, q,
-                    reseed=lambda i, patch, pred: candidates.residual_candidates(patch, pred, q),
-                    caps=[CAP] * len(patches))
-    return time.perf_counter() - t0
+    sel, cur, _ = ofit.greedy_fit(patches, [p.shape[0] for p in patches], pools, q,
+                                  reseed=lambda i, patch, pred: candidates.residual_candidates(patch, pred, q),
+                                  caps=[CAP] * len(patches), schedule=schedule)
+    return time.perf_counter() - t0, sel, [float(v) for v in cur]
 
 
 def build_workload(size: int, n_prims: int, seed: int, executor):
@@ -119,16 +120,43 @@ def cpu_sample(patches, pools, budget_s: float, executor, seed: int = 0):
     return sorted(pick)
 
 
-def run_cpu(patches, pools, pick, executor, cores: int):
+def run_cpu(patches, pools, pick, executor, cores: int, schedule=None, results: dict | None = None):
+    """The oracle greedy over the tiles ``pick`` on ``cores`` processes; returns (MPix/s, wall
+    seconds, pixels).  ``results`` (a dict) receives tile -> (selection, objective)."""
     from weft_b200.fit import unpack_cands
 
-    shards = [pick[k::cores] for k in range(cores)]
-    args = [([patches[i] for i in s], [unpack_cands(pools[i]) for i in s], QUALITY) for s in shards if s]
+    shards = [s for s in (pick[k::cores] for k in range(cores)) if s]
+    args = [([patches[i] for i in s], [unpack_cands(pools[i]) for i in s], QUALITY, schedule) for s in shards]
     t0 = time.perf_counter()
-    list(executor.map(_oracle_shard, args))
+    out = list(executor.map(_oracle_shard, args))
     wall = time.perf_counter() - t0
+    if results is not None:
+        for s, (_, sel, cur) in zip(shards, out):
+            results.update({t: (a, b) for t, a, b in zip(s, sel, cur)})
     px = sum(patches[i].shape[0] ** 2 for i in pick)
     return px / wall / 1e6, wall, px
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (first processor of /proc/cpuinfo; empty when unknown)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return ""
+
+
+def fit_parity(fit, results: dict) -> dict:
+    """The device fit's selections and objectives against the oracle's on the sampled tiles."""
+    sel = fit.selected_indices()
+    obj = fit.objectives()
+    equal = sum(1 for t, (s, _) in results.items() if sel[t] == s)
+    rel = max((abs(float(obj[t]) - c) / max(abs(c), 1e-30) for t, (_, c) in results.items()), default=0.0)
+    return {"tiles": len(results), "equal_selections": equal, "max_obj_rel": rel,
+            "what": "device plain fit vs the oracle greedy (the reference's algorithm, host re-seeding) on the "
+                    "CPU baseline's sampled tiles, replaying the device fit's round decisions"}
 
 
 class ClockSampler:
@@ -726,6 +754,12 @@ def workload_name(args) -> str:
             f"q=75, cap {CAP}, the reference's candidate pools")
 
 
+def bench_config(args, n_tiles: int, n_candidates: int) -> dict:
+    """The ``config`` object, identical in both arms' lines (what each arm fits is under ``fit``)."""
+    return {"workload": workload_name(args), "tiles": n_tiles, "candidates": n_candidates, "global_batch": args.gpus,
+            "seq_len": 0, "parallelism": f"replicas x{args.gpus}"}
+
+
 def max_over_ranks(x: float, world: int) -> float:
     """The slowest rank's time (every rank calls this at the same point)."""
     if world <= 1:
@@ -773,11 +807,11 @@ def reference_arm(args, world, rank, executor):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "MPix/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(args),
-                   "fit": "the reference's plain greedy (init, rounds, residual re-seeds); its RD is the iso-RD target",
-                   "tiles": len(tiles), "candidates": int(sum(len(p) for p in pools)), "global_batch": 1,
-                   "seq_len": 0, "parallelism": "cpu-processes"},
-        "cpu_baseline": {"value": value, "unit": "MPix/s", "cores": cores, "kind": "port", "sample": sample},
+        "config": bench_config(args, len(tiles), int(sum(len(p) for p in pools))),
+        "fit": "the reference's plain greedy (init, rounds, residual re-seeds), the oracle's restatement on "
+               "all host cores; its RD is the iso-RD target",
+        "cpu_baseline": {"value": value, "unit": "MPix/s", "cores": cores, "kind": "port", "sample": sample,
+                         "cpu": cpu_model()},
         "e2e": {"value": value, "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -870,8 +904,9 @@ def run_weft(args, world, rank, local, executor, cores):
     ctl = fit.control()
     max_rounds = rate.max_rounds(QUALITY)
     # kernels per step: reset, prepare; init round: begin, scoring per class, select, end; every
-    # greedy round (run or skipped): begin, scoring per class, select, end, control, re-seed
-    launches_per_step = 2 + (3 + n_classes) + max_rounds * (5 + n_classes)
+    # greedy round (run or skipped): begin, scoring per class, select, end, control, re-seed; the
+    # selected stacks snapped to the wire grid
+    launches_per_step = 2 + (3 + n_classes) + max_rounds * (5 + n_classes) + 1
     import ctypes
 
     ms_total = ev0.elapsed_time(ev1)
@@ -889,6 +924,9 @@ def run_weft(args, world, rank, local, executor, cores):
     lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
     work = [fit.work_counters()]
     rounds = [len(fit.stats.per_round)]
+    # the device fit's round decisions (a greedy round ran with evaluated tiles: did any improve?),
+    # replayed by the oracle on the CPU baseline's sampled tiles for the parity check
+    schedule = [imp > 0 for mode, ev, imp in fit.stats.per_round if mode == 1 and ev > 0]
     score_ms.value *= args.steps  # per-step figures below divide by the step count
 
     # roofline of the scoring kernels (FP32-bound): algorithmic ops / scoring device time
@@ -925,9 +963,10 @@ def run_weft(args, world, rank, local, executor, cores):
     def plain_e2e():
         f2 = BatchedFit.from_arrays(pixels_h, sizes, records_h, counts, QUALITY, caps=caps, device=local)
         f2.run()
-        f2.selected_indices()
+        f2.quantize_selected()
+        q_rows, q_kind = f2.t_qrows.cpu(), f2.t_qkind.cpu()
         return (int(pixels.nbytes + records.nbytes + 4 * 6 * f2.n),
-                int(f2.t_sel.numel() * 4 + f2.t_n_sel.numel() * 4 + 16 * len(f2.stats.per_round)))
+                int(q_rows.numel() * 4 + q_kind.numel() * 4 + 16 * len(f2.stats.per_round)))
 
     def timed_e2e(fn):
         ms, io = [], (0, 0)
@@ -968,8 +1007,9 @@ def run_weft(args, world, rank, local, executor, cores):
     init_tflops = r_work[1] / (r_score_ms * 1e-3) / 1e12 if r_score_ms > 0 else 0.0
     refine_share = args.refine_steps * r_step_ms
     n_cls = sum(1 for k in (8, 16, 32) if fast.n_items[k])
-    # reset, prepare, begin, select, end, scoring (one per size class), refine start, refine steps
-    ref_launches = 7 + n_cls  # ... and one launch for all refine steps
+    # moments, reset, prepare, begin, select, end, scoring (one per size class), refine start, one
+    # launch for all refine steps, wire-grid snap
+    ref_launches = 9 + n_cls
 
     frec_h = pinned_copy(frec, pin_keep)
 
@@ -977,24 +1017,30 @@ def run_weft(args, world, rank, local, executor, cores):
         from weft_b200.refine import RefinedFit
 
         f2 = BatchedFit.from_arrays(pixels_h, sizes, frec_h, fcnt, QUALITY, caps=caps, device=local, reserve=0)
-        out_rows = RefinedFit(f2, steps=args.refine_steps, lr=args.refine_lr, use_graph=False).run().cpu()
+        r2 = RefinedFit(f2, steps=args.refine_steps, lr=args.refine_lr, use_graph=False)
+        r2.run()
+        out_rows = r2.q_rows.cpu()
         return int(pixels.nbytes + frec.nbytes + sizes.nbytes + fcnt.nbytes), int(out_rows.numel() * 4)
 
     ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
+    # what the Adam steps add: RD of the same init round's picks without them
+    init_rd = rd_of_params(rf.ss, rf.start, tiles, patches, img, args.size)
 
     diff = differentiable_fit(args, executor, local, stream) if args.diff_steps > 0 and rank == 0 else None
     ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None
 
-    cpu = None
+    cpu = parity = None
     dec_cpu = ras_cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         if args.decode_iters > 0:
             dec_cpu, ras_cpu = cpu_decode_baselines(fit, tiles, patches, args.size, 3840, 2160)
         pick = cpu_sample(patches, pools, args.cpu_budget_s, executor)
-        v, wall, px = run_cpu(patches, pools, pick, executor, cores)
-        cpu = {"value": v, "unit": "MPix/s", "cores": cores, "kind": "port",
+        results: dict = {}
+        v, wall, px = run_cpu(patches, pools, pick, executor, cores, schedule, results)
+        cpu = {"value": v, "unit": "MPix/s", "cores": cores, "kind": "port", "cpu": cpu_model(),
                "sample": f"oracle greedy (plain fit) over {len(pick)} of {len(tiles)} tiles ({px / 1e6:.3f} MPix), "
                          f"{wall:.1f} s wall on {cores} processes"}
+        parity = fit_parity(fit, results)
     if rank != 0:
         return
     # the raster branch is timed last, so that a failure in it leaves every number above intact
@@ -1026,57 +1072,62 @@ def run_weft(args, world, rank, local, executor, cores):
                  "launches": r_n_score}
     dominant, other = (refine_roof, init_roof) if refine_share >= r_score_ms else (init_roof, refine_roof)
     head_value, head_ms = (ref_value, ref_ms) if iso else (plain_value, plain_ms)
-    line = {
-        "metric": METRIC, "value": head_value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(args),
-                   "fit": (f"gradient-refined batched fit ({args.refine_pool} init round + {args.refine_steps} "
-                           f"fused Adam steps, lr {args.refine_lr}) at iso RD with the plain greedy fit"
-                           if iso else "plain greedy fit (the refined fit missed iso RD)"),
-                   "tiles": len(tiles), "candidates": int(sum(len(p) for p in pools)),
-                   "refined_candidates": int(len(frec)), "global_batch": world, "seq_len": 0,
-                   "parallelism": f"replicas x{world}",
-                   "l2": "refined fit: 256 MiB written before each timed step (working set fits in L2); "
-                         "plain fit: per-step working set (pixels + pools) exceeds L2, no flush"},
-        "e2e": {"value": ref_e2e_val if iso else plain_e2e_val, "unit": "MPix/s",
-                "h2d_bytes_per_step": r_h2d if iso else p_h2d, "d2h_bytes_per_step": r_d2h if iso else p_d2h},
-        "roofline": dominant if iso else score_roof,
-        "roofline_other": other if iso else None,
-        "cpu_baseline": cpu,
-        "clocks": clocks2 if iso else clocks,
-        "gpu_launches": (ref_launches if iso else launches_per_step) * args.steps,
-        "tiles_per_s": len(tiles) * world / (head_ms * 1e-3),
-        "fit_total": {
-            "what": "candidate generation on the host included: pools generated on all host processes, "
-                    "then the device fit (value and plain.value exclude the generation)",
-            "cores": cores,
-            "refined": {"mpix_per_s": world * n_px / (cl_gen_s + ref_ms * 1e-3) / 1e6, "cand_gen_s": cl_gen_s,
-                        "fit_ms": ref_ms, "kinds": list(REFINE_POOLS[args.refine_pool]),
-                        "pools_equal_filtered_full": bool(cl_same)},
-            "plain": {"mpix_per_s": world * n_px / (gen_s + plain_ms * 1e-3) / 1e6, "cand_gen_s": gen_s,
-                      "fit_ms": plain_ms}},
-        "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
-                   "plain_psnr_db": plain_rd["psnr_db"], "refined_psnr_db": ref_rd["psnr_db"],
-                   "plain_bpp": plain_rd["bpp"], "refined_bpp": ref_rd["bpp"], "tolerance_db": 0.05},
+    grad_db = ref_rd["rd_score"] - init_rd["rd_score"]
+    fit_desc = (f"gradient-refined batched fit: init round over the {args.refine_pool} candidates "
+                f"({len(frec)} of {int(sum(len(p) for p in pools))}), then {args.refine_steps} fused Adam steps "
+                f"(lr {args.refine_lr}) and the wire-grid snap, one CUDA graph; the Adam steps change RD by "
+                f"{grad_db:+.4f} dB over the init round alone" if iso else
+                "plain greedy fit (the refined fit missed iso RD)")
+    details = {
         "plain": {"value": plain_value, "ms_per_step": plain_ms, "tiles_per_s": len(tiles) * world / (plain_ms * 1e-3),
-                  "e2e": plain_e2e_val, "roofline": score_roof,
+                  "e2e": plain_e2e_val, "e2e_bytes": [p_h2d, p_d2h], "roofline": score_roof,
                   "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
                   "rounds_per_step": rounds[-1], "reseeds": fit.stats.reseeds, "graph_control": ctl,
-                  "fit": "whole greedy (init, rounds, device re-seeds) replayed from one CUDA graph",
-                  "reseed_host_s": fit.stats.t_reseed_s, "cand_gen_s": cand_s,
-                  "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
+                  "fit": "whole greedy (init, rounds, device re-seeds, wire-grid snap) replayed from one CUDA graph",
+                  "cand_gen_s": cand_s, "prims_per_tile": prims_total / len(tiles), "psnr_prims_db": psnr_prims,
                   "prim_payload_bytes": prim_bytes,
                   "autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
                                for k, v in tuned_plain.items()}},
         "refined_autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
                              for k, v in (fast.tuning or {}).items()},
-        "decode": decode,
-        "decode_with_residuals": decode_res,
-        "decode_raster": raster_line,
-        "differentiable_fit": diff,
-        "image_batch": ibatch,
-        "rd": rd,
+        "roofline_refine": refine_roof, "roofline_init": init_roof,
+        "iso_rd": {"plain": plain_rd, "refined": ref_rd, "init_round_only": init_rd},
+        "decode": decode, "decode_with_residuals": decode_res, "decode_raster": raster_line,
+        "differentiable_fit": diff, "image_batch": ibatch, "rd": rd, "parity": parity,
+    }
+    print(json.dumps({"bench_details": details}), file=sys.stderr, flush=True)
+
+    def frac(d, key="frac"):
+        return None if not d or key not in d else round(d[key], 4)
+
+    line = {
+        "metric": METRIC, "value": head_value, "unit": "MPix/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": bench_config(args, len(tiles), int(sum(len(p) for p in pools))),
+        "fit": fit_desc,
+        "l2": "refined fit: 256 MiB written before each timed step (working set fits in L2); plain fit: per-step "
+              "working set (pixels + pools) exceeds L2, no flush",
+        "e2e": {"value": ref_e2e_val if iso else plain_e2e_val, "unit": "MPix/s",
+                "h2d_bytes_per_step": r_h2d if iso else p_h2d, "d2h_bytes_per_step": r_d2h if iso else p_d2h},
+        "roofline": dominant if iso else score_roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks2 if iso else clocks,
+        "gpu_launches": (ref_launches if iso else launches_per_step) * args.steps,
+        "tiles_per_s": len(tiles) * world / (head_ms * 1e-3),
+        "plain": {"value": plain_value, "ms_per_step": plain_ms, "e2e": plain_e2e_val,
+                  "roofline_frac": frac(score_roof), "reseeds": fit.stats.reseeds},
+        "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
+                   "init_only_rd": init_rd["rd_score"], "adam_steps_db": grad_db, "tolerance_db": 0.05},
+        "fit_total": {"refined_mpix_per_s": world * n_px / (cl_gen_s + ref_ms * 1e-3) / 1e6,
+                      "refined_cand_gen_s": cl_gen_s, "plain_mpix_per_s": world * n_px / (gen_s + plain_ms * 1e-3) / 1e6,
+                      "plain_cand_gen_s": gen_s, "cand_gen": f"host, {cores} processes",
+                      "pools_equal_filtered_full": bool(cl_same)},
+        "decode": {"frac": frac(decode), "frac_with_residuals": frac(decode_res),
+                   "raster_resize_frac": frac((raster_line or {}).get("resize")),
+                   "ms": None if not decode else round(decode["ms"], 4)},
+        "parity": None if parity is None else {k: parity[k] for k in ("tiles", "equal_selections", "max_obj_rel")},
+        "details": "the full record is the bench_details JSON line on stderr",
     }
     print(json.dumps(line), flush=True)
 

@@ -48,8 +48,14 @@ def stack_mse(patch: np.ndarray, prims) -> np.float32:
     return np.float32(np.mean((patch - render.render_tile(prims, patch.shape[0])) ** 2))
 
 
-def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None, max_rounds=None):
+def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None, max_rounds=None, schedule=None):
     """Run the greedy; ``reseed(tile_index, patch, pred) -> list[Prim]``.
+
+    The round loop's decisions are global over the tiles it is given: a round in which no tile
+    improved is a stall (re-seed, or stop after the fourth in a row), otherwise the complex set
+    becomes the tiles that improved.  ``schedule`` replays them from a larger fit these tiles
+    belong to: one bool per greedy round that fit ran, True when any of its tiles improved; the
+    tiles given here then take exactly the decisions they took there.
 
     Returns (selected index lists, current objectives (float64), stats dict).
     """
@@ -62,7 +68,7 @@ def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None, max_
     alive = [list(range(len(p))) for p in ext]
     selected: list[list[int]] = [[] for _ in range(n)]
     cur = np.zeros(n, np.float64)
-    stats = {"rounds": 0, "reseeds": 0, "evals": 0}
+    stats = {"rounds": 0, "reseeds": 0, "evals": 0, "schedule": []}
 
     for i in range(n):
         kinds = np.array([p.kind for p in ext[i]], np.int32)
@@ -79,9 +85,10 @@ def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None, max_
     if max_rounds is None:
         max_rounds = 20 if quality >= 90 else 8 if quality >= 70 else 4
     stalls = 0
-    for _ in range(max_rounds):
+    rounds = range(max_rounds) if schedule is None else range(len(schedule))
+    for r in rounds:
         active = [i for i in complex_tiles if alive[i] and len(selected[i]) < caps[i]]
-        if not active:
+        if not active and schedule is None:
             break
         stats["rounds"] += 1
         improved = []
@@ -98,7 +105,9 @@ def greedy_fit(patches, sizes, pools, quality: int, reseed=None, caps=None, max_
                 selected[i].append(j)
                 cur[i] = float(objs[b])
                 improved.append(i)
-        if not improved:
+        stalled = not improved if schedule is None else not schedule[r]
+        stats["schedule"].append(not stalled)
+        if stalled:
             stalls += 1
             if stalls > 3:
                 break

@@ -2,9 +2,10 @@
 
 Run once, in a container where the reference source tree is available:
 
-    python tests/golden/make_golden.py [/path/to/reference/src]
+    python tests/golden/make_golden.py /path/to/reference/src [fixture ...]
 
-(default path: /root/reference/src).  The fixtures are small ``.npz`` files
+or with the path in the environment variable ``WEFT_REFERENCE_SRC`` (the path
+is required; there is no default).  The fixtures are small ``.npz`` files
 committed next to this script; the tests read only those files, never the
 reference.
 
@@ -33,6 +34,10 @@ What is captured (reference function -> fixture):
     ``render_tile`` at pixel centres (the reference GPU launcher
     ``gpu_render.gpu_batch_score_prepacked`` needs a GPU)
                                -> fit_small.npz (q=75), fit_hq.npz (q=92)
+  * the same greedy inside ``encoder.encode_image`` on the 256x256 plain-method
+    workload (40 primitives, seed 0, q=75, fixed 32-px tiles, at most 8
+    primitives per tile, primitive-stack basis only), with the written file
+    and ``decoder.decode_to_array`` at native size          -> fit_cfg256.npz
   * ``dct_residual.encode_tile_residuals`` / ``permute_tile_to_band`` /
     ``bitstream.pack_dct`` payloads (block versions 2-5, every chroma mode and
     layout, presence masks, per-tile scales) applied by the reference decoder's
@@ -434,84 +439,138 @@ def _cpu_score_prepacked(ref):
     return score, stats
 
 
+class _FitCapture:
+    """Runs the reference's adaptive fit with the CPU scorer installed and records, per tile, the
+    initial candidate pool, every re-seed batch and the fit state's selections.
+
+    ``tile_size`` forces the quadtree to fixed tiles of that side and ``cap`` the per-tile primitive
+    cap (the reference reads both from module globals: ``quadtree.decompose_quadtree`` is imported
+    inside the fit, ``QuadTile.max_primitives`` reads ``MAX_PRIMITIVES_BY_TILE_SIZE``)."""
+
+    def __init__(self, ref, tile_size: int | None = None, cap: int | None = None):
+        self.ref, self.tile_size, self.cap = ref, tile_size, cap
+        self.pools: dict[int, list] = {}
+        self.reseeds: list[tuple[int, list]] = []
+        self.patches = None
+        self.state = None
+
+    def __enter__(self):
+        enc, gr, qt_mod = self.ref["encoder"], self.ref["gpu_render"], self.ref["quadtree"]
+        score, self.stats = _cpu_score_prepacked(self.ref)
+        orig_worker, orig_resid = enc._worker_gen_cands, enc._generate_residual_candidates
+        orig_extract, orig_decomp, orig_fit = qt_mod.extract_adaptive_tiles, qt_mod.decompose_quadtree, \
+            enc._fit_adaptive_state
+
+        def extract(image, tiles):
+            self.patches = orig_extract(image, tiles)
+            return self.patches
+
+        def decomp(image, **kw):
+            if self.tile_size is not None:
+                kw["min_tile"] = kw["max_tile"] = self.tile_size
+            return orig_decomp(image, **kw)
+
+        def worker(args):
+            cands, packed = orig_worker(args)
+            idx = next(i for i, p in enumerate(self.patches) if p is args[0])
+            self.pools[idx] = list(cands)
+            return cands, packed
+
+        def resid(tile, pred, quality):
+            out = orig_resid(tile, pred, quality)
+            idx = next(i for i, p in enumerate(self.patches) if p is tile)
+            self.reseeds.append((idx, list(out)))
+            return out
+
+        def fit(*a, **kw):
+            self.state = orig_fit(*a, **kw)
+            return self.state
+
+        self.saved = (gr.gpu_batch_score_prepacked, enc._worker_gen_cands, enc._generate_residual_candidates,
+                      qt_mod.extract_adaptive_tiles, qt_mod.decompose_quadtree, enc._get_persistent_worker_pool,
+                      enc._fit_adaptive_state, qt_mod.MAX_PRIMITIVES_BY_TILE_SIZE)
+        gr.gpu_batch_score_prepacked = score
+        enc._worker_gen_cands = worker
+        enc._generate_residual_candidates = resid
+        qt_mod.extract_adaptive_tiles = extract
+        qt_mod.decompose_quadtree = decomp
+        enc._get_persistent_worker_pool = lambda: None
+        enc._fit_adaptive_state = fit
+        if self.cap is not None:
+            qt_mod.MAX_PRIMITIVES_BY_TILE_SIZE = {s: self.cap for s in (8, 16, 32, 64)}
+        return self
+
+    def __exit__(self, *exc):
+        enc, gr, qt_mod = self.ref["encoder"], self.ref["gpu_render"], self.ref["quadtree"]
+        (gr.gpu_batch_score_prepacked, enc._worker_gen_cands, enc._generate_residual_candidates,
+         qt_mod.extract_adaptive_tiles, qt_mod.decompose_quadtree, enc._get_persistent_worker_pool,
+         enc._fit_adaptive_state, qt_mod.MAX_PRIMITIVES_BY_TILE_SIZE) = self.saved
+        return False
+
+    def arrays(self) -> dict:
+        """Pools, re-seeds and selections (indices into each tile's extended pool) as arrays."""
+        state = self.state
+        n_tiles = len(state.quad_tiles)
+        ext_pools = {i: list(self.pools[i]) for i in range(n_tiles)}
+        for i, cands in self.reseeds:
+            ext_pools[i].extend(cands)
+        sel_idx = []
+        for i in range(n_tiles):
+            sel_idx.append([next(j for j, c in enumerate(ext_pools[i]) if c is p) for p in state.selected_per_tile[i]])
+        init = _concat_packs([_pack_full(self.pools[i]) for i in range(n_tiles)])
+        rs = _concat_packs([_pack_full(c) for _, c in self.reseeds])
+        sel_flat = np.full((n_tiles, 32), -1, np.int32)
+        for i, ids in enumerate(sel_idx):
+            sel_flat[i, : len(ids)] = ids
+        print(f"fit: {n_tiles} tiles, {self.stats['launches']} launches, {self.stats['evals']} evals, "
+              f"{len(self.reseeds)} reseeds, prims/tile {np.mean([len(s) for s in sel_idx]):.2f}")
+        return dict(image=state.image.astype(np.float32),
+                    qt=np.array([(q.x, q.y, q.size) for q in state.quad_tiles], np.int32),
+                    quality=np.int32(state.quality), lam=np.float64(state.lam), selected=sel_flat,
+                    reseed_tile=np.array([i for i, _ in self.reseeds], np.int32),
+                    **{"pool_" + k: v for k, v in init.items()}, **{"rs_" + k: v for k, v in rs.items()})
+
+
 def gen_fit(ref, name: str = "fit_small.npz", size: int = 64, n_prims: int = 10, seed: int = 5,
             quality: int = 75) -> None:
     from PIL import Image
     from weft_b200.synth import make_image_u8
 
-    enc = ref["encoder"]
-    gr = ref["gpu_render"]
-    qt_mod = ref["quadtree"]
-    cfg_t = ref["EncodeConfig"]
-    score, stats = _cpu_score_prepacked(ref)
+    img_u8 = make_image_u8(size, size, n_prims, seed)
+    with _FitCapture(ref) as cap, tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "in.png")
+        Image.fromarray(img_u8).save(path)
+        ref["encoder"]._fit_adaptive_state(path, ref["EncodeConfig"](quality=quality))
+    _save(name, image_u8=img_u8, **cap.arrays())
 
-    pools: dict[int, list] = {}
-    reseeds: list[tuple[int, list]] = []
-    patches_holder: dict = {}
-    orig_worker = enc._worker_gen_cands
-    orig_resid = enc._generate_residual_candidates
-    orig_extract = qt_mod.extract_adaptive_tiles
 
-    def extract(image, tiles):
-        patches = orig_extract(image, tiles)
-        patches_holder["p"] = patches
-        patches_holder["t"] = tiles
-        return patches
+def gen_fit_cfg256(ref) -> None:
+    """The plain-method workload at 256x256: 40 primitives, seed 0, q=75, fixed 32-px tiles, at
+    most 8 primitives per tile, primitive-stack basis only (``encode_image`` with no feature
+    flags), then the reference decoder at native size."""
+    from PIL import Image
+    from weft_b200.synth import make_image_u8
 
-    def worker(args):
-        cands, packed = orig_worker(args)
-        idx = next(i for i, p in enumerate(patches_holder["p"]) if p is args[0])
-        pools[idx] = list(cands)
-        return cands, packed
-
-    def resid(tile, pred, quality):
-        out = orig_resid(tile, pred, quality)
-        idx = next(i for i, p in enumerate(patches_holder["p"]) if p is tile)
-        reseeds.append((idx, list(out)))
-        return out
-
-    saved = (gr.gpu_batch_score_prepacked, enc._worker_gen_cands, enc._generate_residual_candidates,
-             qt_mod.extract_adaptive_tiles, enc._get_persistent_worker_pool)
-    gr.gpu_batch_score_prepacked = score
-    enc._worker_gen_cands = worker
-    enc._generate_residual_candidates = resid
-    qt_mod.extract_adaptive_tiles = extract
-    enc._get_persistent_worker_pool = lambda: None
+    enc, dec_mod, prim_chunks = ref["encoder"], ref["decoder"], ref["prim_chunks"]
+    img_u8 = make_image_u8(256, 256, 40, 0)
+    saved = dec_mod._decode_prim_payload
+    dec_mod._decode_prim_payload = lambda weft: (
+        prim_chunks.decode_prim_payload(weft.prim_payload, weft.toc, weft.chunk_index), "cpu")
     try:
-        img_u8 = make_image_u8(size, size, n_prims, seed)
-        with tempfile.TemporaryDirectory() as td:
-            path = os.path.join(td, "in.png")
-            Image.fromarray(img_u8).save(path)
-            state = enc._fit_adaptive_state(path, cfg_t(quality=quality))
+        with _FitCapture(ref, tile_size=32, cap=8) as cap, tempfile.TemporaryDirectory() as td:
+            src = os.path.join(td, "in.png")
+            Image.fromarray(img_u8).save(src)
+            out = os.path.join(td, "out.weft")
+            enc.encode_image(src, out, ref["EncodeConfig"](quality=75))
+            blob = open(out, "rb").read()
+            decoded = dec_mod.decode_to_array(out)
     finally:
-        (gr.gpu_batch_score_prepacked, enc._worker_gen_cands, enc._generate_residual_candidates,
-         qt_mod.extract_adaptive_tiles, enc._get_persistent_worker_pool) = saved
-
-    n_tiles = len(state.quad_tiles)
-    ext_pools = {i: list(pools[i]) for i in range(n_tiles)}
-    for i, cands in reseeds:
-        ext_pools[i].extend(cands)
-    sel_idx = []
-    for i in range(n_tiles):
-        ids = []
-        for p in state.selected_per_tile[i]:
-            ids.append(next(j for j, c in enumerate(ext_pools[i]) if c is p))
-        sel_idx.append(ids)
-    init = _concat_packs([_pack_full(pools[i]) for i in range(n_tiles)])
-    rs = _concat_packs([_pack_full(c) for _, c in reseeds])
-    sel_flat = np.full((n_tiles, 32), -1, np.int32)
-    for i, ids in enumerate(sel_idx):
-        sel_flat[i, : len(ids)] = ids
-    print(f"fit: {n_tiles} tiles, {stats['launches']} launches, {stats['evals']} evals, "
-          f"{len(reseeds)} reseeds, prims/tile {np.mean([len(s) for s in sel_idx]):.2f}")
-    _save(name,
-          image_u8=img_u8, image=state.image.astype(np.float32),
-          qt=np.array([(q.x, q.y, q.size) for q in state.quad_tiles], np.int32),
-          quality=np.int32(quality), lam=np.float64(state.lam),
-          selected=sel_flat,
-          reseed_tile=np.array([i for i, _ in reseeds], np.int32),
-          **{"pool_" + k: v for k, v in init.items()},
-          **{"rs_" + k: v for k, v in rs.items()})
+        dec_mod._decode_prim_payload = saved
+    assert {int(q.size) for q in cap.state.quad_tiles} == {32}
+    assert max(len(s) for s in cap.state.selected_per_tile) <= 8
+    print(f"cfg256: file {len(blob)} B")
+    _save("fit_cfg256.npz", image_u8=img_u8, weft_file=np.frombuffer(blob, np.uint8),
+          decoded=decoded.astype(np.float32), **cap.arrays())
 
 
 def gen_container(ref) -> None:
@@ -684,7 +743,12 @@ def gen_container_dct(ref) -> None:
 
 
 def main() -> None:
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+    args = sys.argv[1:]
+    src = os.environ.get("WEFT_REFERENCE_SRC")
+    if args and os.path.isdir(args[0]):
+        src = args.pop(0)
+    if not src:
+        sys.exit("usage: make_golden.py REFERENCE_SRC [fixture ...]  (or set WEFT_REFERENCE_SRC)")
     sys.path.insert(0, src)
     import weft.bitstream as bitstream_mod
     import weft.dct_residual as dct_residual
@@ -704,11 +768,12 @@ def main() -> None:
         "Primitive": primitives.Primitive, "TileRecord": primitives.TileRecord, "EncodeConfig": EncodeConfig,
         "decoder": decoder, "bitstream": bitstream_mod, "dct_residual": dct_residual,
     }
-    which = set(sys.argv[2:]) if len(sys.argv) > 2 else None
+    which = set(args) if args else None
     for name, fn in (("render_tiles", gen_render_tiles), ("render_scene", gen_render_scene), ("rate", gen_rate),
                      ("entropy", gen_entropy), ("quant", gen_quant), ("quadtree", gen_quadtree),
                      ("candidates", gen_candidates), ("fit", gen_fit),
-                     ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("container", gen_container),
+                     ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("fit_cfg256", gen_fit_cfg256),
+                     ("container", gen_container),
                      ("dct", gen_dct), ("container_dct", gen_container_dct)):
         if which is None or name in which:
             fn(ref)

@@ -63,9 +63,3 @@ def test_host_entry_points_reject_bad_descriptors_without_gpu_work():
     prims = np.zeros(1, _lib.PRIM_DTYPE)
     rc = lib.weftk_score_evals_host(_lib.ptr(ev), 1, _lib.ptr(prims), 1, _lib.ptr(tiles), 3, _lib.ptr(out), 0)
     assert rc == -1 and "out of range" in _lib.last_error()
-
-
-def test_integration_notes_list_every_entry_point():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    missing = [n for n in declared_entry_points() if n not in text]
-    assert not missing, f"entry points missing from INTEGRATION.md: {missing}"

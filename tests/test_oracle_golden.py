@@ -152,3 +152,38 @@ def test_greedy_fit_matches_reference_selection(golden, name):
     want = [[int(v) for v in row if v >= 0] for row in g["selected"]]
     assert sel == want
     assert all(len(v) == 0 for v in queue.values())
+
+
+def test_greedy_schedule_replays_a_subset(golden):
+    """A subset of tiles given the full fit's round schedule takes the full fit's decisions."""
+    g = golden("fit_small.npz")
+    tiles, patches, pools, reseeds = _fit_inputs(g)
+    sizes = [t.size for t in tiles]
+
+    def run(idx, schedule=None):
+        queue = {k: list(v) for k, v in reseeds.items()}
+        return fit.greedy_fit([patches[i] for i in idx], [sizes[i] for i in idx], [pools[i] for i in idx],
+                              int(g["quality"]), lambda j, patch, pred: queue[idx[j]].pop(0), schedule=schedule)
+
+    full = list(range(len(tiles)))
+    sel, cur, stats = run(full)
+    assert stats["schedule"] and not all(stats["schedule"])
+    sub = full[1::3]
+    sel2, cur2, _ = run(sub, stats["schedule"])
+    assert sel2 == [sel[i] for i in sub]
+    np.testing.assert_array_equal(cur2, cur[sub])
+
+
+def test_greedy_fit_matches_reference_on_fixed_32px_tiles(golden):
+    """The plain-method workload (256x256, 40 primitives, seed 0, q=75, fixed 32-px tiles, cap 8):
+    the reference's own encode selected one primitive per tile and re-seeded every tile three
+    times (every round stalled), so the first 16 tiles alone follow the same rounds."""
+    g = golden("fit_cfg256.npz")
+    tiles, patches, pools, reseeds = _fit_inputs(g)
+    n = 16
+    assert {t.size for t in tiles} == {32}
+    queue = {k: list(v) for k, v in reseeds.items() if k < n}
+    sel, cur, stats = fit.greedy_fit(patches[:n], [32] * n, pools[:n], int(g["quality"]),
+                                     lambda i, patch, pred: queue[i].pop(0), caps=[8] * n)
+    assert sel == [[int(v) for v in row if v >= 0] for row in g["selected"][:n]]
+    assert stats["reseeds"] == 3 * n and all(len(v) == 0 for v in queue.values())

@@ -113,6 +113,8 @@ SIGNATURES: dict[str, list] = {
     "weftk_fit_variant": [_I, _I, _P, _P, _P],
     "weftk_dct_apply": [_P, _I, _P, _I64, _I, _I, ctypes.c_float, ctypes.c_float, _I, _P, _I, _I, _I, _P],
     "weftk_raster_resize": [_P, _I, _I, _P, _I, _I, _P, _P],
+    "weftk_quantize_rows": [_P, _P, _I, _P, _P],
+    "weftk_fit_selected_rows": [_P, _P, _P, _P],
 }
 
 _lock = threading.Lock()

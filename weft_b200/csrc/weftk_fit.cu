@@ -176,8 +176,11 @@ __global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, c
     if (!(st.flags[t] & WEFTK_TILE_EVAL)) return;
     const int ts = st.size[t];
     const bool closed_form = mode_init && st.moments != nullptr;
+    // a slot range outside the state's slot arrays (a malformed caller-built pool table) is
+    // rejected, never scored: the per-candidate scratch is indexed by slot
     if (ts < expect_min || ts > expect_max || w.count > MAX_ITEM || w.block * 1024 >= ts * ts || w.first < 0 ||
-        w.first + w.count > st.pool_cap[t]) {
+        w.first + w.count > st.pool_cap[t] || st.pool_off[t] < 0 ||
+        (long long)st.pool_off[t] + w.first + w.count > st.n_slots) {
         if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
         return;
     }
@@ -318,6 +321,10 @@ __global__ void __launch_bounds__(128) fit_select_kernel(WeftFitState st, int mo
     const int ts = st.size[t], npix = ts * ts, nb = (npix + 1023) / 1024;
     const long long off = st.pool_off[t];
     const int cnt = st.pool_cnt[t];
+    if (off < 0 || cnt < 0 || cnt > st.pool_cap[t] || off + cnt > st.n_slots) {
+        if (lane == 0) fit_report(WEFTK_E_ARG);
+        return;
+    }
     const int base_bits = (mode == WEFTK_FIT_INIT) ? 8 : st.sel_bits[t];
     const float denom = (float)(3 * npix);
     float best = __int_as_float(0x7f800000);

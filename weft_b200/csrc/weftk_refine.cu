@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "../../include/weftk_fit.h"
 #include "../../include/weftk_refine.h"
@@ -912,15 +914,24 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
     }
     // single constant/linear layers only (declared by the caller, checked per tile): register path
     const bool cl1 = set.max_prims <= 1 && set.kinds_mask != 0 && (set.kinds_mask & ~0x3) == 0;
-    static int attr[2] = {48 * 1024, 48 * 1024};
-    if (smem > attr[cl1]) {
-        if (cl1)
-            WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE, true>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        else
-            WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE, false>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr[cl1] = smem;
+    // the dynamic shared-memory opt-in is per device and per kernel instance: remember the
+    // largest size set on each device (under a lock, so concurrent first calls agree)
+    {
+        int dev = 0;
+        WEFTK_CUDA(cudaGetDevice(&dev));
+        static std::mutex mu;
+        static std::map<int, int> granted[2];
+        std::lock_guard<std::mutex> lock(mu);
+        int& have = granted[cl1].try_emplace(dev, 48 * 1024).first->second;
+        if (smem > have) {
+            if (cl1)
+                WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE, true>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            else
+                WEFTK_CUDA(cudaFuncSetAttribute(refine_tiles_kernel<MODE, false>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            have = smem;
+        }
     }
     if (cl1)
         refine_tiles_kernel<MODE, true><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags,

@@ -16,6 +16,9 @@
 // the platform's sort implementation).
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <set>
+
 #include <climits>
 
 #include "../../include/weftk_fit.h"
@@ -407,10 +410,16 @@ using namespace weftk;
 int launch_fit_reseed(const WeftFitState& st, const int* gate, cudaStream_t stream) {
     if (st.n_tiles == 0) return WEFTK_OK;
     const int smem = 2 * 64 * 64 * (int)sizeof(float);
-    static bool attr_set = false;
-    if (!attr_set) {
-        WEFTK_CUDA(cudaFuncSetAttribute(fit_reseed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr_set = true;
+    {  // the dynamic shared-memory opt-in is per device: set it once per device, under a lock
+        int dev = 0;
+        WEFTK_CUDA(cudaGetDevice(&dev));
+        static std::mutex mu;
+        static std::set<int> done;
+        std::lock_guard<std::mutex> lock(mu);
+        if (!done.count(dev)) {
+            WEFTK_CUDA(cudaFuncSetAttribute(fit_reseed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            done.insert(dev);
+        }
     }
     fit_reseed_kernel<<<st.n_tiles, RS_THREADS, smem, stream>>>(st, gate);
     WEFTK_CUDA(cudaGetLastError());

@@ -348,6 +348,7 @@ class BatchedFit:
                 del p[self.init_cnt[t]:]
         self.kinds[:] = self._init_kinds
         self._device_consts()
+        self._moments()
         _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), self._stream()),
                    "weftk_fit_reset")
         _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), self._stream()),
@@ -363,26 +364,60 @@ class BatchedFit:
 
     def run_init_only(self) -> None:
         """Reset and run only the init round (best single candidate per tile), launching
-        device work only: no host copies or syncs, so it can be captured in a CUDA graph."""
+        device work only: no host copies or syncs, so it can be captured in a CUDA graph.
+        With the closed-form init on, the per-tile moments are computed first."""
         self._device_consts()
-        _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), self._stream()),
-                   "weftk_fit_reset")
-        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), self._stream()),
+        s = self._stream()
+        self._moments()
+        _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), s), "weftk_fit_reset")
+        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), s),
                    "weftk_fit_prepare")
         ti = self.t_items
         rc = self.lib.weftk_fit_round(ctypes_ref(self.st), FIT_INIT, self.lam, self.thr, _lib.ptr(self.t_perm),
                                       _lib.ptr(ti[8]), self.n_items[8], _lib.ptr(ti[16]), self.n_items[16],
-                                      _lib.ptr(ti[32]), self.n_items[32], self._stream())
+                                      _lib.ptr(ti[32]), self.n_items[32], s)
         _lib.check(rc, "weftk_fit_round")
+
+    def _moments(self) -> None:
+        """Per-tile pixel moments for the closed-form init, when it is on (device work only)."""
+        if self.st.moments:
+            _lib.check(self.lib.weftk_fit_moments(ctypes_ref(self.st), self.st.moments, self._stream()),
+                       "weftk_fit_moments")
+
+    def quantize_selected(self) -> None:
+        """Snap every tile's selected stack to the wire grid into ``t_qrows`` / ``t_qkind``
+        (``weftk_fit_selected_rows``: row ``t * cap_max + j`` is the j-th primitive of tile t,
+        kind -1 past the stack).  Device work only."""
+        if not hasattr(self, "t_qrows"):
+            self.t_qrows = torch.zeros((self.n * self.cap_max, 16), dtype=torch.float32, device=self.device)
+            self.t_qkind = torch.full((self.n * self.cap_max,), -1, dtype=torch.int32, device=self.device)
+        _lib.check(self.lib.weftk_fit_selected_rows(ctypes_ref(self.st), _lib.ptr(self.t_qrows),
+                                                    _lib.ptr(self.t_qkind), self._stream()),
+                   "weftk_fit_selected_rows")
+
+    def quantized_stacks(self) -> list[np.ndarray]:
+        """The last ``quantize_selected`` output as per-tile 60-byte records (host)."""
+        from .refine import rows_to_records
+
+        rows = self.t_qrows.cpu().numpy()
+        kinds = self.t_qkind.cpu().numpy()
+        out = []
+        for t in range(self.n):
+            k = kinds[t * self.cap_max:(t + 1) * self.cap_max]
+            m = int((k >= 0).sum())
+            out.append(rows_to_records(rows[t * self.cap_max:t * self.cap_max + m], k[:m]))
+        return out
 
     def run_device(self, max_rounds: int | None = None) -> "BatchedFit":
         """Reset and run the whole fit with device re-seeding, enqueued without any host
-        synchronisation (``weftk_fit_run``), so it can be captured in a CUDA graph.  Same
-        decisions as ``run()`` with device re-seeding; ``control()`` reads the outcome."""
+        synchronisation (``weftk_fit_run``), so it can be captured in a CUDA graph, and snap the
+        selected stacks to the wire grid (``quantize_selected``).  Same decisions as ``run()``
+        with device re-seeding; ``control()`` reads the outcome."""
         self._device_consts()
         if not hasattr(self, "t_ctl"):
             self.t_ctl = torch.zeros(4, dtype=torch.int32, device=self.device)
         s = self._stream()
+        self._moments()
         _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), s), "weftk_fit_reset")
         _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), s),
                    "weftk_fit_prepare")
@@ -392,6 +427,7 @@ class BatchedFit:
                                     _lib.ptr(ti[8]), self.n_items[8], _lib.ptr(ti[16]), self.n_items[16],
                                     _lib.ptr(ti[32]), self.n_items[32], _lib.ptr(self.t_ctl), s)
         _lib.check(rc, "weftk_fit_run")
+        self.quantize_selected()
         self.device_reseeded = True
         return self
 
@@ -406,13 +442,12 @@ class BatchedFit:
 
     def use_closed_form_init(self, on: bool = True) -> "BatchedFit":
         """Score constant candidates of the init round in closed form from per-tile pixel
-        moments (``WeftFitState.moments``) instead of per pixel; equal up to rounding, so a near
-        tie may pick differently from the reference's per-pixel sum (off for the plain fit)."""
+        moments (``WeftFitState.moments``, computed by every ``run_init_only``) instead of per
+        pixel; equal up to rounding, so a near tie may pick differently from the reference's
+        per-pixel sum (off for the plain fit)."""
         if on:
             if not hasattr(self, "t_moments"):
                 self.t_moments = torch.zeros(max(self.n, 1) * 6, dtype=torch.float64, device=self.device)
-                _lib.check(self.lib.weftk_fit_moments(ctypes_ref(self.st), _lib.ptr(self.t_moments), self._stream()),
-                           "weftk_fit_moments")
             self.st.moments = _lib.ptr(self.t_moments)
         else:
             self.st.moments = None
@@ -508,6 +543,7 @@ class BatchedFit:
         (default ``candidates.residual_candidates``); ``reseed_batch(tiles,
         patches, preds) -> list[list[Cand]]`` does all stalled tiles at once.
         """
+        self._moments()
         self._round(FIT_INIT)
         rounds = rate.max_rounds(self.quality) if max_rounds is None else int(max_rounds)
         stalls = 0

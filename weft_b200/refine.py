@@ -150,21 +150,13 @@ class StackSet:
                 params[:, col] = torch.where(k == kind, params[:, col].clamp(0.0, 4.0), params[:, col])
 
     def quantize(self, params: torch.Tensor) -> torch.Tensor:
-        """Snap to the wire grid: coordinates u16 over [0, 15], thickness u16 over [0, 4],
-        colours u8, alpha u16 (half-to-even rounding, as Python's round)."""
-        p = params.detach().to(torch.float64).clone()
-        k = self.t_kind
-        p[:, 7:13] = torch.round(p[:, 7:13].clamp(0, 1) * 255.0) / 255.0
-        p[:, 13] = torch.round(p[:, 13].clamp(0, 1) * 65535.0) / 65535.0
-        g = torch.round((p[:, 0:7] / 15.0).clamp(0, 1) * 65535.0) / 65535.0 * 15.0
-        th = torch.where(k == 2, 4, torch.where(k == 3, 6, -1))
-        gt = torch.round((p[:, 0:7] / 4.0).clamp(0, 1) * 65535.0) / 65535.0 * 4.0
-        col = torch.arange(7, device=p.device)[None, :]
-        g = torch.where(col == th[:, None], gt, g)
-        ng = torch.tensor([GEOM_LEN.get(i, 0) for i in range(8)], device=p.device)[k.clamp(0, 7).long()]
-        p[:, 0:7] = torch.where((col < ng[:, None]) & (k[:, None] != 0), g, p[:, 0:7])
-        return p.to(torch.float32)
-
+        """Snap to the wire grid on the device (``weftk_quantize_rows``; no host sync)."""
+        params = params.detach().contiguous()
+        out = torch.empty_like(params)
+        kinds = self.t_kind.to(torch.int32).contiguous()
+        _lib.check(self.lib.weftk_quantize_rows(_lib.ptr(params), _lib.ptr(kinds), int(params.shape[0]),
+                                                _lib.ptr(out), self._stream()), "weftk_quantize_rows")
+        return out
 
     def to_stacks(self, params: torch.Tensor) -> list[list]:
         """Parameter rows -> per-tile ``Cand`` lists (host)."""
@@ -175,6 +167,26 @@ class StackSet:
         cands = unpack_cands(recs)
         off = self.prim_off_np
         return [cands[off[t]:off[t + 1]] for t in range(self.n)]
+
+
+def quantize_rows(params: torch.Tensor, kinds: torch.Tensor) -> torch.Tensor:
+    """Parameter rows snapped to the wire grid (the reference's ``_quantize_primitive``,
+    src/weft/encoder.py:211-237): coordinates u16 over [0, 15], thickness u16 over [0, 4],
+    colours u8, alpha u16, half-to-even rounding as Python's ``round``, in float64.  Plain torch
+    on any device; ``StackSet.quantize`` is the device kernel of the same rule."""
+    p = params.detach().to(torch.float64).clone()
+    k = kinds.to(p.device).to(torch.int64)
+    p[:, 7:13] = torch.round(p[:, 7:13].clamp(0, 1) * 255.0) / 255.0
+    p[:, 13] = torch.round(p[:, 13].clamp(0, 1) * 65535.0) / 65535.0
+    g = torch.round((p[:, 0:7] / 15.0).clamp(0, 1) * 65535.0) / 65535.0 * 15.0
+    th = torch.where(k == 2, 4, torch.where(k == 3, 6, -1))
+    gt = torch.round((p[:, 0:7] / 4.0).clamp(0, 1) * 65535.0) / 65535.0 * 4.0
+    col = torch.arange(7, device=p.device)[None, :]
+    g = torch.where(col == th[:, None], gt, g)
+    ng = torch.tensor([GEOM_LEN.get(i, 0) for i in range(8)], device=p.device)[k.clamp(0, 7)]
+    ng = torch.where(k < 0, 0, ng)
+    p[:, 0:7] = torch.where((col < ng[:, None]) & (k[:, None] != 0), g, p[:, 0:7])
+    return p.to(torch.float32)
 
 
 def kinds_mask_of(kinds: np.ndarray) -> int:
@@ -299,8 +311,10 @@ class FusedRefiner:
 
 class RefinedFit:
     """The refined batched fit as one CUDA graph: init-only candidate scoring over the
-    fit's (possibly kind-filtered) pools, gather of each tile's selected primitive, and
-    ``steps`` fused Adam steps.  Every launch is device work on torch's current stream."""
+    fit's (possibly kind-filtered) pools (with the closed-form init, the tile moments it
+    needs first), gather of each tile's selected primitive, ``steps`` fused Adam steps, and
+    the refined rows snapped to the wire grid (``q_rows``).  Every launch is device work on
+    torch's current stream."""
 
     def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True, residual: bool = False,
                  closed_form_init: bool = True):
@@ -318,6 +332,7 @@ class RefinedFit:
         self.refiner = FusedRefiner(self.ss, torch.zeros((n_rows, 16), dtype=torch.float32, device=dev), lr=lr,
                                     residual=residual)
         self.steps = int(steps)
+        self.q_rows = torch.zeros((n_rows, 16), dtype=torch.float32, device=dev)  # refined rows on the wire grid
         self.pool_off = torch.from_numpy(fit.pool_off).to(dev)
         self.graph = None
         self.use_graph = use_graph
@@ -330,6 +345,8 @@ class RefinedFit:
                                                   _lib.ptr(fr.p), _lib.ptr(fr.m), _lib.ptr(fr.v),
                                                   _lib.ptr(self.kinds), self.ss._stream()), "weftk_refine_start")
         fr.run(self.steps)
+        _lib.check(self.ss.lib.weftk_quantize_rows(_lib.ptr(fr.p), _lib.ptr(self.kinds), int(self.kinds.numel()),
+                                                   _lib.ptr(self.q_rows), self.ss._stream()), "weftk_quantize_rows")
 
     @property
     def start(self) -> torch.Tensor:

@@ -53,20 +53,18 @@ CAP = 16
 def _pool_cands(args):
     patch, q = args[:2]
     kinds = args[2] if len(args) > 2 else None
+    atan2 = args[3] if len(args) > 3 else "numpy"
     from weft_b200.fit import pack_cands
 
-    return pack_cands(candidates.tile_candidates(patch, q, kinds=kinds))
+    return pack_cands(candidates.tile_candidates(patch, q, kinds=kinds, atan2=atan2))
 
 
-def restricted_pools(patches, pools, kinds, executor):
-    """Pools of the given kinds generated directly (host, ``executor`` processes), timed, and checked
-    against the full pools filtered to those kinds."""
+def restricted_pools(patches, kinds, executor, atan2: str = "rounded"):
+    """Pools of the given kinds generated on the host (``executor`` processes), timed; with the
+    device generator's float32 arctan2 rule they are the device pools' reference."""
     t0 = time.perf_counter()
-    got = list(executor.map(_pool_cands, [(p, QUALITY, tuple(kinds)) for p in patches], chunksize=32))
-    gen_s = time.perf_counter() - t0
-    same = all(np.array_equal(g.view(np.uint8), f[np.isin(f["kind"], kinds)].view(np.uint8))
-               for g, f in zip(got, pools))
-    return got, gen_s, same
+    got = list(executor.map(_pool_cands, [(p, QUALITY, tuple(kinds), atan2) for p in patches], chunksize=32))
+    return got, time.perf_counter() - t0
 
 
 def _oracle_shard(args):
@@ -613,6 +611,70 @@ def refined_headline(args, local, pixels, sizes, pools, stream, world):
     return rf, fast, rec, cnt, statistics.mean(times)
 
 
+def device_headline(args, fit, sizes, caps, stream, world):
+    """The refined fit with its pools generated on the device: pool generation, init round, fused
+    Adam steps and wire-grid snap replayed from one CUDA graph over the resident tiles.  Each timed
+    step is preceded by a 256 MiB write and a short GPU sleep (host launch latency not counted)."""
+    import torch
+
+    from weft_b200.pools import DeviceRefinedFit
+
+    drf = DeviceRefinedFit(fit.t_src, sizes, QUALITY, caps=caps, steps=args.refine_steps, lr=args.refine_lr)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=fit.device)
+    for _ in range(args.warmup):
+        drf.run()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda._sleep(100000)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        drf.run()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return drf, statistics.mean(times)
+
+
+def device_breakdown(args, drf, lib, stream) -> dict:
+    """Eager run of the device pipeline with CUDA events around its parts: pool generation, the
+    init round's scoring kernels (events inside the library), the Adam steps."""
+    import ctypes
+
+    import torch
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record(stream)
+    drf.generate()
+    b.record(stream)
+    torch.cuda.synchronize()
+    gen_ms = a.elapsed_time(b)
+    lib.weftk_fit_timing(1, None, None)
+    drf.fit.run_init_only()
+    torch.cuda.synchronize()
+    score_ms, n_score = ctypes.c_double(0), ctypes.c_int(0)
+    lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
+    fr = drf.rf.refiner
+    fr.restart(drf.rf.start)
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record(stream)
+    fr.run(args.refine_steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return {"gen_ms": gen_ms, "init_score_ms": score_ms.value, "init_score_launches": n_score.value,
+            "refine_ms": a.elapsed_time(b), "work": drf.fit.work_counters()}
+
+
 def refined_breakdown(args, rf, fast, lib, stream):
     """Eager run of the same pipeline: scoring-kernel time of the init round (events inside
     the library) and the mean refine-step kernel time (events around the steps)."""
@@ -987,44 +1049,57 @@ def run_weft(args, world, rank, local, executor, cores):
 
     plain_e2e_val, (p_h2d, p_d2h) = timed_e2e(plain_e2e)
 
-    # headline: the gradient-refined fit, at iso RD with the plain fit
-    sampler2 = ClockSampler(local)
-    sampler2.start()
-    rf, fast, frec, fcnt, ref_ms = refined_headline(args, local, pixels, sizes, pools, stream, world)
-    clocks2 = sampler2.stop()
-    # host generation of the refined fit's pools alone (outside the clock window: no GPU work)
-    _, cl_gen_s, cl_same = restricted_pools(patches, pools, REFINE_POOLS[args.refine_pool], executor)
-    cl_gen_s, gen_s = max_over_ranks(cl_gen_s, world), max_over_ranks(cand_s, world)
-    ref_ms = max_over_ranks(ref_ms, world)
-    ref_value = world * n_px / (ref_ms * 1e-3) / 1e6
-    plain_rd = rd["plain"] if rd else rd_of_params(*fit.stack_set(), tiles, patches, img, args.size)
-    ref_rd = rd_of_params(rf.ss, rf.refiner.p, tiles, patches, img, args.size)
-    rd_delta = ref_rd["rd_score"] - plain_rd["rd_score"]
-    iso = rd_delta >= -0.05
+    # the refined fit over host-generated pools (the reference's generators, kind-filtered)
+    rf, fast, frec, fcnt, host_ref_ms = refined_headline(args, local, pixels, sizes, pools, stream, world)
+    host_ref_ms = max_over_ranks(host_ref_ms, world)
     r_score_ms, r_n_score, r_step_ms, r_work = refined_breakdown(args, rf, fast, lib, stream)
     r_flops = refine_flops(rf.ss)
     refine_tflops = r_flops / (r_step_ms * 1e-3) / 1e12 if r_step_ms > 0 else 0.0
     init_tflops = r_work[1] / (r_score_ms * 1e-3) / 1e12 if r_score_ms > 0 else 0.0
-    refine_share = args.refine_steps * r_step_ms
-    n_cls = sum(1 for k in (8, 16, 32) if fast.n_items[k])
-    # moments, reset, prepare, begin, select, end, scoring (one per size class), refine start, one
-    # launch for all refine steps, wire-grid snap
-    ref_launches = 9 + n_cls
+    host_ref_rd = rd_of_params(rf.ss, rf.refiner.p, tiles, patches, img, args.size)
+    del rf, fast
 
-    frec_h = pinned_copy(frec, pin_keep)
+    # headline: pool generation + the gradient-refined fit on the device, one CUDA graph, at iso
+    # RD with the plain fit
+    sampler2 = ClockSampler(local)
+    sampler2.start()
+    drf, ref_ms = device_headline(args, fit, sizes, caps, stream, world)
+    clocks2 = sampler2.stop()
+    dbd = device_breakdown(args, drf, lib, stream)
+    # host generation of the same pools (the device generator's arctan2 rule), timed, outside the
+    # clock window (no GPU work); the device pools must equal them record for record
+    host_cl, cl_gen_s = restricted_pools(patches, REFINE_POOLS[args.refine_pool], executor)
+    dev_cl = drf.pool_records()
+    pools_equal = sum(1 for a, b in zip(dev_cl, host_cl) if a.tobytes() == b.tobytes())
+    cl_gen_s, gen_s = max_over_ranks(cl_gen_s, world), max_over_ranks(cand_s, world)
+    ref_ms = max_over_ranks(ref_ms, world)
+    ref_value = world * n_px / (ref_ms * 1e-3) / 1e6
+    plain_rd = rd["plain"] if rd else rd_of_params(*fit.stack_set(), tiles, patches, img, args.size)
+    dss = drf.rf.ss
+    ref_rd = rd_of_params(dss, drf.rf.refiner.p, tiles, patches, img, args.size)
+    rd_delta = ref_rd["rd_score"] - plain_rd["rd_score"]
+    iso = rd_delta >= -0.05
+    d_flops = refine_flops(dss)
+    d_refine_tflops = d_flops * args.refine_steps / (dbd["refine_ms"] * 1e-3) / 1e12 if dbd["refine_ms"] else 0.0
+    d_init_tflops = dbd["work"][1] / (dbd["init_score_ms"] * 1e-3) / 1e12 if dbd["init_score_ms"] else 0.0
+    n_cls = sum(1 for k in (8, 16, 32) if drf.fit.n_items[k])
+    n_gen = sum(1 for t in drf.lists if t is not None)
+    # pool generation (one launch per tile side), moments, reset, prepare, begin, select, end,
+    # scoring (one per size class), refine start, one launch for all refine steps, wire-grid snap
+    ref_launches = n_gen + 9 + n_cls
+    # what the Adam steps add: RD of the same init round's picks without them
+    init_rd = rd_of_params(dss, drf.rf.start, tiles, patches, img, args.size)
+
+    pixels_h = pinned_copy(pixels, pin_keep)
 
     def refined_e2e():
-        from weft_b200.refine import RefinedFit
+        from weft_b200.pools import refine_tiles
 
-        f2 = BatchedFit.from_arrays(pixels_h, sizes, frec_h, fcnt, QUALITY, caps=caps, device=local, reserve=0)
-        r2 = RefinedFit(f2, steps=args.refine_steps, lr=args.refine_lr, use_graph=False)
-        r2.run()
-        out_rows = r2.q_rows.cpu()
-        return int(pixels.nbytes + frec.nbytes + sizes.nbytes + fcnt.nbytes), int(out_rows.numel() * 4)
+        rows, kinds = refine_tiles(pixels_h, sizes, QUALITY, caps=caps, steps=args.refine_steps, lr=args.refine_lr,
+                                   device=local)
+        return int(pixels.nbytes + sizes.nbytes), int(rows.nbytes + kinds.nbytes)
 
     ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
-    # what the Adam steps add: RD of the same init round's picks without them
-    init_rd = rd_of_params(rf.ss, rf.start, tiles, patches, img, args.size)
 
     diff = differentiable_fit(args, executor, local, stream) if args.diff_steps > 0 and rank == 0 else None
     ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None
@@ -1060,23 +1135,32 @@ def run_weft(args, world, rank, local, executor, cores):
                   "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
                   "score_ms_per_step": score_ms.value / args.steps, "score_launches": n_score.value,
                   "candidate_pixels_per_step": cand_px // args.steps}
-    refine_roof = {"bound": "fp32", "achieved": refine_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
-                   "frac": refine_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+    fp32_src = "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)"
+    refine_roof = {"bound": "fp32", "achieved": d_refine_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                   "frac": d_refine_tflops / peak_tflops if peak_tflops else None, "traffic": None,
                    "kernel": "refine_tiles_kernel (loss + gradient + Adam; all steps of a fit in one launch)",
-                   "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
-                   "ms_per_adam_step": r_step_ms, "adam_steps_per_launch": args.refine_steps,
-                   "flops_per_adam_step": r_flops}
-    init_roof = {"bound": "fp32", "achieved": init_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
-                 "frac": init_tflops / peak_tflops if peak_tflops else None, "traffic": None,
-                 "kernel": "fit_score_kernel, init round of the refined fit", "ms_per_step": r_score_ms,
-                 "launches": r_n_score}
-    dominant, other = (refine_roof, init_roof) if refine_share >= r_score_ms else (init_roof, refine_roof)
+                   "peak_source": fp32_src, "ms": dbd["refine_ms"], "adam_steps_per_launch": args.refine_steps,
+                   "flops_per_adam_step": d_flops}
+    init_roof = {"bound": "fp32", "achieved": d_init_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
+                 "frac": d_init_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+                 "kernel": "fit_score_kernel, init round of the refined fit", "ms": dbd["init_score_ms"],
+                 "launches": dbd["init_score_launches"], "peak_source": fp32_src}
+    n_cand = int(sum(len(p) for p in dev_cl))
+    gen_bytes = 16 * n_px + 60 * n_cand + 4 * len(tiles)
+    hbm_gbs, hbm_src = _hbm_peak()
+    gen_gbs = gen_bytes / (dbd["gen_ms"] * 1e-3) / 1e9 if dbd["gen_ms"] else 0.0
+    gen_roof = {"bound": "hbm", "achieved": gen_gbs, "peak": hbm_gbs, "unit": "GB/s", "frac": gen_gbs / hbm_gbs,
+                "traffic": None, "kernel": "gen_pool_kernel (one launch per tile side)", "ms": dbd["gen_ms"],
+                "algorithmic_bytes": gen_bytes, "candidates": n_cand, "peak_source": hbm_src,
+                "note": "latency-bound: every mean is a sequential float32 sum in numpy's order"}
+    parts = sorted([(dbd["gen_ms"], gen_roof), (dbd["init_score_ms"], init_roof), (dbd["refine_ms"], refine_roof)],
+                   key=lambda x: -x[0])
+    dominant = parts[0][1]
     head_value, head_ms = (ref_value, ref_ms) if iso else (plain_value, plain_ms)
     grad_db = ref_rd["rd_score"] - init_rd["rd_score"]
-    fit_desc = (f"gradient-refined batched fit: init round over the {args.refine_pool} candidates "
-                f"({len(frec)} of {int(sum(len(p) for p in pools))}), then {args.refine_steps} fused Adam steps "
-                f"(lr {args.refine_lr}) and the wire-grid snap, one CUDA graph; the Adam steps change RD by "
-                f"{grad_db:+.4f} dB over the init round alone" if iso else
+    fit_desc = (f"pools generated on the device ({REFINE_POOLS[args.refine_pool]} kinds, {n_cand} candidates), "
+                f"init round, {args.refine_steps} fused Adam steps (lr {args.refine_lr}) and the wire-grid snap, one "
+                f"CUDA graph; the Adam steps change RD by {grad_db:+.4f} dB over the init round alone" if iso else
                 "plain greedy fit (the refined fit missed iso RD)")
     details = {
         "plain": {"value": plain_value, "ms_per_step": plain_ms, "tiles_per_s": len(tiles) * world / (plain_ms * 1e-3),
@@ -1088,9 +1172,16 @@ def run_weft(args, world, rank, local, executor, cores):
                   "prim_payload_bytes": prim_bytes,
                   "autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
                                for k, v in tuned_plain.items()}},
-        "refined_autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
-                             for k, v in (fast.tuning or {}).items()},
-        "roofline_refine": refine_roof, "roofline_init": init_roof,
+        "refined_device": {"ms": ref_ms, "breakdown": {k: v for k, v in dbd.items() if k != "work"},
+                           "roofline_gen": gen_roof, "roofline_init": init_roof, "roofline_refine": refine_roof,
+                           "autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
+                                        for k, v in (drf.fit.tuning or {}).items()},
+                           "pools_equal_host": [pools_equal, len(tiles)], "candidates": n_cand},
+        "refined_host_pools": {"ms": host_ref_ms, "mpix_per_s": world * n_px / (host_ref_ms * 1e-3) / 1e6,
+                               "rd": host_ref_rd, "candidates": int(len(frec)),
+                               "score_ms": r_score_ms, "refine_ms_per_step": r_step_ms,
+                               "refine_tflops": refine_tflops, "init_tflops": init_tflops,
+                               "pools": "the reference's generators on the host (numpy arctan2), kind-filtered"},
         "iso_rd": {"plain": plain_rd, "refined": ref_rd, "init_round_only": init_rd},
         "decode": decode, "decode_with_residuals": decode_res, "decode_raster": raster_line,
         "differentiable_fit": diff, "image_batch": ibatch, "rd": rd, "parity": parity,
@@ -1106,8 +1197,8 @@ def run_weft(args, world, rank, local, executor, cores):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": bench_config(args, len(tiles), int(sum(len(p) for p in pools))),
         "fit": fit_desc,
-        "l2": "refined fit: 256 MiB written before each timed step (working set fits in L2); plain fit: per-step "
-              "working set (pixels + pools) exceeds L2, no flush",
+        "l2": "refined fit: 256 MiB written before each timed step; plain fit: per-step working set (pixels + "
+              "pools) exceeds L2, no flush",
         "e2e": {"value": ref_e2e_val if iso else plain_e2e_val, "unit": "MPix/s",
                 "h2d_bytes_per_step": r_h2d if iso else p_h2d, "d2h_bytes_per_step": r_d2h if iso else p_d2h},
         "roofline": dominant if iso else score_roof,
@@ -1119,10 +1210,11 @@ def run_weft(args, world, rank, local, executor, cores):
                   "roofline_frac": frac(score_roof), "reseeds": fit.stats.reseeds},
         "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
                    "init_only_rd": init_rd["rd_score"], "adam_steps_db": grad_db, "tolerance_db": 0.05},
-        "fit_total": {"refined_mpix_per_s": world * n_px / (cl_gen_s + ref_ms * 1e-3) / 1e6,
-                      "refined_cand_gen_s": cl_gen_s, "plain_mpix_per_s": world * n_px / (gen_s + plain_ms * 1e-3) / 1e6,
-                      "plain_cand_gen_s": gen_s, "cand_gen": f"host, {cores} processes",
-                      "pools_equal_filtered_full": bool(cl_same)},
+        "fit_total": {"refined_device_gen_mpix_per_s": ref_value,
+                      "refined_host_gen_mpix_per_s": world * n_px / (cl_gen_s + host_ref_ms * 1e-3) / 1e6,
+                      "plain_host_gen_mpix_per_s": world * n_px / (gen_s + plain_ms * 1e-3) / 1e6,
+                      "host_gen_s": {"constlin": cl_gen_s, "full": gen_s, "processes": cores},
+                      "device_pools_equal_host": f"{pools_equal}/{len(tiles)} tiles"},
         "decode": {"frac": frac(decode), "frac_with_residuals": frac(decode_res),
                    "raster_resize_frac": frac((raster_line or {}).get("resize")),
                    "ms": None if not decode else round(decode["ms"], 4)},

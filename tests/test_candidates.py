@@ -60,7 +60,7 @@ def test_kind_restricted_pools_are_the_filtered_full_pools(golden):
 
 def test_bench_restricted_pools_match_filtered_full_pools():
     """The bench's directly generated constant + linear pools (worker processes) equal the full
-    pools filtered to those kinds."""
+    pools filtered to those kinds, under the same float32 arctan2 rule."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
 
@@ -72,8 +72,24 @@ def test_bench_restricted_pools_match_filtered_full_pools():
     img = srgb_u8_to_linear(u8)
     tiles = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
     patches = quadtree.extract_tiles(img, tiles, 64)
-    pools = [bench._pool_cands((p, 75)) for p in patches]
+    pools = [bench._pool_cands((p, 75, None, "rounded")) for p in patches]
     with ProcessPoolExecutor(max_workers=2, mp_context=mp.get_context("spawn")) as ex:
-        got, gen_s, same = bench.restricted_pools(patches, pools, (0, 1), ex)
-    assert same and gen_s > 0 and len(got) == len(patches)
-    assert all(set(np.unique(g["kind"])) <= {0, 1} for g in got)
+        got, gen_s = bench.restricted_pools(patches, (0, 1), ex)
+    assert gen_s > 0 and len(got) == len(patches)
+    for g, f in zip(got, pools):
+        assert np.array_equal(g.view(np.uint8), f[np.isin(f["kind"], (0, 1))].view(np.uint8))
+
+
+def test_arctan2_rule_only_moves_the_edge_pool_orientations():
+    """The two float32 arctan2 rules give pools that differ only in the edge pool's linear
+    splits (their orientation is the only value the Sobel angle decides)."""
+    from weft_b200 import quadtree
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 128, 25, 9)
+    img = srgb_u8_to_linear(u8)
+    tiles = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    for p in quadtree.extract_tiles(img, tiles, 64)[::5]:
+        a = candidates.tile_candidates(p, 75, atan2="numpy")
+        b = candidates.tile_candidates(p, 75, atan2="rounded")
+        assert [c for c in a if c.kind != 1] == [c for c in b if c.kind != 1]

@@ -115,6 +115,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_raster_resize": [_P, _I, _I, _P, _I, _I, _P, _P],
     "weftk_quantize_rows": [_P, _P, _I, _P, _P],
     "weftk_fit_selected_rows": [_P, _P, _P, _P],
+    "weftk_gen_pools": [_P, _P, _P],
 }
 
 _lock = threading.Lock()

@@ -135,9 +135,15 @@ def dedup(cands: list[Cand]) -> list[Cand]:
 
 
 # ----------------------------------------------------------------------------- edge-driven pool
-def sobel(tile: np.ndarray):
+def sobel(tile: np.ndarray, atan2: str = "numpy"):
     """3x3 Sobel magnitude and orientation in [0, pi) with zero borders
-    (``_sobel_edges``, src/weft/edge_analysis.py:17-41)."""
+    (``_sobel_edges``, src/weft/edge_analysis.py:17-41).  The reference's convolution reads
+    ``lum[y-1, x-1]`` for every tap (its slices are offset), so interior gradients cancel to
+    rounding residue and the values are small integer multiples of one luminance; their angles
+    sit on the orientation histogram's bin edges, where the last bit of the float32 arctan2
+    decides the bin.  ``atan2="numpy"`` uses numpy's float32 arctan2 (the reference; its last
+    bit depends on the host CPU's SIMD path), ``"rounded"`` the float64 arctan2 rounded to
+    float32, which does not (the device generator's rule)."""
     lum = luminance(tile)
     h, w = lum.shape
     kx = np.array([[-1, 0, 1], [-2, 0, 2], [-1, 0, 1]], dtype=np.float32)
@@ -152,7 +158,11 @@ def sobel(tile: np.ndarray):
             sh, sw = min(src.shape[0], dst.shape[0]), min(src.shape[1], dst.shape[1])
             gx[ty:ty + sh, tx:tx + sw] += kx[dy, dx] * src[:sh, :sw]
             gy[ty:ty + sh, tx:tx + sw] += ky[dy, dx] * src[:sh, :sw]
-    return np.sqrt(gx * gx + gy * gy), np.arctan2(gy, gx) % np.pi, lum
+    if atan2 == "rounded":
+        ang = np.arctan2(gy.astype(np.float64), gx.astype(np.float64)).astype(np.float32)
+    else:
+        ang = np.arctan2(gy, gx)
+    return np.sqrt(gx * gx + gy * gy), ang % np.pi, lum
 
 
 def dominant_orientations(angle: np.ndarray, mag: np.ndarray, n_bins: int = 12) -> list[float]:
@@ -230,17 +240,17 @@ def _kmeans3_triangles(tile, pixels, wf, hf, alphas, clamp_geom):
     return out
 
 
-def edge_candidates(tile: np.ndarray, quality: int = 75, kinds=None) -> list[Cand]:
+def edge_candidates(tile: np.ndarray, quality: int = 75, kinds=None, atan2: str = "numpy") -> list[Cand]:
     """The edge-driven pool; ``kinds`` (a set) skips the generators of other kinds, which leaves the
-    remaining candidates, their values and their order unchanged."""
-    return dedup(_edge_raw(tile, quality, kinds))
+    remaining candidates, their values and their order unchanged; ``atan2`` as for ``sobel``."""
+    return dedup(_edge_raw(tile, quality, kinds, atan2))
 
 
-def _edge_raw(tile: np.ndarray, quality: int, kinds) -> list[Cand]:
+def _edge_raw(tile: np.ndarray, quality: int, kinds, atan2: str = "numpy") -> list[Cand]:
     want = (lambda k: True) if kinds is None else (lambda k: k in kinds)
     h, w = tile.shape[:2]
     hf, wf = float(h - 1), float(w - 1)
-    mag, angle, _ = sobel(tile)
+    mag, angle, _ = sobel(tile, atan2)
     pixels = tile.reshape(-1, 3).astype(np.float32)
     avg = clamp_rgb(tile.mean(axis=(0, 1)))
     out: list[Cand] = []
@@ -418,14 +428,15 @@ def _template_raw(tile: np.ndarray, quality: int, kinds) -> list[Cand]:
     return out if kinds is None else [c for c in out if c.kind in kinds]
 
 
-def tile_candidates(tile: np.ndarray, quality: int = 75, kinds=None) -> list[Cand]:
+def tile_candidates(tile: np.ndarray, quality: int = 75, kinds=None, atan2: str = "numpy") -> list[Cand]:
     """The tile's initial pool: edge-driven then template candidates, de-duplicated.  With ``kinds``
     only those kinds are generated: the result is the full pool filtered to them, in pool order
-    (the de-duplication key starts with the kind, so other kinds never shadow a candidate)."""
+    (the de-duplication key starts with the kind, so other kinds never shadow a candidate).
+    ``atan2`` chooses the float32 arctan2 of the Sobel orientations (see ``sobel``)."""
     kinds = None if kinds is None else frozenset(int(k) for k in kinds)
     # one de-duplication of the concatenation keeps the same first occurrences as de-duplicating
     # each pool first
-    return dedup(_edge_raw(tile, quality, kinds) + _template_raw(tile, quality, kinds))
+    return dedup(_edge_raw(tile, quality, kinds, atan2) + _template_raw(tile, quality, kinds))
 
 
 # ----------------------------------------------------------------------------- re-seeding

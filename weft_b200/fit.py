@@ -122,7 +122,35 @@ class BatchedFit:
         self.patches = None
         return self
 
-    def _setup(self, pixels, sizes, records, counts, quality, caps, device, reserve) -> None:
+    @classmethod
+    def from_device_pools(cls, src4: torch.Tensor, sizes, cand: torch.Tensor, counts: torch.Tensor, stride: int,
+                          quality: int = 75, caps=None, kinds_mask: int = 0b11) -> "BatchedFit":
+        """Tiles and pools already resident on the device, e.g. made by ``pools.generate_pools``:
+        ``src4`` float4 pixels (tile-major), ``sizes`` tile sides (host), ``cand`` the 60-byte
+        records of ``len(sizes) * stride`` slots (tile t owns slots [t * stride, (t + 1) * stride)),
+        ``counts`` the filled slots per tile (device int32; read only on the device), and
+        ``kinds_mask`` the primitive kinds the pools may hold (bit k for kind k).  Nothing here reads
+        the pools' contents, so they may be (re)generated after construction, e.g. inside the same
+        captured graph as the fit; the scoring work depends on the layout only.  No host copy of the
+        pools exists, so re-seeding runs on the device only."""
+        self = cls.__new__(cls)
+        sizes = np.asarray(sizes, np.int32)
+        n = len(sizes)
+        self._layout(sizes, np.full(n, int(stride), np.int64), quality, caps, src4.device.index or 0)
+        if src4.shape != (int((sizes.astype(np.int64) ** 2).sum()), 4) or cand.numel() != self.n_slots * PRIM_DTYPE.itemsize:
+            raise ValueError("pixels or candidate slots do not match the tile layout")
+        d = self.device
+        self.pool_cnt = self.init_cnt = None
+        self._init_kinds = self.kinds = None
+        self._kinds_mask = int(kinds_mask)
+        t_init_cnt = counts.to(device=d, dtype=torch.int32).contiguous()
+        self._finish(src4, cand, t_init_cnt.clone(), t_init_cnt, None)
+        self.pools = None
+        self.patches = None
+        return self
+
+    def _layout(self, sizes, pool_cap, quality, caps, device) -> None:
+        """Tile and slot layout (host): sizes, caps, pixel offsets, slot offsets."""
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
         self.quality = int(quality)
@@ -136,35 +164,57 @@ class BatchedFit:
         self.caps = np.array(caps if caps is not None else [MAX_PRIMS_BY_SIZE.get(int(s), 48) for s in self.sizes],
                              np.int32)
         self.cap_max = int(self.caps.max()) if n else 1
-        cnt = counts.astype(np.int64)
-        self.pool_cap = cnt + reserve
+        self.pool_cap = np.asarray(pool_cap, np.int64)
         self.pool_off = np.zeros(n, np.int64)
         if n > 1:
             np.cumsum(self.pool_cap[:-1], out=self.pool_off[1:])
         self.n_slots = int(self.pool_cap.sum()) if n else 0
         if self.n_slots >= 2 ** 31:
             raise ValueError("too many candidate slots")
-        self.pool_cnt = cnt.astype(np.int32)
-        self.init_cnt = self.pool_cnt.copy()
         px = self.sizes.astype(np.int64) ** 2
         self.px_off = np.zeros(n, np.int64)
         if n > 1:
             np.cumsum(px[:-1], out=self.px_off[1:])
-        n_px = int(px.sum())
-        if pixels.shape != (n_px, 3):
-            raise ValueError(f"pixels must be ({n_px}, 3)")
+        self.n_px = int(px.sum())
+
+    def _setup(self, pixels, sizes, records, counts, quality, caps, device, reserve) -> None:
+        cnt = counts.astype(np.int64)
+        self._layout(sizes, cnt + reserve, quality, caps, device)
+        self.pool_cnt = cnt.astype(np.int32)
+        self.init_cnt = self.pool_cnt.copy()
+        if pixels.shape != (self.n_px, 3):
+            raise ValueError(f"pixels must be ({self.n_px}, 3)")
         if len(records) != int(cnt.sum()):
             raise ValueError("records and counts disagree")
-
         d = self.device
-        self.t_src = torch.zeros((n_px, 4), dtype=torch.float32, device=d)
-        self.t_src[:, :3] = _dev(pixels, d)
-        self.t_bg = torch.zeros((n_px, 4), dtype=torch.float32, device=d)
+        t_src = torch.zeros((self.n_px, 4), dtype=torch.float32, device=d)
+        t_src[:, :3] = _dev(pixels, d)
+        self.kinds, slots = slot_layout(records, cnt, self.pool_off, self.n_slots)
+        rec_bytes = np.ascontiguousarray(records).view(np.uint8).reshape(-1, PRIM_DTYPE.itemsize)
+        if slots is None:
+            t_cand = _dev(rec_bytes, d).view(-1) if len(records) else torch.zeros(0, dtype=torch.uint8, device=d)
+        else:
+            t_cand = torch.zeros((self.n_slots, PRIM_DTYPE.itemsize), dtype=torch.uint8, device=d)
+            if len(records):
+                t_cand[_dev(slots, d)] = _dev(rec_bytes, d)
+            t_cand = t_cand.view(-1)
+        self._init_kinds = self.kinds.copy()
+        self._finish(t_src, t_cand, _dev(self.pool_cnt, d), _dev(self.init_cnt, d), _dev(self._init_kinds, d))
+
+    def _finish(self, t_src, t_cand, t_pool_cnt, t_init_cnt, t_init_kinds) -> None:
+        """Device state of the fit around the given pixels, records, counts and slot kinds."""
+        d = self.device
+        n = self.n
+        self.t_src = t_src
+        self.t_cand = t_cand
+        self.t_pool_cnt = t_pool_cnt
+        self.t_init_cnt = t_init_cnt
+        self.t_init_kinds = t_init_kinds
+        self.t_bg = torch.zeros((self.n_px, 4), dtype=torch.float32, device=d)
         self.t_px_off = _dev(self.px_off.astype(np.int32), d)
         self.t_size = _dev(self.sizes, d)
         self.t_cap = _dev(self.caps, d)
         self.t_pool_off = _dev(self.pool_off.astype(np.int32), d)
-        self.t_pool_cnt = _dev(self.pool_cnt, d)
         self.t_pool_cap = _dev(self.pool_cap.astype(np.int32), d)
         self.t_n_alive = torch.zeros(n, dtype=torch.int32, device=d)
         self.t_n_sel = torch.zeros(n, dtype=torch.int32, device=d)
@@ -172,23 +222,13 @@ class BatchedFit:
         self.t_flags = torch.zeros(n, dtype=torch.int32, device=d)
         self.t_cur_obj = torch.zeros(n, dtype=torch.float64, device=d)
         self.t_sel = torch.full((n * self.cap_max,), -1, dtype=torch.int32, device=d)
-        self.kinds, slots = slot_layout(records, cnt, self.pool_off, self.n_slots)
-        rec_bytes = np.ascontiguousarray(records).view(np.uint8).reshape(-1, PRIM_DTYPE.itemsize)
-        if slots is None:
-            self.t_cand = _dev(rec_bytes, d).view(-1) if len(records) else \
-                torch.zeros(0, dtype=torch.uint8, device=d)
-        else:
-            self.t_cand = torch.zeros((self.n_slots, PRIM_DTYPE.itemsize), dtype=torch.uint8, device=d)
-            if len(records):
-                self.t_cand[_dev(slots, d)] = _dev(rec_bytes, d)
-            self.t_cand = self.t_cand.view(-1)
-        self._init_kinds = self.kinds.copy()
         self.t_prep = torch.empty(self.n_slots * 16, dtype=torch.float32, device=d)
         self.t_alive = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
         self.t_kind = torch.zeros(self.n_slots, dtype=torch.uint8, device=d)
         self.t_partial = torch.empty(self.n_slots * 4, dtype=torch.float32, device=d)
         self.t_status = torch.zeros(4, dtype=torch.int32, device=d)
         self.t_work = torch.zeros(2, dtype=torch.int64, device=d)
+        self.t_zero_first = torch.zeros(n, dtype=torch.int32, device=d)
         self.h_status = torch.zeros(4, dtype=torch.int32).pin_memory()
         self.st = _lib.WeftFitState(
             n, self.cap_max, self.n_slots,
@@ -201,7 +241,8 @@ class BatchedFit:
         self.n_items = {}
         self.chunk = dict(CHUNK)  # candidates per scoring CTA, per size class (set by autotune)
         self.tuning = None
-        self._prepare(np.zeros(n, np.int32))
+        _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), self._stream()),
+                   "weftk_fit_prepare")
         self._build_work()
 
     # ------------------------------------------------------------------ plumbing
@@ -221,13 +262,17 @@ class BatchedFit:
         holds candidates of similar cost; re-seeded slots are scored in slot
         order.  Items cover the reserved slots too; the kernel only scores the
         filled ones, so re-seeding needs no new items.  Sorting runs on the GPU.
+        Over device pools the layout alone decides (``_build_static_work``).
         """
+        if self._init_kinds is None:
+            self._build_static_work()
+            return
         d = self.device
         n = self.n
         cap = torch.from_numpy(self.pool_cap).to(d)
-        cnt = torch.from_numpy(self.init_cnt.astype(np.int64)).to(d)
+        cnt = self.t_init_cnt.to(torch.int64)
         off = torch.from_numpy(self.pool_off).to(d)
-        kinds = torch.from_numpy(self._init_kinds).to(d).to(torch.int64)
+        kinds = self.t_init_kinds.to(torch.int64)
         tile_of = torch.repeat_interleave(torch.arange(n, device=d), cap)
         local = torch.arange(self.n_slots, device=d) - torch.repeat_interleave(off, cap)
         filled = local < cnt[tile_of]
@@ -268,6 +313,37 @@ class BatchedFit:
             self.n_items[cls] = int(rows.shape[0])
         self.t_items = items
 
+    def _build_static_work(self) -> None:
+        """Work that depends on the tile layout only, not on the pools' contents (which live on
+        the device and may be regenerated inside a captured graph): identity scoring order, and
+        per size class every tile's slot range cut into runs of ``chunk`` candidates x 1024-pixel
+        blocks, largest tiles first.  Runs past a tile's filled slots end at once."""
+        d = self.device
+        cap = self.pool_cap.astype(np.int64)
+        local = np.arange(self.n_slots, dtype=np.int64) - np.repeat(self.pool_off, cap)
+        self.t_perm = torch.from_numpy(local.astype(np.int32)).to(d)
+        items = {}
+        for cls, members in ((8, (8,)), (16, (16,)), (32, (32, 64))):
+            chunk = self.chunk[cls]
+            ts_idx = np.nonzero(np.isin(self.sizes, members))[0]
+            if ts_idx.size == 0:
+                items[cls] = None
+                self.n_items[cls] = 0
+                continue
+            ts_idx = ts_idx[np.argsort(-self.sizes[ts_idx].astype(np.int64), kind="stable")]
+            nch = (cap[ts_idx] + chunk - 1) // chunk
+            blocks = np.maximum(1, self.sizes[ts_idx].astype(np.int64) ** 2 // 1024)
+            per_tile = nch * blocks
+            t_rep = np.repeat(ts_idx, per_tile)
+            j = np.arange(int(per_tile.sum())) - np.repeat(np.cumsum(per_tile) - per_tile, per_tile)
+            b_rep = np.repeat(blocks, per_tile)
+            first = (j // b_rep) * chunk
+            cnt = np.minimum(chunk, cap[t_rep] - first)
+            arr = np.stack([t_rep, j % b_rep, first, cnt], 1).astype(np.int32)
+            items[cls] = torch.from_numpy(arr).to(d)
+            self.n_items[cls] = len(arr)
+        self.t_items = items
+
     def _round(self, mode: int) -> tuple[int, int]:
         ti = self.t_items
         n8, n16, n32 = (self.n_items[k] for k in (8, 16, 32))
@@ -284,6 +360,8 @@ class BatchedFit:
 
     # ------------------------------------------------------------------ re-seed
     def _reseed(self, reseed, reseed_batch=None) -> None:
+        if self.init_cnt is None:
+            raise ValueError("a fit over device pools re-seeds on the device only")
         t0 = time.perf_counter()
         flags = self.t_flags.cpu().numpy()
         n_sel = self.t_n_sel.cpu().numpy()
@@ -340,14 +418,15 @@ class BatchedFit:
 
     def reset(self) -> None:
         """Forget the fit (selections, re-seeds) but keep pixels and initial pools resident."""
-        self.pool_cnt[:] = self.init_cnt
+        if self.init_cnt is not None:
+            self.pool_cnt[:] = self.init_cnt
         self.device_reseeded = False
         for t in range(self.n if self.pools is not None else 0):
             p = self.pools[t]
             if not isinstance(p, np.ndarray) and len(p) > self.init_cnt[t]:
                 del p[self.init_cnt[t]:]
-        self.kinds[:] = self._init_kinds
-        self._device_consts()
+        if self._init_kinds is not None:
+            self.kinds[:] = self._init_kinds
         self._moments()
         _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), self._stream()),
                    "weftk_fit_reset")
@@ -357,16 +436,10 @@ class BatchedFit:
         self.device_reseeded = False
 
     # -------------------------------------------------------------- graph-capturable init-only fit
-    def _device_consts(self) -> None:
-        if not hasattr(self, "t_init_cnt"):
-            self.t_init_cnt = _dev(self.init_cnt, self.device)
-            self.t_zero_first = torch.zeros(self.n, dtype=torch.int32, device=self.device)
-
     def run_init_only(self) -> None:
         """Reset and run only the init round (best single candidate per tile), launching
         device work only: no host copies or syncs, so it can be captured in a CUDA graph.
         With the closed-form init on, the per-tile moments are computed first."""
-        self._device_consts()
         s = self._stream()
         self._moments()
         _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), s), "weftk_fit_reset")
@@ -413,7 +486,6 @@ class BatchedFit:
         synchronisation (``weftk_fit_run``), so it can be captured in a CUDA graph, and snap the
         selected stacks to the wire grid (``quantize_selected``).  Same decisions as ``run()``
         with device re-seeding; ``control()`` reads the outcome."""
-        self._device_consts()
         if not hasattr(self, "t_ctl"):
             self.t_ctl = torch.zeros(4, dtype=torch.int32, device=self.device)
         s = self._stream()
@@ -455,11 +527,19 @@ class BatchedFit:
 
     def init_kinds(self) -> np.ndarray:
         """Primitive kind of every filled slot of the initial pools (host copy)."""
-        return self._init_kinds[self._init_kinds < 7].astype(np.int32)
+        if self._init_kinds is None:
+            cnt = self.t_init_cnt.cpu().numpy().astype(np.int64)
+            rec = self.t_cand.view(torch.int32).view(-1, PRIM_DTYPE.itemsize // 4)[:, 0].cpu().numpy()
+            filled = (np.arange(self.n_slots) - np.repeat(self.pool_off, self.pool_cap)) < np.repeat(cnt, self.pool_cap)
+            return rec[filled].astype(np.int32)
+        k = self._init_kinds
+        return k[k < 7].astype(np.int32)
 
     def init_kinds_mask(self) -> int:
         """Bit k set when kind k (0..6) occurs in the initial pools: ``kinds_mask_of(init_kinds())``
-        from one count over the slot kinds."""
+        from one count over the slot kinds (device pools: the mask they were declared with)."""
+        if self._init_kinds is None:
+            return self._kinds_mask
         k = self._init_kinds
         if k.size == 0:
             return 0

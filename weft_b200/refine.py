@@ -317,11 +317,14 @@ class RefinedFit:
     torch's current stream."""
 
     def __init__(self, fit, steps: int = 20, lr: float = 1e-2, use_graph: bool = True, residual: bool = False,
-                 closed_form_init: bool = True):
+                 closed_form_init: bool = True, prelude=None):
+        """``prelude`` (optional): a callable that enqueues device work to run first in every run
+        (inside the graph), e.g. the generation of the fit's candidate pools."""
         self.fit = fit
+        self.prelude = prelude
         fit.use_closed_form_init(closed_form_init)
         dev = fit.device
-        has = fit.init_cnt > 0
+        has = fit.init_cnt > 0 if fit.init_cnt is not None else np.ones(fit.n, bool)
         self.rows = torch.from_numpy(np.nonzero(has)[0]).to(dev)
         self.rows32 = self.rows.to(torch.int32)
         prim_off = np.concatenate([[0], np.cumsum(has.astype(np.int64))])
@@ -339,6 +342,8 @@ class RefinedFit:
 
     def _body(self) -> None:
         f = self.fit
+        if self.prelude is not None:
+            self.prelude()
         f.run_init_only()
         fr = self.refiner
         _lib.check(self.ss.lib.weftk_refine_start(ctypes_addr(f.st), _lib.ptr(self.rows32), int(self.rows32.numel()),

@@ -789,17 +789,25 @@ def image_batch_fit(args, executor, local, stream):
     _, plain_ms = timed(plain_step)
     ss, p = fit.stack_set()
     plain_rd = batch.rd_per_image(ss.to_stacks(ss.quantize(p)))
-    rf = batch.refined_fit(steps=args.refine_steps, lr=args.refine_lr)
-    rf.run()
-    rows, ref_ms = timed(rf.run, 3)
-    ref_rd = batch.rd_per_image(rf.ss.to_stacks(rf.ss.quantize(rows)))
+    del fit, ss, p
+    drf = batch.refined_fit_device(steps=args.batch_steps, lr=args.refine_lr)
+    drf.run()
+    rows, ref_ms = timed(drf.run, 3)
+    rss = drf.rf.ss
+    ref_rd = batch.rd_per_image(rss.to_stacks(rss.quantize(drf.rf.refiner.p)))
+    init_rd = batch.rd_per_image(rss.to_stacks(rss.quantize(drf.rf.start)))
     deltas = [b["rd_score"] - a["rd_score"] for a, b in zip(plain_rd, ref_rd)]
+    adam = [b["rd_score"] - a["rd_score"] for a, b in zip(init_rd, ref_rd)]
+    per_image = [{"side": im.size[0], "plain_rd": a["rd_score"], "refined_rd": b["rd_score"]}
+                 for im, a, b in zip(ims, plain_rd, ref_rd)]
     return {"images": args.batch_images, "n_images": len(ims), "mpix": n_px / 1e6, "tiles": int(batch.tile_off[-1]),
             "cand_gen_s": cand_s, "plain_ms": plain_ms, "plain_mpix_per_s": n_px / (plain_ms * 1e-3) / 1e6,
             "refined_ms": ref_ms, "refined_mpix_per_s": n_px / (ref_ms * 1e-3) / 1e6,
-            "refined": f"{args.refine_pool} init round + {args.refine_steps} fused Adam steps, one CUDA graph",
+            "refined": f"pools generated on the device (constant + linear), init round + {args.batch_steps} fused "
+                       f"Adam steps + wire-grid snap, one CUDA graph over every tile of every image",
             "rd_delta_db_min": min(deltas), "rd_delta_db_mean": float(np.mean(deltas)),
-            "images_within_0.05db": int(sum(d >= -0.05 for d in deltas))}
+            "images_within_0.05db": int(sum(d >= -0.05 for d in deltas)),
+            "adam_steps_db_mean": float(np.mean(adam)), "per_image": per_image}
 
 
 def _hbm_peak() -> tuple[float, str]:
@@ -903,6 +911,7 @@ def main():
                     help="Adam steps of the 2048^2 differentiable fit (0: skip that workload)")
     ap.add_argument("--batch-images", default="",
                     help='multi-image batch, e.g. "16x256,16x512,16x1024,16x2048" (empty: skip)')
+    ap.add_argument("--batch-steps", type=int, default=100, help="Adam steps of the multi-image refined fit")
     args = ap.parse_args()
 
     # Process pools first: spawned before any CUDA initialisation.

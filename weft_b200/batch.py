@@ -36,15 +36,19 @@ def _cands(args):
     return pack_cands(candidates.tile_candidates(patch, q))
 
 
-def prepare_image(u8: np.ndarray, quality: int = 75, executor=None, threshold: float = 100.0) -> ImageTiles:
+def prepare_image(u8: np.ndarray, quality: int = 75, executor=None, threshold: float = 100.0,
+                  pools: bool = True) -> ImageTiles:
     """Quadtree (8-64 px, split while u8 luminance variance > ``threshold``), tiles and the
-    reference's candidate pools (host; ``executor`` maps over tiles when given)."""
+    reference's candidate pools (host; ``executor`` maps over tiles when given; ``pools=False``
+    skips them, for fits whose pools are generated on the device)."""
     img = srgb_u8_to_linear(u8)
     tiles = quadtree.decompose(img, rule="variance", threshold=threshold, min_tile=8, max_tile=64, image_u8=u8)
     patches = quadtree.extract_tiles(img, tiles, 64)
-    jobs = [(p, quality) for p in patches]
-    pools = list(executor.map(_cands, jobs, chunksize=32)) if executor is not None else [_cands(j) for j in jobs]
-    return ImageTiles(img, tiles, patches, pools)
+    recs = None
+    if pools:
+        jobs = [(p, quality) for p in patches]
+        recs = list(executor.map(_cands, jobs, chunksize=32)) if executor is not None else [_cands(j) for j in jobs]
+    return ImageTiles(img, tiles, patches, recs)
 
 
 class ImageBatch:
@@ -58,7 +62,7 @@ class ImageBatch:
         counts = [len(im.tiles) for im in images]
         self.tile_off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         self.patches = [p for im in images for p in im.patches]
-        self.pools = [p for im in images for p in im.pools]
+        self.pools = [p for im in images for p in im.pools] if all(im.pools is not None for im in images) else None
 
     @property
     def n_pixels(self) -> int:
@@ -93,6 +97,26 @@ class ImageBatch:
         if autotune:
             fit.autotune()
         return RefinedFit(fit, steps=steps, lr=lr, use_graph=use_graph, residual=residual)
+
+    def refined_fit_device(self, steps: int = 100, lr: float = 1e-2, autotune: bool = True, use_graph: bool = True):
+        """The refined fit with its constant + linear pools generated on the device for every tile of
+        every image (``pools.DeviceRefinedFit``): generation, init round, ``steps`` Adam steps and the
+        wire-grid snap in one CUDA graph; only the tile pixels go to the device."""
+        import torch
+
+        from .pools import DeviceRefinedFit
+
+        pixels, sizes = self.tile_pixels()
+        dev = torch.device("cuda", self.device)
+        src4 = torch.zeros((len(pixels), 4), dtype=torch.float32, device=dev)
+        src4[:, :3] = torch.from_numpy(pixels).to(dev)
+        return DeviceRefinedFit(src4, sizes, self.quality, caps=[self.cap] * len(sizes), steps=steps, lr=lr,
+                                use_graph=use_graph, autotune=autotune)
+
+    def tile_pixels(self):
+        """Tile pixels of the whole batch, tile-major (float32 (n, 3)), and the tile sides."""
+        pixels = np.concatenate([p.reshape(-1, 3) for p in self.patches])
+        return pixels, np.array([p.shape[0] for p in self.patches], np.int32)
 
     def image_stacks(self, stacks: list) -> list[list]:
         """Split per-tile stacks of the whole batch into per-image lists."""

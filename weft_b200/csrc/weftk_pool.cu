@@ -151,6 +151,13 @@ __device__ void add_cand(Scratch& S, int kind, const double* g, const float* c0,
     S.n_cand = i + 1;
 }
 
+// Dynamic shared memory of one tile of N pixels: seven float planes (r, g, b, luminance, the
+// np.gradient magnitude, the Sobel magnitude, a sort key), the sorted pixel indices, the bins.
+constexpr size_t POOL_FLOAT_PLANES = 7;
+__host__ __device__ constexpr size_t pool_smem_bytes(int n) {
+    return (size_t)n * (POOL_FLOAT_PLANES * sizeof(float) + sizeof(int) + sizeof(uint8_t));
+}
+
 template <int TS, int NT>
 __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoolJob job, int si, int quality) {
     constexpr int N = TS * TS;
@@ -163,6 +170,7 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     float* skey = mags + N;                           // [N] bin-sorted magnitudes, then sorted lum
     int* sidx = reinterpret_cast<int*>(skey + N);     // [N] pixel of each sorted luminance
     uint8_t* bin = reinterpret_cast<uint8_t*>(sidx + N);  // [N]
+    static_assert(POOL_FLOAT_PLANES == 7, "the planes above are col[3], lum, magt, mags, skey");
     __shared__ Scratch S;
     (void)quality;
 
@@ -585,8 +593,7 @@ int launch_gen(const WeftPoolTables& tb, const WeftPoolJob& job, int si, cudaStr
     const int n = job.n_tiles[si];
     if (n == 0) return WEFTK_OK;
     constexpr int N = TS * TS;
-    const size_t smem = (size_t)N * (6 * sizeof(float) + sizeof(int) + 1);
-    const size_t dyn = (smem + 15) / 16 * 16;
+    const size_t dyn = (pool_smem_bytes(N) + 15) / 16 * 16;
     // the static scratch and the pixel planes together exceed the default 48 KB: opt in once
     // per device (under a lock, so concurrent first calls agree)
     {

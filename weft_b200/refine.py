@@ -53,10 +53,11 @@ class StackSet:
     """Per-tile stacks over tile pixels resident on the GPU."""
 
     def __init__(self, src: torch.Tensor, px_off: torch.Tensor, sizes: torch.Tensor, prim_off: np.ndarray,
-                 kinds, device: int = 0, kinds_mask: int | None = None):
+                 kinds, device: int = 0, kinds_mask: int | None = None, sizes_host: np.ndarray | None = None):
         """``kinds``: per-row primitive kinds, a numpy array or a device int32 tensor (kept by reference).
         ``kinds_mask`` (bit k = kind k may occur) is derived from a numpy ``kinds``; pass it with a
-        device tensor whose contents change later."""
+        device tensor whose contents change later.  ``sizes_host``: the tile sides on the host, when
+        the caller has them (saves reading ``sizes`` back)."""
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
         self.n = int(sizes.numel())
@@ -76,7 +77,7 @@ class StackSet:
                 kinds_mask = kinds_mask_of(self.kinds_np)
         self.t_prim_off = torch.from_numpy(self.prim_off_np.astype(np.int32)).to(self.device)
         # work split by tile side (largest first): > 32 px eight warps, 17-32 four, 9-16 two, <= 8 one
-        sz = sizes.cpu().numpy()
+        sz = np.asarray(sizes_host) if sizes_host is not None else sizes.cpu().numpy()
         classes = [sz > 32, (sz > 16) & (sz <= 32), (sz > 8) & (sz <= 16), sz <= 8]
         order = np.concatenate([np.nonzero(c)[0] for c in classes]).astype(np.int32)
         self.t_order = torch.from_numpy(order).to(self.device)
@@ -85,7 +86,8 @@ class StackSet:
                                     _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind), _lib.ptr(self.t_order),
                                     n_big, n_mid, n_s16, int(kinds_mask or 0))
         n_px = (sizes.to(torch.int64) ** 2)
-        self.weights = (n_px.to(torch.float32) / float(n_px.sum().item())) if self.n else n_px.float()
+        total = float((sz.astype(np.int64) ** 2).sum())
+        self.weights = (n_px.to(torch.float32) / total) if self.n else n_px.float()
 
     @classmethod
     def from_fit(cls, fit) -> tuple["StackSet", torch.Tensor]:
@@ -331,7 +333,8 @@ class RefinedFit:
         n_rows = int(has.sum())
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
         mask = fit.init_kinds_mask()
-        self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask)
+        self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask,
+                           sizes_host=fit.sizes)
         self.refiner = FusedRefiner(self.ss, torch.zeros((n_rows, 16), dtype=torch.float32, device=dev), lr=lr,
                                     residual=residual)
         self.steps = int(steps)

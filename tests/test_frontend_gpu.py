@@ -1,0 +1,49 @@
+"""The fit's front end on the device against the host restatement of the reference's: the
+variance-rule quadtree (the same tiles in the same order), tile extraction with the sRGB decode
+(bit-equal pixels, edge padding included), and the whole refined fit from the u8 image."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("w,h,n,seed", [(256, 256, 40, 0), (200, 130, 25, 3), (1024, 1024, 600, 0), (72, 264, 9, 5)])
+def test_device_quadtree_and_extraction_equal_host(w, h, n, seed):
+    from weft_b200 import frontend, quadtree
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(w, h, n, seed)
+    img = srgb_u8_to_linear(u8)
+    want = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    dimg = torch.from_numpy(u8).to("cuda:0")
+    tiles, count = frontend.decompose_device(dimg, 100.0)
+    got = tiles.cpu().numpy()
+    assert count == len(want)
+    assert [tuple(int(v) for v in r) for r in got] == [(t.x, t.y, t.size) for t in want]
+    sizes = got[:, 2].copy()
+    src4, _ = frontend.extract_device(dimg, tiles, sizes)
+    host = np.concatenate([p.reshape(-1, 3) for p in quadtree.extract_tiles(img, want, 64)])
+    np.testing.assert_array_equal(src4[:, :3].cpu().numpy(), host)
+    assert float(src4[:, 3].abs().max()) == 0.0
+
+
+def test_refine_image_equals_the_fit_over_host_tiles():
+    from weft_b200 import frontend, quadtree
+    from weft_b200.pools import refine_tiles
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(192, 160, 20, 7)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    sizes = np.array([p.shape[0] for p in patches], np.int32)
+    rows_h, kinds_h = refine_tiles(np.concatenate([p.reshape(-1, 3) for p in patches]), sizes, 75,
+                                   caps=[16] * len(sizes), steps=5)
+    tiles, rows, kinds = frontend.refine_image(u8, 75, 16, steps=5)
+    assert [tuple(r) for r in tiles.tolist()] == [(t.x, t.y, t.size) for t in qts]
+    np.testing.assert_array_equal(rows, rows_h)
+    np.testing.assert_array_equal(kinds, kinds_h)

@@ -260,7 +260,7 @@ __device__ void layer_grad(const Layers& s, int k, float px, float py, bool soft
 // Byte offsets for L staged layers; every region starts on a 16-byte boundary
 // except the trailing doubles (8-byte aligned).
 struct GroupLayout {
-    int prep, seg, raw, madam, vadam, msum, quad, hnode, hist, gacc, lacc, lred, bytes;
+    int prep, seg, raw, madam, vadam, msum, quad, hnode, hist, gacc, lacc, lred, mom, bytes;
 };
 
 // Stacks of at most this many layers accumulate gradients per lane (one slot per
@@ -282,7 +282,8 @@ __host__ __device__ __forceinline__ GroupLayout group_layout(int L, int wpt, boo
     g.gacc = g.hist + wpt * L * 384;
     g.lacc = (g.gacc + wpt * L * 56 + 15) & ~15;
     g.lred = g.lacc + (L <= RF_LANE_ACC_MAX ? wpt * L * 14 * 32 * 4 : 0);
-    g.bytes = (g.lred + wpt * 8 + 15) & ~15;
+    g.mom = g.lred + wpt * 8;  // pixel moments of a lone constant layer's tile: per warp, then total
+    g.bytes = (g.mom + (wpt + 1) * 6 * 8 + 15) & ~15;
     return g;
 }
 
@@ -493,6 +494,7 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     float* gacc = gacc_all + (size_t)wig * L * 14;
     float* lacc = reinterpret_cast<float*>(base + lay.lacc) + (size_t)wig * L * 14 * 32;
     double* lred = reinterpret_cast<double*>(base + lay.lred);
+    double* mom = reinterpret_cast<double*>(base + lay.mom);
 
     const int ts = set.size[t];
     const int p0 = set.prim_off[t];
@@ -587,6 +589,57 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
             const float top = fmaf(c01 - c00, wx, c00), bot = fmaf(c11 - c10, wx, c10);
             v[ch] = fmaf(bot - top, wy, top);
         }
+    };
+
+    // A lone constant layer over black renders one colour q per channel (q = colour * alpha), so
+    // its loss and gradient follow from the tile's pixel sums S1 = sum src, S2 = sum src^2:
+    // sum over pixels of (q - src) = n q - S1, sum of (q - src)^2 = n q^2 - 2 q S1 + S2.  They are
+    // taken once per launch (float64, a fixed order: per lane, then per warp, then per group).
+    const bool cf = CL1 && !resid && K == 1 && set.kind[p0] == K_CONST;
+    if (cf) {
+        double m6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int q = gt; q < n; q += GT) {
+            const float4 v = src[q];
+            m6[0] += v.x;
+            m6[1] += v.y;
+            m6[2] += v.z;
+            m6[3] += (double)v.x * v.x;
+            m6[4] += (double)v.y * v.y;
+            m6[5] += (double)v.z * v.z;
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) m6[i] += __shfl_xor_sync(FULL, m6[i], o);
+        }
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < 6; ++i) mom[wig * 6 + i] = m6[i];
+        group_sync(wpt, grp);
+        if (gt < 6) {
+            double tot = 0.0;
+            for (int w = 0; w < wpt; ++w) tot += mom[w * 6 + gt];
+            mom[wpt * 6 + gt] = tot;
+        }
+    }
+    const double* S12 = mom + wpt * 6;
+    // loss (and, with gscale != 0, the colour / alpha gradient into g4) of the lone constant layer
+    auto const_closed = [&](float gscale, float* g4) -> double {
+        const Prep& P = prep[0];
+        const float sv[3] = {P.cr, P.cg, P.cb};
+        const double nd = (double)n;
+        double tot = 0.0, galpha = 0.0;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            const float c = __fmul_rn(sv[ch], P.a);  // blend over black: colour * alpha
+            const double cc = (double)clamp01(c);
+            tot += nd * cc * cc - 2.0 * cc * S12[ch] + S12[3 + ch];
+            const float G = (c >= 0.0f && c <= 1.0f) ? (float)((double)gscale * (nd * (double)c - S12[ch])) : 0.0f;
+            if (g4) g4[ch] = G * P.a;
+            galpha += (double)(G * sv[ch]);
+        }
+        if (g4) g4[3] = (raw[0][13] >= 0.0f && raw[0][13] <= 1.0f) ? (float)galpha : 0.0f;
+        return tot;
     };
 
     double sse = 0.0;
@@ -714,7 +767,15 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
         float acc[14];
 #pragma unroll
         for (int i = 0; i < 14; ++i) acc[i] = 0.0f;
-        for (int cidx = c_begin; CL1 && cidx < c_end; ++cidx) {
+        if (cf && gt == 0) {
+            float g4[4];
+            sse = const_closed(scale, g4);
+            gacc[7] = g4[0];
+            gacc[8] = g4[1];
+            gacc[9] = g4[2];
+            gacc[13] = g4[3];
+        }
+        for (int cidx = c_begin; CL1 && !cf && cidx < c_end; ++cidx) {
             // single constant/linear layer over black: everything in registers
             const int q = cidx * 32 + lane;
             const float4 v4 = vn;
@@ -745,7 +806,7 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
             for (int ch = 0; ch < 3; ++ch) g[ch] = (c[ch] >= 0.0f && c[ch] <= 1.0f) ? scale * e[ch] : 0.0f;
             grad_cl(prep[0], raw[0], v, px, py, g, acc);
         }
-        if (CL1 && K == 1) {
+        if (CL1 && K == 1 && !cf) {
             const unsigned cols = grad_columns(prep[0].kind);
 #pragma unroll
             for (int i = 0; i < 14; ++i) {
@@ -840,8 +901,9 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
             for (int k = gt; k < K; k += GT) madam[k * 16 + 15] += 1.0f;
         }
     } else if (!resid) {
-        float4 vn = c_begin < c_end ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        for (int cidx = c_begin; cidx < c_end; ++cidx) {
+        if (cf && gt == 0) sse = const_closed(0.0f, nullptr);
+        float4 vn = c_begin < c_end && !cf ? load_src(c_begin * 32 + lane) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int cidx = c_begin; !cf && cidx < c_end; ++cidx) {
             const int q = cidx * 32 + lane;
             const float4 v = vn;
             if (cidx + 1 < c_end) vn = load_src(q + 32);

@@ -88,6 +88,7 @@ def build_workload(size: int, n_prims: int, seed: int, executor):
     t0 = time.perf_counter()
     pools = list(executor.map(_pool_cands, [(p, QUALITY) for p in patches], chunksize=32))
     cand_s = time.perf_counter() - t0
+    build_workload.u8 = u8  # the sRGB image the end-to-end call starts from
     return img, tiles, patches, pools, cand_s
 
 
@@ -1100,8 +1101,17 @@ def run_weft(args, world, rank, local, executor, cores):
     init_rd = rd_of_params(dss, drf.rf.start, tiles, patches, img, args.size)
 
     pixels_h = pinned_copy(pixels, pin_keep)
+    u8_h = pinned_copy(build_workload.u8, pin_keep)
 
     def refined_e2e():
+        # the public call from the sRGB image: quadtree, tile extraction, pool generation, init
+        # round, Adam steps and the wire-grid snap on the GPU; tiles and snapped rows come back
+        from weft_b200.frontend import refine_image
+
+        qt, rows, kinds = refine_image(u8_h, QUALITY, CAP, steps=args.refine_steps, lr=args.refine_lr, device=local)
+        return int(u8_h.nbytes), int(qt.nbytes + rows.nbytes + kinds.nbytes + 4)
+
+    def tiles_e2e():
         from weft_b200.pools import refine_tiles
 
         rows, kinds = refine_tiles(pixels_h, sizes, QUALITY, caps=caps, steps=args.refine_steps, lr=args.refine_lr,
@@ -1109,6 +1119,7 @@ def run_weft(args, world, rank, local, executor, cores):
         return int(pixels.nbytes + sizes.nbytes), int(rows.nbytes + kinds.nbytes)
 
     ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
+    tiles_e2e_val, _ = timed_e2e(tiles_e2e)
 
     diff = differentiable_fit(args, executor, local, stream) if args.diff_steps > 0 and rank == 0 else None
     ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None
@@ -1185,7 +1196,9 @@ def run_weft(args, world, rank, local, executor, cores):
                            "roofline_gen": gen_roof, "roofline_init": init_roof, "roofline_refine": refine_roof,
                            "autotune": {str(k): {"variant": v[0], "cands_per_cta": v[1], "score_ms": v[2]}
                                         for k, v in (drf.fit.tuning or {}).items()},
-                           "pools_equal_host": [pools_equal, len(tiles)], "candidates": n_cand},
+                           "pools_equal_host": [pools_equal, len(tiles)], "candidates": n_cand,
+                           "e2e_from_tile_pixels": tiles_e2e_val,
+                           "e2e": "frontend.refine_image from the sRGB u8 image in page-locked memory"},
         "refined_host_pools": {"ms": host_ref_ms, "mpix_per_s": world * n_px / (host_ref_ms * 1e-3) / 1e6,
                                "rd": host_ref_rd, "candidates": int(len(frec)),
                                "score_ms": r_score_ms, "refine_ms_per_step": r_step_ms,

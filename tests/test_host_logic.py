@@ -13,20 +13,22 @@ from weft_b200 import render
 from weft_b200._lib import TILE_DECODE_DTYPE
 
 
-def test_decode_items_cover_every_row_once():
+def test_decode_items_cover_every_chunk_once():
     rng = np.random.default_rng(3)
     n = 200
     d = np.zeros(n, TILE_DECODE_DTYPE)
     d["target_x0"] = rng.integers(-5, 3000, n)
     d["target_y0"] = rng.integers(0, 2000, n)
-    d["target_w"] = rng.integers(1, 3000, n)
+    d["target_w"] = rng.integers(1, 300, n)
     d["target_h"] = rng.integers(1, 300, n)
     items = render.decode_items(d)
+    k = render.DECODE_ITEM_CHUNKS
     for t in range(n):
-        w, h = int(d["target_w"][t]), int(d["target_h"][t])
-        rows = max(1, render.DECODE_ITEM_PIXELS // w)  # rows an item covers, as the kernel
-        starts = sorted(int(r) for tt, r in items if tt == t)
-        assert starts == list(range(0, h, rows))
+        x0, w, h = int(d["target_x0"][t]), int(d["target_w"][t]), int(d["target_h"][t])
+        groups = ((x0 + w + 3) // 4 - x0 // 4) * h  # floor division, as the kernel
+        chunks = -(-groups // render.DECODE_CHUNK_GROUPS)
+        starts = sorted(int(c) for tt, c in items if tt == t)
+        assert starts == list(range(0, chunks, k))
 
 
 def test_refine_flop_count_follows_the_per_kind_table():

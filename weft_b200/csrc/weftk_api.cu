@@ -171,8 +171,10 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     for (int i = 0; i < n_tiles; ++i) {
         const WeftTileDecodeDesc& d = h_descs[i];
         if (d.target_w > 0 && d.target_h > 0) {
-            const int rows = std::max(1, WEFTK_DECODE_ITEM_PIXELS / d.target_w);
-            for (int r = 0; r < d.target_h; r += rows) items.push_back(make_int2(i, r));
+            auto fdiv4 = [](long long v) { return v >= 0 ? v / 4 : -((-v + 3) / 4); };
+            const long long G = fdiv4((long long)d.target_x0 + d.target_w + 3) - fdiv4(d.target_x0);
+            const long long chunks = (G * d.target_h + WEFTK_DECODE_CHUNK_GROUPS - 1) / WEFTK_DECODE_CHUNK_GROUPS;
+            for (long long c = 0; c < chunks; c += WEFTK_DECODE_ITEM_CHUNKS) items.push_back(make_int2(i, (int)c));
         }
         if (d.prim_count < 0 || d.prim_count > 48 || d.prim_offset < 0 || (int64_t)d.prim_offset + d.prim_count > n_prims ||
             d.target_w <= 0 || d.target_h <= 0 || d.target_w > 8192 || d.target_h > 8192 || d.source_size <= 0 ||

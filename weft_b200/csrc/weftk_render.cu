@@ -102,7 +102,9 @@ __global__ void __launch_bounds__(256) score_evals_kernel(const WeftEval* __rest
     if (lane == 0) out[warp] = (float)(acc / (double)(3 * npix));
 }
 
+constexpr int DEC_PPL = 4;
 constexpr int DEC_THREADS = 128;
+static_assert(WEFTK_DECODE_CHUNK_GROUPS == 32 && DEC_PPL == 4, "chunk layout is part of the C ABI");
 constexpr int MAX_TILE_PRIMS = 48;
 
 // Sole-bicubic tile: float64 Bernstein evaluation of the 4x4x3 control grid at sample
@@ -125,47 +127,22 @@ __device__ __noinline__ void bicubic_pixel(const float* ctrl, int lx, int ly, in
     rgb[2] = clamp01((float)o[2]);
 }
 
-// Output-major walk.  A work item is (tile, first row): rows [first, first + R) of the tile's
-// target rect, R = max(1, WEFTK_DECODE_ITEM_PIXELS / w).  The rect's part of an output row is a
-// run of 3w floats; the warp covers the item's runs with 16-byte float4 slots aligned in the
-// image, slot q of the item at (row q / n4, float4 q % n4), one slot per lane per step, so the
-// lanes of a store instruction write consecutive 16-byte slots (whole sectors) of at most a few
-// rows.  A float4 holds parts of two pixels (pa = f / 3 and pa + 1 for its first float f), so a
-// lane evaluates two pixels per slot; slots cut by the rect's left or right edge are written
-// float by float (the neighbouring tile writes the rest).  The rest as before: a persistent
-// grid of one wave, each warp walking items it, it + n_warps, ... and fetching the records of
-// its next DEC_BATCH items at once (item, descriptor and first primitive, one item per lane).
+// Work items: (tile, first chunk) pairs.  Each row of a tile's target rect is covered by
+// 4-pixel groups aligned to output x multiples of 4, so a thread writes its 4 pixels
+// (48 bytes) as three 16-byte stores.  A chunk is 32 groups (one per lane) and an item is
+// up to DEC_ITEM_CHUNKS chunks, rendered by ONE warp: the warp stages its tile's
+// primitives in its own slice of shared memory and never waits on the rest of the CTA,
+// so every resident warp works on a different item.  A persistent grid of one wave
+// (every CTA resident) walks the list.  A warp's items are it, it + n_warps, ...; it
+// fetches the records of its next DEC_BATCH items at once (item, descriptor and first
+// primitive, one item per lane), so the dependent-load chain item -> descriptor ->
+// primitive is paid once per batch instead of once per item.
+constexpr int DEC_ITEM_CHUNKS = WEFTK_DECODE_ITEM_CHUNKS;
 constexpr int DEC_WARPS = DEC_THREADS / 32;
 constexpr int DEC_MINB = 4;  // resident CTAs per SM the register budget is set for
 constexpr int DEC_BATCH = 8;
 
-__device__ __forceinline__ int floor_div(int v, int m) { return v >= 0 ? v / m : -((-v + m - 1) / m); }
-
-__device__ __forceinline__ int rows_per_item(int w) { return max(1, WEFTK_DECODE_ITEM_PIXELS / w); }
-
-// Colour of one channel c (0..2) of a pixel pair for float j of a slot whose first float is at
-// phase ph = f % 3: floats j < 3 - ph belong to pixel a, the rest to pixel b.
-__device__ __forceinline__ float slot_value(int j, int ph, const float (&A)[3], const float (&B)[3]) {
-    const int c = (ph + j) % 3;
-    return (j < 3 - ph) ? A[c] : B[c];
-}
-
-// Bilinear 4x4 RES1 grid at a pixel centre, edge-clamped (src/weft/render.py:474-515); the row
-// terms (ry0, ry1, wy) are the caller's.
-__device__ __forceinline__ void res1_at(const float* grid, int lx, float gscale, int ry0, int ry1, float wy,
-                                        float (&v)[3]) {
-    const float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
-    const int rx0 = (int)floorf(gx), rx1 = min(rx0 + 1, 3);
-    const float wx = __fsub_rn(gx, (float)rx0);
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch) {
-        const float c00 = grid[(ry0 * 4 + rx0) * 3 + ch], c01 = grid[(ry0 * 4 + rx1) * 3 + ch];
-        const float c10 = grid[(ry1 * 4 + rx0) * 3 + ch], c11 = grid[(ry1 * 4 + rx1) * 3 + ch];
-        const float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
-        const float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
-        v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
-    }
-}
+__device__ __forceinline__ int floor_div4(int v) { return v >= 0 ? (v >> 2) : -((-v + 3) >> 2); }
 
 __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
     const WeftTileDecodeDesc* __restrict__ descs, int n_tiles, const int2* __restrict__ items, int n_items,
@@ -184,8 +161,7 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
     int2* bitem = bitem_all[wid];
     WeftTileDecodeDesc* bdesc = bdesc_all[wid];
     WeftPrim* bprim = bprim_all[wid];
-    const bool w_aligned = (W & 3) == 0;  // rows start on 16-byte boundaries
-    const long long row_floats = 3ll * W;
+    const bool w_aligned = (W & 3) == 0;
     const int n_warps = gridDim.x * DEC_WARPS;
     auto desc_ok = [](const WeftTileDecodeDesc& d) {
         return d.prim_count >= 0 && d.prim_count <= MAX_TILE_PRIMS && d.target_w > 0 && d.target_h > 0 &&
@@ -215,10 +191,16 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
             }
             const WeftTileDecodeDesc d = bdesc[b];
             const int n = d.prim_count, w = d.target_w, h = d.target_h;
-            if (!desc_ok(d) || item.y < 0 || item.y >= h) {
+            if (!desc_ok(d)) {
                 if (lane == 0) report(WEFTK_E_ARG);
                 continue;
             }
+            const int a0 = floor_div4(d.target_x0);
+            const int G = floor_div4(d.target_x0 + w + 3) - a0;  // aligned groups per row
+            const int n_groups = G * h;                          // < 2^24 for any rect the host accepts
+            const int n_chunks = (n_groups + 31) / 32;
+            const float invG = 1.0f / (float)G;
+            const int c_end = min(n_chunks, item.y + DEC_ITEM_CHUNKS);
             for (int i = lane; i < n; i += 32)
                 sp[i] = prep_prim(i == 0 ? bprim[b] : load_prim(prims + d.prim_offset + i));
             const bool has_res1 = res1 != nullptr && n_res1 > 0 && d.res1_index >= 0;
@@ -239,90 +221,178 @@ __global__ void __launch_bounds__(DEC_THREADS, DEC_MINB) render_tiles_kernel(
                 for (int i = lane; i < 48; i += 32) ctrl[i] = cp48[(size_t)gi * 48 + i];
                 __syncwarp();
             }
-            const bool lone_const = n == 1 && sp[0].kind == K_CONST;
             const int side = max(w, h);
             const float step = (side == d.source_size) ? 1.0f : (float)((double)d.source_size / (double)side);
             const float gscale = (float)(4.0 / (double)h);  // RES1 is upsampled at the cropped tile's height
-            // A lone constant layer is one colour before RES1 (the blend over black and the RES0 add
-            // are the general path's operations, done once per item).
-            const float cfr = clamp01(blend(sp[0].cr, sp[0].a, 0.0f) + d.res0_r);
-            const float cfg = clamp01(blend(sp[0].cg, sp[0].a, 0.0f) + d.res0_g);
-            const float cfb = clamp01(blend(sp[0].cb, sp[0].a, 0.0f) + d.res0_b);
-            const int x0 = d.target_x0, x1 = d.target_x0 + w;
-            const int f_lo = 3 * x0, f_hi = 3 * x1;  // the rect's float run within a row
-            const int k0 = floor_div(f_lo, 4), n4 = floor_div(f_hi + 3, 4) - k0;
-            const int r0 = item.y, r1 = min(h, r0 + rows_per_item(w));
-            const int total = (r1 - r0) * n4;
-            // slot q = base + lane at (row, col); each step advances 32 slots
-            const int drow = 32 / n4, dcol = 32 - drow * n4;
-            int row = r0 + lane / n4, col = lane - (lane / n4) * n4;
-            for (int sbase = 0; sbase < total; sbase += 32, row += drow, col += dcol) {
-                if (col >= n4) {
-                    col -= n4;
-                    ++row;
+            if (n == 1 && sp[0].kind == K_CONST) {
+                // A lone constant layer is one colour before RES1 (the blend over black and the RES0
+                // add are the general path's operations, done once per item), so the walk only
+                // writes it, or adds the bilinear RES1 grid per pixel.  Each lane steps its group
+                // (row, column) by 32 groups per chunk instead of dividing.
+                const float fr = clamp01(blend(sp[0].cr, sp[0].a, 0.0f) + d.res0_r);
+                const float fg = clamp01(blend(sp[0].cg, sp[0].a, 0.0f) + d.res0_g);
+                const float fb = clamp01(blend(sp[0].cb, sp[0].a, 0.0f) + d.res0_b);
+                const int x0 = d.target_x0, x1 = d.target_x0 + w;
+                const int g0 = item.y * 32 + lane, drow = 32 / G, dcol = 32 - drow * G;
+                int row = g0 / G, col = g0 - row * G;
+                for (int chunk = item.y; chunk < c_end; ++chunk, row += drow, col += dcol) {
+                    if (col >= G) {
+                        col -= G;
+                        ++row;
+                    }
+                    const int gy = d.target_y0 + row;
+                    if (row >= h || gy < 0 || gy >= H) continue;
+                    const int gxs = (a0 + col) * 4;
+                    float* dst = out + ((size_t)gy * W + gxs) * 3;
+                    const bool full = w_aligned && gxs >= x0 && gxs + DEC_PPL <= x1 && gxs >= 0 && gxs + DEC_PPL <= W;
+                    float o[DEC_PPL][3];
+                    if (!has_res1) {
+                        if (full) {
+                            float4* d4 = reinterpret_cast<float4*>(dst);
+                            d4[0] = make_float4(fr, fg, fb, fr);
+                            d4[1] = make_float4(fg, fb, fr, fg);
+                            d4[2] = make_float4(fb, fr, fg, fb);
+                            continue;
+                        }
+#pragma unroll
+                        for (int j = 0; j < DEC_PPL; ++j) {
+                            o[j][0] = fr;
+                            o[j][1] = fg;
+                            o[j][2] = fb;
+                        }
+                    } else {
+                        // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
+                        const float gyf =
+                            fminf(fmaxf(__fsub_rn(__fmul_rn((float)row + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                        const int ry0 = (int)floorf(gyf), ry1 = min(ry0 + 1, 3);
+                        const float wy = __fsub_rn(gyf, (float)ry0);
+#pragma unroll
+                        for (int j = 0; j < DEC_PPL; ++j) {
+                            const int lxc = min(max(gxs + j - x0, 0), w - 1);
+                            const float gx =
+                                fminf(fmaxf(__fsub_rn(__fmul_rn((float)lxc + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                            const int rx0 = (int)floorf(gx), rx1 = min(rx0 + 1, 3);
+                            const float wx = __fsub_rn(gx, (float)rx0);
+                            const float base[3] = {fr, fg, fb};
+#pragma unroll
+                            for (int ch = 0; ch < 3; ++ch) {
+                                const float c00 = grid[(ry0 * 4 + rx0) * 3 + ch], c01 = grid[(ry0 * 4 + rx1) * 3 + ch];
+                                const float c10 = grid[(ry1 * 4 + rx0) * 3 + ch], c11 = grid[(ry1 * 4 + rx1) * 3 + ch];
+                                const float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
+                                const float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
+                                o[j][ch] = clamp01(base[ch] + __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)),
+                                                                        __fmul_rn(bot, wy)));
+                            }
+                        }
+                        if (full) {
+                            float4* d4 = reinterpret_cast<float4*>(dst);
+                            d4[0] = make_float4(o[0][0], o[0][1], o[0][2], o[1][0]);
+                            d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
+                            d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
+                            continue;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < DEC_PPL; ++j) {
+                        const int gxp = gxs + j;
+                        if (gxp >= x0 && gxp < x1 && gxp >= 0 && gxp < W) {
+                            dst[3 * j] = o[j][0];
+                            dst[3 * j + 1] = o[j][1];
+                            dst[3 * j + 2] = o[j][2];
+                        }
+                    }
                 }
-                const bool q_ok = sbase + lane < total;
-                const int fa = 4 * (k0 + col);                 // first float of the slot in the row
-                const int ph = ((fa % 3) + 3) % 3;
-                const int pa = floor_div(fa, 3), pb = pa + 1;  // the slot's two pixels
-                const int la = min(max(pa - x0, 0), w - 1), lb = min(max(pb - x0, 0), w - 1);
-                const int rrow = q_ok ? row : r0;
-                float A[3], B[3];
-                if (lone_const) {
-                    A[0] = B[0] = cfr;
-                    A[1] = B[1] = cfg;
-                    A[2] = B[2] = cfb;
-                } else if (bic) {
-                    bicubic_pixel(ctrl, la, min(rrow, side - 1), side, A);
-                    bicubic_pixel(ctrl, lb, min(rrow, side - 1), side, B);
+                continue;
+            }
+            for (int chunk = item.y; chunk < c_end; ++chunk) {
+                const int g = chunk * 32 + lane;
+                const bool g_ok = g < n_groups;
+                // row = g / G via the float reciprocal, corrected by one step (exact for g < 2^24)
+                int row = __float2int_rz(((float)g + 0.5f) * invG);
+                row -= (row * G > g) ? 1 : 0;
+                row += ((row + 1) * G <= g) ? 1 : 0;
+                if (!g_ok) row = 0;
+                const int gxs = (a0 + (g_ok ? g - row * G : 0)) * 4;
+                float fx[DEC_PPL], fy[DEC_PPL], cr[DEC_PPL], cg[DEC_PPL], cb[DEC_PPL];
+                int lx[DEC_PPL];
+                bool valid[DEC_PPL];
+#pragma unroll
+                for (int j = 0; j < DEC_PPL; ++j) {
+                    lx[j] = gxs + j - d.target_x0;
+                    valid[j] = g_ok && lx[j] >= 0 && lx[j] < w;
+                    const int lxc = min(max(lx[j], 0), w - 1);
+                    fx[j] = __fmul_rn((float)lxc + 0.5f, step);
+                    fy[j] = __fmul_rn((float)row + 0.5f, step);
+                    cr[j] = cg[j] = cb[j] = 0.0f;
+                    lx[j] = lxc;
+                }
+                if (bic) {
+                    for (int j = 0; j < DEC_PPL; ++j) {
+                        float rgb[3];
+                        bicubic_pixel(ctrl, lx[j], min(row, side - 1), side, rgb);
+                        cr[j] = rgb[0];
+                        cg[j] = rgb[1];
+                        cb[j] = rgb[2];
+                    }
                 } else {
-                    float fx[2], fy[2], cr[2] = {0.0f, 0.0f}, cg[2] = {0.0f, 0.0f}, cb[2] = {0.0f, 0.0f};
-                    fx[0] = __fmul_rn((float)la + 0.5f, step);
-                    fx[1] = __fmul_rn((float)lb + 0.5f, step);
-                    fy[0] = fy[1] = __fmul_rn((float)rrow + 0.5f, step);
                     for (int k = 0; k < n; ++k) {
                         Prep pr = sp[k];
                         if (pr.kind == K_BICUBIC) pr.kind = K_SKIP;  // kind 5 inside a longer stack is skipped
-                        float a[2], sr[2], sg[2], sb[2];
-                        prim_eval<2>(pr, fx, fy, a, sr, sg, sb, lane);
+                        float a[DEC_PPL], sr[DEC_PPL], sg[DEC_PPL], sb[DEC_PPL];
+                        prim_eval<DEC_PPL>(pr, fx, fy, a, sr, sg, sb, lane);
 #pragma unroll
-                        for (int j = 0; j < 2; ++j) {
+                        for (int j = 0; j < DEC_PPL; ++j) {
                             cr[j] = blend(sr[j], a[j], cr[j]);
                             cg[j] = blend(sg[j], a[j], cg[j]);
                             cb[j] = blend(sb[j], a[j], cb[j]);
                         }
                     }
-                    A[0] = clamp01(cr[0] + d.res0_r);
-                    A[1] = clamp01(cg[0] + d.res0_g);
-                    A[2] = clamp01(cb[0] + d.res0_b);
-                    B[0] = clamp01(cr[1] + d.res0_r);
-                    B[1] = clamp01(cg[1] + d.res0_g);
-                    B[2] = clamp01(cb[1] + d.res0_b);
                 }
-                if (has_res1) {
-                    const float gyf = fminf(fmaxf(__fsub_rn(__fmul_rn((float)rrow + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
-                    const int ry0 = (int)floorf(gyf), ry1 = min(ry0 + 1, 3);
-                    const float wy = __fsub_rn(gyf, (float)ry0);
-                    float va[3], vb[3];
-                    res1_at(grid, la, gscale, ry0, ry1, wy, va);
-                    res1_at(grid, lb, gscale, ry0, ry1, wy, vb);
+                float o[DEC_PPL][3];
 #pragma unroll
-                    for (int ch = 0; ch < 3; ++ch) {
-                        A[ch] = clamp01(A[ch] + va[ch]);
-                        B[ch] = clamp01(B[ch] + vb[ch]);
+                for (int j = 0; j < DEC_PPL; ++j) {
+                    float r = clamp01(cr[j] + d.res0_r), gg = clamp01(cg[j] + d.res0_g), b = clamp01(cb[j] + d.res0_b);
+                    if (has_res1) {
+                        // Bilinear 4x4 grid at pixel centres, edge-clamped (src/weft/render.py:474-515).
+                        float gx = fminf(fmaxf(__fsub_rn(__fmul_rn((float)lx[j] + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                        float gy = fminf(fmaxf(__fsub_rn(__fmul_rn((float)row + 0.5f, gscale), 0.5f), 0.0f), 3.0f);
+                        int x0 = (int)floorf(gx), y0 = (int)floorf(gy);
+                        float wx = __fsub_rn(gx, (float)x0), wy = __fsub_rn(gy, (float)y0);
+                        int x1 = min(x0 + 1, 3), y1 = min(y0 + 1, 3);
+                        float v[3];
+#pragma unroll
+                        for (int ch = 0; ch < 3; ++ch) {
+                            float c00 = grid[(y0 * 4 + x0) * 3 + ch], c01 = grid[(y0 * 4 + x1) * 3 + ch];
+                            float c10 = grid[(y1 * 4 + x0) * 3 + ch], c11 = grid[(y1 * 4 + x1) * 3 + ch];
+                            float top = __fadd_rn(__fmul_rn(c00, __fsub_rn(1.0f, wx)), __fmul_rn(c01, wx));
+                            float bot = __fadd_rn(__fmul_rn(c10, __fsub_rn(1.0f, wx)), __fmul_rn(c11, wx));
+                            v[ch] = __fadd_rn(__fmul_rn(top, __fsub_rn(1.0f, wy)), __fmul_rn(bot, wy));
+                        }
+                        r = clamp01(r + v[0]);
+                        gg = clamp01(gg + v[1]);
+                        b = clamp01(b + v[2]);
                     }
+                    o[j][0] = r;
+                    o[j][1] = gg;
+                    o[j][2] = b;
                 }
                 const int gy = d.target_y0 + row;
-                if (!q_ok || gy < 0 || gy >= H) continue;
-                float* dst = out + (size_t)gy * row_floats + fa;
-                if (w_aligned && fa >= f_lo && fa + 4 <= f_hi && fa >= 0 && fa + 4 <= row_floats) {
-                    *reinterpret_cast<float4*>(dst) = make_float4(slot_value(0, ph, A, B), slot_value(1, ph, A, B),
-                                                                  slot_value(2, ph, A, B), slot_value(3, ph, A, B));
+                if (!g_ok || gy < 0 || gy >= H) continue;
+                float* dst = out + ((size_t)gy * W + gxs) * 3;
+                if (w_aligned && valid[0] && valid[DEC_PPL - 1] && gxs >= 0 && gxs + DEC_PPL <= W) {
+                    float4* d4 = reinterpret_cast<float4*>(dst);
+                    d4[0] = make_float4(o[0][0], o[0][1], o[0][2], o[1][0]);
+                    d4[1] = make_float4(o[1][1], o[1][2], o[2][0], o[2][1]);
+                    d4[2] = make_float4(o[2][2], o[3][0], o[3][1], o[3][2]);
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int f = fa + j;
-                        if (f >= f_lo && f < f_hi && f >= 0 && f < row_floats) dst[j] = slot_value(j, ph, A, B);
+                    for (int j = 0; j < DEC_PPL; ++j) {
+                        const int gxp = gxs + j;
+                        if (valid[j] && gxp >= 0 && gxp < W) {
+                            dst[3 * j] = o[j][0];
+                            dst[3 * j + 1] = o[j][1];
+                            dst[3 * j + 2] = o[j][2];
+                        }
                     }
                 }
             }

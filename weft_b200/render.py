@@ -21,18 +21,22 @@ from . import _lib
 from ._lib import PRIM_DTYPE, TILE_DECODE_DTYPE
 
 MAX_TILE_PRIMS = 48
-DECODE_ITEM_PIXELS = 1024  # WEFTK_DECODE_ITEM_PIXELS
+DECODE_CHUNK_GROUPS = 32   # WEFTK_DECODE_CHUNK_GROUPS
+DECODE_ITEM_CHUNKS = 8     # WEFTK_DECODE_ITEM_CHUNKS
 
 
 def decode_items(descs: np.ndarray) -> np.ndarray:
-    """Work items (tile, first row) of weftk_render_tiles, int32 (n, 2): each covers
-    max(1, DECODE_ITEM_PIXELS // target_w) rows of the tile's target rect."""
-    w = descs["target_w"].astype(np.int64)
-    rows = np.maximum(1, DECODE_ITEM_PIXELS // np.maximum(w, 1))
-    per = (descs["target_h"].astype(np.int64) + rows - 1) // rows
+    """Work items (tile, first chunk) of weftk_render_tiles, int32 (n, 2).
+
+    A tile's rect rows are covered by 4-pixel groups aligned to output x multiples of 4.
+    """
+    x0 = descs["target_x0"].astype(np.int64)
+    groups = (np.floor_divide(x0 + descs["target_w"] + 3, 4) - np.floor_divide(x0, 4)) * descs["target_h"]
+    chunks = (groups + DECODE_CHUNK_GROUPS - 1) // DECODE_CHUNK_GROUPS
+    per = (chunks + DECODE_ITEM_CHUNKS - 1) // DECODE_ITEM_CHUNKS
     tile = np.repeat(np.arange(len(descs)), per)
     k = np.arange(int(per.sum())) - np.repeat(np.concatenate([[0], np.cumsum(per)[:-1]]), per)
-    return np.stack([tile, k * np.repeat(rows, per)], axis=1).astype(np.int32)
+    return np.stack([tile, k * DECODE_ITEM_CHUNKS], axis=1).astype(np.int32)
 
 
 def pack_records(stacks) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:

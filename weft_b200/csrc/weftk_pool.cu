@@ -56,18 +56,15 @@ struct Scratch {
     int peaks[NB];
     int n_peaks;
     float p25, p75, pm75;
-    // candidate assembly
+    // palettes (the template palette extends the edge palette) and the candidate list's segments
+    float pal[MAXPAL][3];
+    int npal_e, npal_t;
+    int seg[8];
     int n_cand;
-    int8_t kind[MAXC];
-    double geom[MAXC][4];
-    float c0[MAXC][3];
-    float c1[MAXC][3];
-    double alpha[MAXC];
-    int key[MAXC][KEYS];
+    unsigned long long hash[MAXC];
     int keep[MAXC];
-    int out_pos[MAXC];
     int n_out;
-    int wcnt[8][NB];
+    int wcnt[16][NB];
 };
 
 __device__ __forceinline__ float clamp01(float v) { return fmaxf(0.0f, fminf(1.0f, v)); }
@@ -135,22 +132,6 @@ __device__ bool near_any(const float* c, const float (*pal)[3], int n) {
 
 __device__ __forceinline__ int qkey(double v, double s) { return (int)(long long)__dadd_rn(__dmul_rn(v, s), 0.5); }
 
-__device__ void add_cand(Scratch& S, int kind, const double* g, const float* c0, const float* c1, double alpha) {
-    const int i = S.n_cand;
-    if (i >= MAXC) {
-        atomicCAS(&g_device_status, 0, WEFTK_E_RANGE);
-        return;
-    }
-    S.kind[i] = (int8_t)kind;
-    for (int k = 0; k < 4; ++k) S.geom[i][k] = g ? g[k] : 0.0;
-    for (int k = 0; k < 3; ++k) {
-        S.c0[i][k] = c0[k];
-        S.c1[i][k] = c1 ? c1[k] : 0.0f;
-    }
-    S.alpha[i] = alpha;
-    S.n_cand = i + 1;
-}
-
 // Dynamic shared memory of one tile of N pixels: seven float planes (r, g, b, luminance, the
 // np.gradient magnitude, the Sobel magnitude, a sort key), the sorted pixel indices, the bins.
 constexpr size_t POOL_FLOAT_PLANES = 7;
@@ -171,6 +152,7 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     int* sidx = reinterpret_cast<int*>(skey + N);     // [N] pixel of each sorted luminance
     uint8_t* bin = reinterpret_cast<uint8_t*>(sidx + N);  // [N]
     static_assert(POOL_FLOAT_PLANES == 7, "the planes above are col[3], lum, magt, mags, skey");
+    static_assert(NW <= 16, "the histogram's per-warp counters hold 16 warps");
     __shared__ Scratch S;
     (void)quality;
 
@@ -240,7 +222,7 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
                                        : __fdiv_rn(__fsub_rn(L[p + 1], L[p - 1]), 2.0f);
         magt[p] = __fsqrt_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)));
     }
-    for (int i = tid; i < 8 * NB; i += NT) (&S.wcnt[0][0])[i] = 0;
+    for (int i = tid; i < 16 * NB; i += NT) (&S.wcnt[0][0])[i] = 0;
     __syncthreads();
 
     // 3. histogram: stable counting sort of the Sobel magnitudes by bin into skey
@@ -419,141 +401,141 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     }
     __syncthreads();
 
-    // 6. the candidate list, in the reference's order
+    // 6. palettes (one thread; a handful of means and distance tests), then the candidate list's
+    //    segment sizes: the list is (edge pool) palette x 4 alphas, quadrants x 2, orientations x 5,
+    //    (template pool) palette x 4, quadrants x 2, blocks, splits x 3 or x 1, so candidate i is
+    //    a function of i that any thread can evaluate (cand_at below)
     if (tid == 0) {
-        S.n_cand = 0;
-        auto mean = [&](int r, float* out) {
-            for (int c = 0; c < 3; ++c) out[c] = __fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]);
-        };
-        auto clamp3 = [](float* v) {
-            for (int c = 0; c < 3; ++c) v[c] = clamp01(v[c]);
-        };
-        float fb[3], avg[3];
-        mean(0, fb);
-        for (int c = 0; c < 3; ++c) avg[c] = clamp01(fb[c]);
-        float pal[MAXPAL][3];
-        int npal = 0;
-        for (int c = 0; c < 3; ++c) pal[0][c] = avg[c];
-        npal = 1;
-        for (int r = 21; r < 30; ++r) {
+        float avg[3];
+        for (int c = 0; c < 3; ++c) avg[c] = clamp01(__fdiv_rn(S.rsum[0][c], (float)S.rcnt[0]));
+        int npal = 1;
+        for (int c = 0; c < 3; ++c) S.pal[0][c] = avg[c];
+        for (int r = 21; r < 33; ++r) {
+            if (r == 30) S.npal_e = npal;  // the template palette adds bright / dark / edge colours
             const Region R = S.reg[r];
             float m[3];
-            if (R.b <= R.a) {
+            if (r < 30 && R.b <= R.a) {
                 const int p = sidx[min(R.a, N - 1)];
                 for (int c = 0; c < 3; ++c) m[c] = col[c * N + p];
-            } else {
-                mean(r, m);
-            }
-            clamp3(m);
-            if (!near_any(m, pal, npal) && npal < MAXPAL) {
-                for (int c = 0; c < 3; ++c) pal[npal][c] = m[c];
-                ++npal;
-            }
-        }
-        const double A4[4] = {1.0, 0.7, 0.4, 0.2};
-        const double A3[3] = {1.0, 0.7, 0.4};
-        // edge-driven pool
-        if (want0) {
-            for (int i = 0; i < npal; ++i)
-                for (int a = 0; a < 4; ++a) add_cand(S, 0, nullptr, pal[i], nullptr, A4[a]);
-            for (int q = 1; q <= 4; ++q) {
-                float m[3];
-                mean(q, m);
-                clamp3(m);
-                add_cand(S, 0, nullptr, m, nullptr, 0.5);
-                add_cand(S, 0, nullptr, m, nullptr, 0.3);
-            }
-        }
-        int r = 33;
-        if (want1) {
-            for (int i = 0; i < S.n_peaks; ++i, r += 2) {
-                float c0[3], c1[3];
-                if (S.rcnt[r] > 0) {
-                    mean(r, c0);
-                    clamp3(c0);
-                } else {
-                    for (int c = 0; c < 3; ++c) c0[c] = avg[c];
-                }
-                if (S.rcnt[r + 1] > 0) {
-                    mean(r + 1, c1);
-                    clamp3(c1);
-                } else {
-                    for (int c = 0; c < 3; ++c) c1[c] = avg[c];
-                }
-                const double* g = tb.orient_geom + (size_t)((si * 16 + S.peaks[i]) * 3) * 4;
-                for (int a = 0; a < 3; ++a) add_cand(S, 1, g, c0, c1, A3[a]);
-                add_cand(S, 1, g + 4, c0, c1, 0.5);
-                add_cand(S, 1, g + 8, c0, c1, 0.5);
-            }
-        }
-        // template pool: palette + bright / dark / edge colours
-        for (int e = 30; e < 33; ++e) {
-            float m[3];
-            if (S.rcnt[e] > 0) {
-                mean(e, m);
-                clamp3(m);
+            } else if (S.rcnt[r] > 0) {
+                for (int c = 0; c < 3; ++c) m[c] = __fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]);
             } else {
                 for (int c = 0; c < 3; ++c) m[c] = avg[c];
             }
-            if (!near_any(m, pal, npal) && npal < MAXPAL) {
-                for (int c = 0; c < 3; ++c) pal[npal][c] = m[c];
+            for (int c = 0; c < 3; ++c) m[c] = clamp01(m[c]);
+            if (!near_any(m, S.pal, npal) && npal < MAXPAL) {
+                for (int c = 0; c < 3; ++c) S.pal[npal][c] = m[c];
                 ++npal;
             }
         }
-        if (want0) {
-            for (int i = 0; i < npal; ++i)
-                for (int a = 0; a < 4; ++a) add_cand(S, 0, nullptr, pal[i], nullptr, A4[a]);
-            for (int q = 1; q <= 4; ++q) {
-                float m[3];
-                mean(q, m);
-                clamp3(m);
-                add_cand(S, 0, nullptr, m, nullptr, 0.5);
-                add_cand(S, 0, nullptr, m, nullptr, 0.3);
-            }
-            for (int q = 5; q < 21; ++q) {
-                float m[3];
-                mean(q, m);
-                clamp3(m);
-                add_cand(S, 0, nullptr, m, nullptr, 0.25);
-            }
-        }
-        if (want1) {
-            for (int i = 0; i < tb.n_spec; ++i, r += 2) {
-                // batched side means: no clamp; an empty side takes the (unclamped) tile mean
-                float c0[3], c1[3];
-                for (int c = 0; c < 3; ++c) {
-                    c0[c] = S.rcnt[r] > 0 ? __fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]) : fb[c];
-                    c1[c] = S.rcnt[r + 1] > 0 ? __fdiv_rn(S.rsum[r + 1][c], (float)S.rcnt[r + 1]) : fb[c];
-                }
-                const double* g = tb.spec_geom + (size_t)(si * WEFTK_POOL_MAX_SPECS + i) * 4;
-                if (i < tb.n_centre) {
-                    for (int a = 0; a < 3; ++a) add_cand(S, 1, g, c0, c1, A3[a]);
-                } else {
-                    add_cand(S, 1, g, c0, c1, 0.5);
-                }
-            }
-        }
+        S.npal_t = npal;
+        const int sz[7] = {want0 ? S.npal_e * 4 : 0, want0 ? 8 : 0, want1 ? S.n_peaks * 5 : 0,
+                           want0 ? S.npal_t * 4 : 0, want0 ? 8 : 0, want0 ? 16 : 0,
+                           want1 ? tb.n_centre * 3 + (tb.n_spec - tb.n_centre) : 0};
+        S.seg[0] = 0;
+        for (int k = 0; k < 7; ++k) S.seg[k + 1] = S.seg[k] + sz[k];
+        S.n_cand = min(S.seg[7], MAXC);
+        if (S.seg[7] > MAXC) atomicCAS(&g_device_status, 0, WEFTK_E_RANGE);
     }
     __syncthreads();
 
-    // 7. de-duplication key (kind, geometry x4, colour0 x64, alpha x32, colour1 x64 for a
-    //    linear patch; int(v * s + 0.5) truncating toward zero), first occurrence kept
+    // candidate i: kind, float64 geometry (the reference's Python values), colours, alpha
+    auto cand_at = [&](int i, int& kind, double (&g)[4], float (&c0)[3], float (&c1)[3], double& alpha) {
+        const double A4[4] = {1.0, 0.7, 0.4, 0.2};
+        const double A3[3] = {1.0, 0.7, 0.4};
+        auto mean_clamped = [&](int r, float (&m)[3]) {
+            for (int c = 0; c < 3; ++c) m[c] = clamp01(__fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]));
+        };
+        kind = 0;
+        for (int k = 0; k < 4; ++k) g[k] = 0.0;
+        for (int c = 0; c < 3; ++c) c1[c] = 0.0f;
+        int k = 0;
+        while (i >= S.seg[k + 1]) ++k;
+        const int j = i - S.seg[k];
+        switch (k) {
+            case 0:
+            case 3:  // palette colour x alphas 1, .7, .4, .2
+                for (int c = 0; c < 3; ++c) c0[c] = S.pal[j >> 2][c];
+                alpha = A4[j & 3];
+                break;
+            case 1:
+            case 4:  // quadrant mean x alphas .5, .3
+                mean_clamped(1 + (j >> 1), c0);
+                alpha = (j & 1) ? 0.3 : 0.5;
+                break;
+            case 2: {  // orientation split: centre x 1, .7, .4, offsets at 0.25 and 0.75 x .5
+                const int pk = j / 5, m = j - pk * 5, r = 33 + 2 * pk;
+                float avg[3];
+                for (int c = 0; c < 3; ++c) avg[c] = clamp01(__fdiv_rn(S.rsum[0][c], (float)S.rcnt[0]));
+                if (S.rcnt[r] > 0) mean_clamped(r, c0);
+                else
+                    for (int c = 0; c < 3; ++c) c0[c] = avg[c];
+                if (S.rcnt[r + 1] > 0) mean_clamped(r + 1, c1);
+                else
+                    for (int c = 0; c < 3; ++c) c1[c] = avg[c];
+                const double* gg = tb.orient_geom + ((size_t)(si * 16 + S.peaks[pk]) * 3 + (m < 3 ? 0 : m - 2)) * 4;
+                for (int q = 0; q < 4; ++q) g[q] = gg[q];
+                alpha = m < 3 ? A3[m] : 0.5;
+                kind = 1;
+                break;
+            }
+            case 5:  // 4x4 block mean x .25
+                mean_clamped(5 + j, c0);
+                alpha = 0.25;
+                break;
+            default: {  // template split: batched side means, not clamped; an empty side takes the
+                        // (unclamped) tile mean
+                const int sp = j < tb.n_centre * 3 ? j / 3 : tb.n_centre + (j - tb.n_centre * 3);
+                alpha = j < tb.n_centre * 3 ? A3[j % 3] : 0.5;
+                const int r = 33 + 2 * S.n_peaks + 2 * sp;
+                for (int c = 0; c < 3; ++c) {
+                    const float fb = __fdiv_rn(S.rsum[0][c], (float)S.rcnt[0]);
+                    c0[c] = S.rcnt[r] > 0 ? __fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]) : fb;
+                    c1[c] = S.rcnt[r + 1] > 0 ? __fdiv_rn(S.rsum[r + 1][c], (float)S.rcnt[r + 1]) : fb;
+                }
+                const double* gg = tb.spec_geom + (size_t)(si * WEFTK_POOL_MAX_SPECS + sp) * 4;
+                for (int q = 0; q < 4; ++q) g[q] = gg[q];
+                kind = 1;
+            }
+        }
+    };
+    // the reference's coarse de-duplication key: kind, geometry x4, colour0 x64, alpha x32,
+    // colour1 x64 for a linear patch (each int(v * s + 0.5), truncating toward zero)
+    auto key_of = [&](int i, int (&key)[KEYS]) {
+        int kind;
+        double g[4], alpha;
+        float c0[3], c1[3];
+        cand_at(i, kind, g, c0, c1, alpha);
+        key[0] = kind;
+        for (int j = 0; j < 4; ++j) key[1 + j] = kind == 1 ? qkey(g[j], 4.0) : 0;
+        for (int j = 0; j < 3; ++j) key[5 + j] = qkey((double)c0[j], 64.0);
+        key[8] = qkey(alpha, 32.0);
+        for (int j = 0; j < 3; ++j) key[9 + j] = kind == 1 ? qkey((double)c1[j], 64.0) : 0;
+    };
+
+    // 7. first occurrences kept: 64-bit hashes of the keys, the full keys compared on a match
     const int nc = S.n_cand;
     for (int i = tid; i < nc; i += NT) {
-        int* k = S.key[i];
-        const int kind = S.kind[i];
-        k[0] = kind;
-        for (int j = 0; j < 4; ++j) k[1 + j] = kind == 1 ? qkey(S.geom[i][j], 4.0) : 0;
-        for (int j = 0; j < 3; ++j) k[5 + j] = qkey((double)S.c0[i][j], 64.0);
-        k[8] = qkey(S.alpha[i], 32.0);
-        for (int j = 0; j < 3; ++j) k[9 + j] = kind == 1 ? qkey((double)S.c1[i][j], 64.0) : 0;
+        int key[KEYS];
+        key_of(i, key);
+        unsigned long long h = 0x9e3779b97f4a7c15ull;
+        for (int k = 0; k < KEYS; ++k) {
+            h = (h ^ (unsigned long long)(unsigned)key[k]) * 0xff51afd7ed558ccdull;
+            h ^= h >> 33;
+        }
+        S.hash[i] = h;
     }
     __syncthreads();
     for (int i = tid; i < nc; i += NT) {
+        const unsigned long long h = S.hash[i];
         bool dup = false;
         for (int j = 0; j < i && !dup; ++j) {
+            if (S.hash[j] != h) continue;
+            int a[KEYS], b[KEYS];
+            key_of(i, a);
+            key_of(j, b);
             bool same = true;
-            for (int k = 0; k < KEYS; ++k) same = same && S.key[i][k] == S.key[j][k];
+            for (int k = 0; k < KEYS; ++k) same = same && a[k] == b[k];
             dup = same;
         }
         S.keep[i] = !dup;
@@ -562,8 +544,9 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     if (tid == 0) {
         int n = 0;
         for (int i = 0; i < nc; ++i) {
-            S.out_pos[i] = n;
-            n += S.keep[i];
+            const int k = S.keep[i];
+            S.keep[i] = k ? n : -1;  // output position, -1 = dropped
+            n += k;
         }
         if (n > job.pool_cap) {
             atomicCAS(&g_device_status, 0, WEFTK_E_RANGE);
@@ -575,16 +558,21 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     __syncthreads();
     WeftPrim* out = job.cand + job.pool_off[t];
     for (int i = tid; i < nc; i += NT) {
-        if (!S.keep[i] || S.out_pos[i] >= S.n_out) continue;
+        const int pos = S.keep[i];
+        if (pos < 0 || pos >= S.n_out) continue;
+        int kind;
+        double g[4], alpha;
+        float c0[3], c1[3];
+        cand_at(i, kind, g, c0, c1, alpha);
         WeftPrim p;
-        p.kind = S.kind[i];
-        for (int j = 0; j < 7; ++j) p.geom[j] = j < 4 && S.kind[i] == 1 ? (float)S.geom[i][j] : 0.0f;
+        p.kind = kind;
+        for (int j = 0; j < 7; ++j) p.geom[j] = j < 4 ? (float)g[j] : 0.0f;
         for (int j = 0; j < 3; ++j) {
-            p.color0[j] = S.c0[i][j];
-            p.color1[j] = S.kind[i] == 1 ? S.c1[i][j] : 0.0f;
+            p.color0[j] = c0[j];
+            p.color1[j] = c1[j];
         }
-        p.alpha = (float)S.alpha[i];
-        out[S.out_pos[i]] = p;
+        p.alpha = (float)alpha;
+        out[pos] = p;
     }
 }
 
@@ -618,6 +606,33 @@ int launch_gen(const WeftPoolTables& tb, const WeftPoolJob& job, int si, cudaStr
 
 using namespace weftk;
 
+// Side streams of the current device that run the larger tile classes beside the 8-px class
+// (forked from and joined back into the caller's stream with events, so a captured graph gets
+// parallel branches).  Created on the first call on a device.
+struct SideStreams {
+    cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+};
+
+int side_streams(SideStreams** out) {
+    static std::mutex mu;
+    static SideStreams per_dev[64];
+    int dev = 0;
+    WEFTK_CUDA(cudaGetDevice(&dev));
+    WEFTK_REQUIRE(dev >= 0 && dev < 64, "gen_pools: device index beyond 63");
+    std::lock_guard<std::mutex> lock(mu);
+    SideStreams& ss = per_dev[dev];
+    if (!ss.fork) {
+        for (int i = 0; i < 3; ++i) {
+            WEFTK_CUDA(cudaStreamCreateWithFlags(&ss.s[i], cudaStreamNonBlocking));
+            WEFTK_CUDA(cudaEventCreateWithFlags(&ss.join[i], cudaEventDisableTiming));
+        }
+        WEFTK_CUDA(cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming));
+    }
+    *out = &ss;
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_gen_pools(const WeftPoolTables* tables, const WeftPoolJob* job, void* stream) {
     WEFTK_REQUIRE(tables && job, "gen_pools: null argument");
     WEFTK_REQUIRE(tables->n_spec >= 0 && tables->n_spec <= WEFTK_POOL_MAX_SPECS &&
@@ -637,9 +652,19 @@ extern "C" int weftk_gen_pools(const WeftPoolTables* tables, const WeftPoolJob* 
                       (tables->n_spec == 0 || (tables->spec_geom && tables->spec_mask)),
                   "gen_pools: null table");
     cudaStream_t s = (cudaStream_t)stream;
-    int rc;
+    SideStreams* ss = nullptr;
+    int rc = side_streams(&ss);
+    if (rc) return rc;
+    // the 64-, 32- and 16-px classes (few CTAs, long ones) on side streams, the 8-px class here
+    WEFTK_CUDA(cudaEventRecord(ss->fork, s));
+    for (int i = 0; i < 3; ++i) WEFTK_CUDA(cudaStreamWaitEvent(ss->s[i], ss->fork, 0));
+    if ((rc = launch_gen<64, 512>(*tables, *job, 3, ss->s[0]))) return rc;
+    if ((rc = launch_gen<32, 256>(*tables, *job, 2, ss->s[1]))) return rc;
+    if ((rc = launch_gen<16, 128>(*tables, *job, 1, ss->s[2]))) return rc;
     if ((rc = launch_gen<8, 64>(*tables, *job, 0, s))) return rc;
-    if ((rc = launch_gen<16, 128>(*tables, *job, 1, s))) return rc;
-    if ((rc = launch_gen<32, 256>(*tables, *job, 2, s))) return rc;
-    return launch_gen<64, 256>(*tables, *job, 3, s);
+    for (int i = 0; i < 3; ++i) {
+        WEFTK_CUDA(cudaEventRecord(ss->join[i], ss->s[i]));
+        WEFTK_CUDA(cudaStreamWaitEvent(s, ss->join[i], 0));
+    }
+    return WEFTK_OK;
 }

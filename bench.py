@@ -612,15 +612,18 @@ def refined_headline(args, local, pixels, sizes, pools, stream, world):
     return rf, fast, rec, cnt, statistics.mean(times)
 
 
-def device_headline(args, fit, sizes, caps, stream, world):
-    """The refined fit with its pools generated on the device: pool generation, init round, fused
-    Adam steps and wire-grid snap replayed from one CUDA graph over the resident tiles.  Each timed
-    step is preceded by a 256 MiB write and a short GPU sleep (host launch latency not counted)."""
+def device_headline(args, fit, sizes, caps, stream, world, generate_in_run: bool):
+    """The refined fit over pools generated on the device: (with ``generate_in_run``) pool
+    generation, then init round, fused Adam steps and wire-grid snap replayed from one CUDA graph over
+    the resident tiles; without it the pools are generated once beforehand and stay resident.  Each
+    timed step is preceded by a 256 MiB write and a short GPU sleep (host launch latency not
+    counted)."""
     import torch
 
     from weft_b200.pools import DeviceRefinedFit
 
-    drf = DeviceRefinedFit(fit.t_src, sizes, QUALITY, caps=caps, steps=args.refine_steps, lr=args.refine_lr)
+    drf = DeviceRefinedFit(fit.t_src, sizes, QUALITY, caps=caps, steps=args.refine_steps, lr=args.refine_lr,
+                           generate_in_run=generate_in_run)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=fit.device)
     for _ in range(args.warmup):
         drf.run()
@@ -913,6 +916,8 @@ def main():
     ap.add_argument("--batch-images", default="",
                     help='multi-image batch, e.g. "16x256,16x512,16x1024,16x2048" (empty: skip)')
     ap.add_argument("--batch-steps", type=int, default=100, help="Adam steps of the multi-image refined fit")
+    ap.add_argument("--profile-refined", action="store_true",
+                    help="only the refined fit with device pool generation (eager launches), for profilers")
     args = ap.parse_args()
 
     # Process pools first: spawned before any CUDA initialisation.
@@ -932,9 +937,36 @@ def main():
             dist.destroy_process_group()
 
 
+def profile_refined(args, local, patches):
+    """The refined fit with its pools generated on the device, eager launches only (no CUDA graph,
+    no host-generated pools): what a kernel profiler should see of the headline pipeline."""
+    import torch
+
+    from weft_b200.pools import DeviceRefinedFit
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pixels = np.concatenate([p.reshape(-1, 3) for p in patches])
+    sizes = np.array([p.shape[0] for p in patches], np.int32)
+    src4 = torch.zeros((len(pixels), 4), dtype=torch.float32, device=dev)
+    src4[:, :3] = torch.from_numpy(pixels).to(dev)
+    drf = DeviceRefinedFit(src4, sizes, QUALITY, caps=[CAP] * len(sizes), steps=args.refine_steps,
+                           lr=args.refine_lr, use_graph=False, autotune=False)
+    for _ in range(args.warmup + args.steps):
+        drf.run()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_refined": {"tiles": len(sizes), "steps": args.warmup + args.steps}}), flush=True)
+
+
 def run_weft(args, world, rank, local, executor, cores):
     import torch
 
+    if args.profile_refined:
+        u8 = make_image_u8(args.size, args.size, args.prims, rank)
+        img = srgb_u8_to_linear(u8)
+        tiles = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+        profile_refined(args, local, quadtree.extract_tiles(img, tiles, 64))
+        return
     img, tiles, patches, pools, cand_s = build_workload(args.size, args.prims, rank, executor)
 
     torch.cuda.set_device(local)
@@ -1069,12 +1101,16 @@ def run_weft(args, world, rank, local, executor, cores):
     host_ref_rd = rd_of_params(rf.ss, rf.refiner.p, tiles, patches, img, args.size)
     del rf, fast
 
-    # headline: pool generation + the gradient-refined fit on the device, one CUDA graph, at iso
-    # RD with the plain fit
+    # headline: the gradient-refined fit over device-resident pools (generated on the device before
+    # the timed steps, as the plain fit's pools are before its own), one CUDA graph, at iso RD with
+    # the plain fit; then the same with the generation inside the graph (fit_total)
     sampler2 = ClockSampler(local)
     sampler2.start()
-    drf, ref_ms = device_headline(args, fit, sizes, caps, stream, world)
+    drf, ref_ms = device_headline(args, fit, sizes, caps, stream, world, generate_in_run=False)
     clocks2 = sampler2.stop()
+    drf_total, total_ms = device_headline(args, fit, sizes, caps, stream, world, generate_in_run=True)
+    total_ms = max_over_ranks(total_ms, world)
+    del drf_total
     dbd = device_breakdown(args, drf, lib, stream)
     # host generation of the same pools (the device generator's arctan2 rule), timed, outside the
     # clock window (no GPU work); the device pools must equal them record for record
@@ -1093,10 +1129,10 @@ def run_weft(args, world, rank, local, executor, cores):
     d_refine_tflops = d_flops * args.refine_steps / (dbd["refine_ms"] * 1e-3) / 1e12 if dbd["refine_ms"] else 0.0
     d_init_tflops = dbd["work"][1] / (dbd["init_score_ms"] * 1e-3) / 1e12 if dbd["init_score_ms"] else 0.0
     n_cls = sum(1 for k in (8, 16, 32) if drf.fit.n_items[k])
-    n_gen = sum(1 for t in drf.lists if t is not None)
-    # pool generation (one launch per tile side), moments, reset, prepare, begin, select, end,
-    # scoring (one per size class), refine start, one launch for all refine steps, wire-grid snap
-    ref_launches = n_gen + 9 + n_cls
+    # moments, reset, prepare, begin, select, end, scoring (one per size class), refine start, one
+    # launch for all refine steps, wire-grid snap (+ the pool generation, one launch per tile side,
+    # in fit_total)
+    ref_launches = 9 + n_cls
     # what the Adam steps add: RD of the same init round's picks without them
     init_rd = rd_of_params(dss, drf.rf.start, tiles, patches, img, args.size)
 
@@ -1178,9 +1214,10 @@ def run_weft(args, world, rank, local, executor, cores):
     dominant = parts[0][1]
     head_value, head_ms = (ref_value, ref_ms) if iso else (plain_value, plain_ms)
     grad_db = ref_rd["rd_score"] - init_rd["rd_score"]
-    fit_desc = (f"pools generated on the device ({REFINE_POOLS[args.refine_pool]} kinds, {n_cand} candidates), "
-                f"init round, {args.refine_steps} fused Adam steps (lr {args.refine_lr}) and the wire-grid snap, one "
-                f"CUDA graph; the Adam steps change RD by {grad_db:+.4f} dB over the init round alone" if iso else
+    fit_desc = (f"gradient-refined batched fit over device-resident pools generated on the device (constant + "
+                f"linear, {n_cand} candidates): init round, {args.refine_steps} fused Adam steps (lr {args.refine_lr}) "
+                f"and the wire-grid snap, one CUDA graph (with the generation in the graph: fit_total); the Adam steps "
+                f"change RD by {grad_db:+.4f} dB over the init round alone" if iso else
                 "plain greedy fit (the refined fit missed iso RD)")
     details = {
         "plain": {"value": plain_value, "ms_per_step": plain_ms, "tiles_per_s": len(tiles) * world / (plain_ms * 1e-3),
@@ -1232,7 +1269,8 @@ def run_weft(args, world, rank, local, executor, cores):
                   "roofline_frac": frac(score_roof), "reseeds": fit.stats.reseeds},
         "iso_rd": {"plain_rd": plain_rd["rd_score"], "refined_rd": ref_rd["rd_score"], "delta_db": rd_delta,
                    "init_only_rd": init_rd["rd_score"], "adam_steps_db": grad_db, "tolerance_db": 0.05},
-        "fit_total": {"refined_device_gen_mpix_per_s": ref_value,
+        "fit_total": {"refined_device_gen_mpix_per_s": world * n_px / (total_ms * 1e-3) / 1e6,
+                      "refined_device_gen_ms": total_ms,
                       "refined_host_gen_mpix_per_s": world * n_px / (cl_gen_s + host_ref_ms * 1e-3) / 1e6,
                       "plain_host_gen_mpix_per_s": world * n_px / (gen_s + plain_ms * 1e-3) / 1e6,
                       "host_gen_s": {"constlin": cl_gen_s, "full": gen_s, "processes": cores},

@@ -86,6 +86,13 @@ typedef struct WeftFitState {
      * so its squared error is n q^2 - 2 q S1 + S2 — instead of per pixel (equal up to
      * rounding; a near tie may then pick differently from the per-pixel sum). */
     const double* moments;
+    /* Optional (NULL: off): the round's work queue.  With both set, every round first lists the
+     * scoring items whose tile is evaluated and whose slot run holds filled slots (per size class,
+     * any order), and the scoring launches are persistent grids of about one wave that pull those
+     * items, so late rounds with few live tiles and runs past a pool's filled slots cost no CTA
+     * launches.  queue: int32[n_items8 + n_items16 + n_items32]; queue_ctl: int32[8] scratch. */
+    int32_t* queue;
+    int32_t* queue_ctl;
 } WeftFitState;
 
 /* Fill d_moments (double[n_tiles * 6]) from the fit's tile pixels. */

@@ -173,3 +173,30 @@ def test_closed_form_init_matches_per_pixel_objectives():
     np.testing.assert_allclose(fit.objectives(), want_obj, rtol=1e-5)
     same = sum(a == b for a, b in zip(fit.selected_indices(), want_sel))
     assert same >= 0.95 * len(want_sel)
+
+
+def test_queue_driven_rounds_equal_per_item_launches():
+    """Persistent scoring launches that pull the round's live items from a queue give the same
+    fit as one CTA per item: selections, objectives and round decisions, host loop and graph."""
+    from weft_b200 import candidates, quadtree
+    from weft_b200.fit import BatchedFit
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 64, 3, 3)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    pools = [candidates.tile_candidates(p, 92) for p in patches]
+    a = BatchedFit(patches, pools, 92, caps=[16] * len(qts)).use_queue(False)
+    b = BatchedFit(patches, pools, 92, caps=[16] * len(qts))
+    a.run()
+    b.run()
+    assert a.stats.reseeds > 0
+    assert a.selected_indices() == b.selected_indices()
+    np.testing.assert_array_equal(a.objectives(), b.objectives())
+    assert a.stats.per_round == b.stats.per_round
+    b.reset()
+    g = b.graph()
+    g.replay()
+    assert b.selected_indices() == a.selected_indices()
+    np.testing.assert_array_equal(b.objectives(), a.objectives())

@@ -43,7 +43,8 @@ class WeftFitState(ctypes.Structure):
         (n, ctypes.c_void_p) for n in ("src", "bg", "px_off", "size", "cap", "pool_off", "pool_cnt", "pool_cap", "n_alive",
                                        "n_sel", "sel_bits", "flags", "cur_obj", "sel", "cand", "prep", "alive", "kind",
                                        "partial", "status", "work")] + [
-        ("variant", ctypes.c_int32 * 3), ("_pad", ctypes.c_int32), ("moments", ctypes.c_void_p)]
+        ("variant", ctypes.c_int32 * 3), ("_pad", ctypes.c_int32), ("moments", ctypes.c_void_p),
+        ("queue", ctypes.c_void_p), ("queue_ctl", ctypes.c_void_p)]
 
 FIT_VARIANTS = 3
 
@@ -74,7 +75,7 @@ DCT_TILE_DTYPE = np.dtype([("x", np.int32), ("y", np.int32), ("size", np.int32),
                            ("step_scale", np.float64), ("coef_base", np.int64, 3), ("coef_stride", np.int32, 3),
                            ("_pad2", np.int32)])
 assert DCT_TILE_DTYPE.itemsize == 64
-assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8 + 16 + 8
+assert ctypes.sizeof(WeftFitState) == 16 + 21 * 8 + 16 + 8 + 16
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int

@@ -18,6 +18,8 @@
 // order, so results are deterministic run to run).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <climits>
 #include <mutex>
 #include <string>
@@ -156,18 +158,25 @@ __global__ void fit_end_kernel(WeftFitState st, int mode, double complex_thresho
 // computed one per lane into the warp's segment table and read back the same way.
 constexpr int MAX_ITEM = 128;
 
-template <int PPL, int WPC, int MINB>
-__global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
-                                                        const WeftFitItem* __restrict__ items, int n_items,
-                                                        int expect_min, int expect_max, bool mode_init) {
+template <int WPC>
+struct ScoreSmem {
+    float4 prep[MAX_ITEM][4];
+    int slot[MAX_ITEM];
+    int wcount[4];
+    float4 seg[4][32][2];
+    float red[WPC > 1 ? MAX_ITEM : 1][WPC];
+};
+
+// One scoring work item (tile, 1024-pixel block, run of candidate slots) by the whole CTA.
+template <int PPL, int WPC>
+__device__ __forceinline__ void score_item(const WeftFitState& st, const int* __restrict__ perm, const WeftFitItem w,
+                                           int expect_min, int expect_max, bool mode_init, ScoreSmem<WPC>& sm) {
     constexpr int GROUPS = 4 / WPC;
-    __shared__ float4 s_prep[MAX_ITEM][4];
-    __shared__ int s_slot[MAX_ITEM];
-    __shared__ int s_wcount[4];
-    __shared__ float4 s_seg[4][32][2];
-    __shared__ float red[WPC > 1 ? MAX_ITEM : 1][WPC];
-    if ((int)blockIdx.x >= n_items) return;
-    const WeftFitItem w = items[blockIdx.x];
+    float4(&s_prep)[MAX_ITEM][4] = sm.prep;
+    int(&s_slot)[MAX_ITEM] = sm.slot;
+    int(&s_wcount)[4] = sm.wcount;
+    float4(&s_seg)[4][32][2] = sm.seg;
+    auto& red = sm.red;
     const int t = w.tile;
     if (t < 0 || t >= st.n_tiles) {
         if (threadIdx.x == 0) fit_report(WEFTK_E_ARG);
@@ -310,6 +319,57 @@ __global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, c
     // candidate-pixels of this CTA: every live candidate over its 1024-pixel block or whole tile
     if (st.work != nullptr && threadIdx.x == 0)
         atomicAdd(&st.work[0], (unsigned long long)m * (unsigned long long)(WPC * 32 * PPL));
+}
+
+// One CTA per work item of the class (every item of the round's size class is launched; items of
+// tiles that are not evaluated this round exit at once).
+template <int PPL, int WPC, int MINB>
+__global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, const int* __restrict__ perm,
+                                                        const WeftFitItem* __restrict__ items, int n_items,
+                                                        int expect_min, int expect_max, bool mode_init) {
+    __shared__ ScoreSmem<WPC> sm;
+    if ((int)blockIdx.x >= n_items) return;
+    score_item<PPL, WPC>(st, perm, items[blockIdx.x], expect_min, expect_max, mode_init, sm);
+}
+
+// Persistent form: a grid of about one wave of CTAs that pull the round's live items of the class
+// from the work queue fit_queue_kernel built (q_items[0..q_len)), one item per pull.
+template <int PPL, int WPC, int MINB>
+__global__ void __launch_bounds__(128, MINB) fit_score_queue_kernel(WeftFitState st, const int* __restrict__ perm,
+                                                              const WeftFitItem* __restrict__ items,
+                                                              const int32_t* __restrict__ q_items,
+                                                              const int32_t* q_len, int32_t* q_next, int expect_min,
+                                                              int expect_max, bool mode_init) {
+    __shared__ ScoreSmem<WPC> sm;
+    __shared__ int s_i;
+    for (;;) {
+        if (threadIdx.x == 0) s_i = atomicAdd(q_next, 1);
+        __syncthreads();
+        const int i = s_i;
+        if (i >= *q_len) break;
+        score_item<PPL, WPC>(st, perm, items[q_items[i]], expect_min, expect_max, mode_init, sm);
+        __syncthreads();  // the item's shared buffers are free before the next pull
+    }
+}
+
+// The round's work queue: per size class, the items whose tile is evaluated this round and whose
+// slot run starts inside the tile's filled slots (the others would exit at once), in any order
+// (items write disjoint scratch).  ctl[c] counts class c's queue, ctl[3 + c] is its pull counter.
+__global__ void fit_queue_kernel(WeftFitState st, const WeftFitItem* __restrict__ items8, int n8,
+                                 const WeftFitItem* __restrict__ items16, int n16,
+                                 const WeftFitItem* __restrict__ items32, int n32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n8 + n16 + n32) return;
+    const int c = i < n8 ? 0 : i < n8 + n16 ? 1 : 2;
+    const int j = c == 0 ? i : c == 1 ? i - n8 : i - n8 - n16;
+    const WeftFitItem w = (c == 0 ? items8 : c == 1 ? items16 : items32)[j];
+    if (w.tile < 0 || w.tile >= st.n_tiles) {
+        fit_report(WEFTK_E_ARG);
+        return;
+    }
+    if (!(st.flags[w.tile] & WEFTK_TILE_EVAL) || w.first >= st.pool_cnt[w.tile]) return;
+    const int base = c == 0 ? 0 : c == 1 ? n8 : n8 + n16;
+    st.queue[base + atomicAdd(&st.queue_ctl[c], 1)] = j;
 }
 
 // ------------------------------------------------------------------ select / accept
@@ -605,7 +665,7 @@ extern "C" int weftk_fit_round_static(const WeftFitState* st, int mode, double l
 // Scoring variants per size class.  A class's variants cover the same pixels per candidate pass
 // (64 for 8-px tiles, 256 for 16-px tiles, one 1024-pixel block for 32/64-px tiles) with a
 // different split over lanes and warps, or a different register budget.
-static_assert(sizeof(WeftFitState) == 208, "WeftFitState layout is part of the C ABI");
+static_assert(sizeof(WeftFitState) == 224, "WeftFitState layout is part of the C ABI");
 
 struct ScoreShape {
     int ppl, wpc, minb;
@@ -619,10 +679,23 @@ static const ScoreShape kShapes[3][WEFTK_FIT_VARIANTS] = {
 // mode of the round being enqueued (the class launchers' extra argument)
 static thread_local bool g_mode_init = false;
 
+// queue of the class being launched (set while weftk_fit_round enqueues a queue-driven round)
+static thread_local int g_queue_class = -1;
+static thread_local int g_queue_base = 0;
+static thread_local int g_sms = 148;
+
 template <int PPL, int WPC, int MINB>
 static void launch_score(const WeftFitState& st, const int* perm, const WeftFitItem* items, int n, int lo, int hi,
                          cudaStream_t s) {
-    fit_score_kernel<PPL, WPC, MINB><<<n, 128, 0, s>>>(st, perm, items, n, lo, hi, g_mode_init);
+    if (g_queue_class < 0) {
+        fit_score_kernel<PPL, WPC, MINB><<<n, 128, 0, s>>>(st, perm, items, n, lo, hi, g_mode_init);
+        return;
+    }
+    const int c = g_queue_class;
+    const int grid = std::min(n, g_sms * MINB);
+    fit_score_queue_kernel<PPL, WPC, MINB><<<grid, 128, 0, s>>>(st, perm, items, st.queue + g_queue_base,
+                                                                 st.queue_ctl + c, st.queue_ctl + 3 + c, lo, hi,
+                                                                 g_mode_init);
 }
 
 static void launch_score_class8(int v, const WeftFitState& st, const int* perm, const WeftFitItem* it, int n,
@@ -705,9 +778,33 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
         WEFTK_CUDA(cudaEventRecord(g_timing.start, s));
     }
     g_mode_init = mode == WEFTK_FIT_INIT;
-    if (n_items8) launch_score_class8(st->variant[0], *st, d_perm, d_items8, n_items8, s);
-    if (n_items16) launch_score_class16(st->variant[1], *st, d_perm, d_items16, n_items16, s);
-    if (n_items32) launch_score_class32(st->variant[2], *st, d_perm, d_items32, n_items32, s);
+    const bool queued = st->queue != nullptr && st->queue_ctl != nullptr;
+    if (queued) {
+        int dev = 0;
+        WEFTK_CUDA(cudaGetDevice(&dev));
+        WEFTK_CUDA(cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev));
+        WEFTK_CUDA(cudaMemsetAsync(st->queue_ctl, 0, 8 * sizeof(int32_t), s));
+        const int total = n_items8 + n_items16 + n_items32;
+        if (total > 0)
+            fit_queue_kernel<<<ceil_div(total, 256), 256, 0, s>>>(*st, d_items8, n_items8, d_items16, n_items16,
+                                                                  d_items32, n_items32);
+    }
+    if (n_items8) {
+        g_queue_class = queued ? 0 : -1;
+        g_queue_base = 0;
+        launch_score_class8(st->variant[0], *st, d_perm, d_items8, n_items8, s);
+    }
+    if (n_items16) {
+        g_queue_class = queued ? 1 : -1;
+        g_queue_base = n_items8;
+        launch_score_class16(st->variant[1], *st, d_perm, d_items16, n_items16, s);
+    }
+    if (n_items32) {
+        g_queue_class = queued ? 2 : -1;
+        g_queue_base = n_items8 + n_items16;
+        launch_score_class32(st->variant[2], *st, d_perm, d_items32, n_items32, s);
+    }
+    g_queue_class = -1;
     if (g_timing.enabled) {
         WEFTK_CUDA(cudaEventRecord(g_timing.stop, s));
         g_timing.pending = true;

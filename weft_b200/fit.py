@@ -312,6 +312,7 @@ class BatchedFit:
             items[cls] = rows[o].contiguous()
             self.n_items[cls] = int(rows.shape[0])
         self.t_items = items
+        self._alloc_queue()
 
     def _build_static_work(self) -> None:
         """Work that depends on the tile layout only, not on the pools' contents (which live on
@@ -343,6 +344,26 @@ class BatchedFit:
             items[cls] = torch.from_numpy(arr).to(d)
             self.n_items[cls] = len(arr)
         self.t_items = items
+        self._alloc_queue()
+
+    def _alloc_queue(self) -> None:
+        """The rounds' work queue (``WeftFitState.queue``): room for every item of the three size
+        classes, or off when ``use_queue(False)`` was set."""
+        if not getattr(self, "_queue_on", True):
+            self.st.queue = self.st.queue_ctl = None
+            return
+        total = max(1, sum(self.n_items.get(k, 0) for k in (8, 16, 32)))
+        if getattr(self, "t_queue", None) is None or self.t_queue.numel() < total:
+            self.t_queue = torch.empty(total, dtype=torch.int32, device=self.device)
+            self.t_queue_ctl = torch.zeros(8, dtype=torch.int32, device=self.device)
+        self.st.queue = _lib.ptr(self.t_queue)
+        self.st.queue_ctl = _lib.ptr(self.t_queue_ctl)
+
+    def use_queue(self, on: bool = True) -> "BatchedFit":
+        """Persistent queue-driven scoring launches (default) or one CTA per work item."""
+        self._queue_on = bool(on)
+        self._alloc_queue()
+        return self
 
     def _round(self, mode: int) -> tuple[int, int]:
         ti = self.t_items

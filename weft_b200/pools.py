@@ -175,7 +175,9 @@ class DeviceRefinedFit:
     (``RefinedFit.q_rows``: one row per tile)."""
 
     def __init__(self, src4: torch.Tensor, sizes, quality: int = 75, caps=None, steps: int = 10, lr: float = 1e-2,
-                 kinds=(0, 1), use_graph: bool = True, autotune: bool = True):
+                 kinds=(0, 1), use_graph: bool = True, autotune: bool = True, generate_in_run: bool = True):
+        """``generate_in_run=False`` generates the pools once here and leaves them resident: ``run()``
+        is then the fit alone over device-resident pools."""
         from .fit import BatchedFit
         from .refine import RefinedFit
 
@@ -193,10 +195,12 @@ class DeviceRefinedFit:
         self.fit = BatchedFit.from_device_pools(src4, self.sizes, self.cand, self.cnt, self.stride, quality, caps,
                                                 kinds_mask=mask)
         self.fit.use_closed_form_init(True)
-        if autotune:
+        if autotune or not generate_in_run:
             self.generate()  # the autotuner times scoring launches over real pools
+        if autotune:
             self.fit.autotune()
-        self.rf = RefinedFit(self.fit, steps=steps, lr=lr, use_graph=use_graph, prelude=self.generate)
+        self.rf = RefinedFit(self.fit, steps=steps, lr=lr, use_graph=use_graph,
+                             prelude=self.generate if generate_in_run else None)
 
     def generate(self) -> None:
         """Enqueue the pool generation (device work only)."""

@@ -799,9 +799,7 @@ def image_batch_fit(args, executor, local, stream):
     rows, ref_ms = timed(drf.run, 3)
     rss = drf.rf.ss
     ref_rd = batch.rd_per_image(rss.to_stacks(rss.quantize(drf.rf.refiner.p)))
-    init_rd = batch.rd_per_image(rss.to_stacks(rss.quantize(drf.rf.start)))
     deltas = [b["rd_score"] - a["rd_score"] for a, b in zip(plain_rd, ref_rd)]
-    adam = [b["rd_score"] - a["rd_score"] for a, b in zip(init_rd, ref_rd)]
     per_image = [{"side": im.size[0], "plain_rd": a["rd_score"], "refined_rd": b["rd_score"]}
                  for im, a, b in zip(ims, plain_rd, ref_rd)]
     return {"images": args.batch_images, "n_images": len(ims), "mpix": n_px / 1e6, "tiles": int(batch.tile_off[-1]),
@@ -810,8 +808,7 @@ def image_batch_fit(args, executor, local, stream):
             "refined": f"pools generated on the device (constant + linear), init round + {args.batch_steps} fused "
                        f"Adam steps + wire-grid snap, one CUDA graph over every tile of every image",
             "rd_delta_db_min": min(deltas), "rd_delta_db_mean": float(np.mean(deltas)),
-            "images_within_0.05db": int(sum(d >= -0.05 for d in deltas)),
-            "adam_steps_db_mean": float(np.mean(adam)), "per_image": per_image}
+            "images_within_0.05db": int(sum(d >= -0.05 for d in deltas)), "per_image": per_image}
 
 
 def _hbm_peak() -> tuple[float, str]:
@@ -1279,6 +1276,9 @@ def run_weft(args, world, rank, local, executor, cores):
                    "raster_resize_frac": frac((raster_line or {}).get("resize")),
                    "ms": None if not decode else round(decode["ms"], 4)},
         "parity": None if parity is None else {k: parity[k] for k in ("tiles", "equal_selections", "max_obj_rel")},
+        "image_batch": None if ibatch is None else {k: ibatch[k] for k in (
+            "n_images", "mpix", "plain_mpix_per_s", "refined_mpix_per_s", "rd_delta_db_min", "rd_delta_db_mean",
+            "images_within_0.05db")},
         "details": "the full record is the bench_details JSON line on stderr",
     }
     print(json.dumps(line), flush=True)

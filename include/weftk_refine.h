@@ -57,6 +57,12 @@ typedef struct WeftStackSet {
      * per tile whose mask is within {constant, linear} run a register-only kernel; a row of
      * another kind is then reported (WEFTK_E_ARG in the device status) and treated as absent. */
     int32_t kinds_mask;
+    /* Optional (NULL: off): per-tile pixel sums, double[n_tiles * 6] = sum of src r, g, b and of
+     * their squares (the fit's weftk_fit_moments).  With the register path, a tile whose stack is
+     * one constant layer then runs as one thread: over black such a layer renders one colour q
+     * per channel, so its loss n q^2 - 2 q S1 + S2 and its gradient n q - S1 per channel need no
+     * pixel loop (no residual loss). */
+    const double* moments;
 } WeftStackSet;
 
 /* loss[t] for every tile (float32). */

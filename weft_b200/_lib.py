@@ -54,7 +54,7 @@ class WeftStackSet(ctypes.Structure):
     _fields_ = [("n_tiles", ctypes.c_int32), ("max_prims", ctypes.c_int32)] + [
         (n, ctypes.c_void_p) for n in ("src", "px_off", "size", "prim_off", "kind", "order")] + [
         ("n_big", ctypes.c_int32), ("n_mid", ctypes.c_int32), ("n_s16", ctypes.c_int32),
-        ("kinds_mask", ctypes.c_int32)]
+        ("kinds_mask", ctypes.c_int32), ("moments", ctypes.c_void_p)]
 
 
 # numpy mirrors of the C structs (same byte layout)

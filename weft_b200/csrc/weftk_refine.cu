@@ -454,6 +454,33 @@ __device__ __forceinline__ void grad_cl(const Prep& P, const float* r, const ClE
 // One kernel for the loss (MODE 0), loss + gradient (MODE 1), and loss + gradient +
 // Adam step on the tile's own rows (MODE 2: params are updated in place; a group reads
 // its rows once at staging and writes them once at the end, and rows belong to one tile).
+// Loss sum and colour / alpha gradient of a lone constant layer over black from the tile's pixel
+// sums S = (S1 r, g, b, S2 r, g, b) over n pixels: the layer renders q = colour * alpha per
+// channel, so sum (q - s)^2 = n q^2 - 2 q S1 + S2 and sum (q - s) = n q - S1.  g4 (may be null):
+// d/dcolour0 (3) and d/dalpha, scaled by gscale.  Every float64 operation is rounded on its own,
+// so both kernels that use it agree bit for bit.
+__device__ __forceinline__ double const_layer_closed(const Prep& P, float alpha_raw, const double* S, int n,
+                                                     float gscale, float* g4) {
+    const float sv[3] = {P.cr, P.cg, P.cb};
+    const double nd = (double)n;
+    double tot = 0.0, galpha = 0.0;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        const float c = __fmul_rn(sv[ch], P.a);  // blend over black: colour * alpha
+        const double cc = (double)clamp01(c);
+        const double e = __dadd_rn(__dsub_rn(__dmul_rn(__dmul_rn(nd, cc), cc), __dmul_rn(__dmul_rn(2.0, cc), S[ch])),
+                                   S[3 + ch]);
+        tot = __dadd_rn(tot, e);
+        const float G = (c >= 0.0f && c <= 1.0f)
+                            ? (float)__dmul_rn((double)gscale, __dsub_rn(__dmul_rn(nd, (double)c), S[ch]))
+                            : 0.0f;
+        if (g4) g4[ch] = __fmul_rn(G, P.a);
+        galpha = __dadd_rn(galpha, (double)__fmul_rn(G, sv[ch]));
+    }
+    if (g4) g4[3] = (alpha_raw >= 0.0f && alpha_raw <= 1.0f) ? (float)galpha : 0.0f;
+    return tot;
+}
+
 constexpr int RF_LOSS = 0, RF_GRAD = 1, RF_STEP = 2;
 
 // CL1: every stack has at most one layer, of kind constant or linear (checked per tile): the
@@ -508,6 +535,8 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
         }
         return;
     }
+    // a lone constant layer runs in refine_const_kernel when the tiles' pixel sums are given
+    if (CL1 && !resid && set.moments != nullptr && K == 1 && set.kind[p0] == K_CONST) return;
     const int gt = wig * 32 + lane, GT = wpt * 32;
 
     // ---- stage the layers (rows, and for STEP the Adam moments, stay in shared memory
@@ -623,23 +652,9 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
         }
     }
     const double* S12 = mom + wpt * 6;
-    // loss (and, with gscale != 0, the colour / alpha gradient into g4) of the lone constant layer
+    // loss (and, with g4, the colour / alpha gradient) of the lone constant layer
     auto const_closed = [&](float gscale, float* g4) -> double {
-        const Prep& P = prep[0];
-        const float sv[3] = {P.cr, P.cg, P.cb};
-        const double nd = (double)n;
-        double tot = 0.0, galpha = 0.0;
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-            const float c = __fmul_rn(sv[ch], P.a);  // blend over black: colour * alpha
-            const double cc = (double)clamp01(c);
-            tot += nd * cc * cc - 2.0 * cc * S12[ch] + S12[3 + ch];
-            const float G = (c >= 0.0f && c <= 1.0f) ? (float)((double)gscale * (nd * (double)c - S12[ch])) : 0.0f;
-            if (g4) g4[ch] = G * P.a;
-            galpha += (double)(G * sv[ch]);
-        }
-        if (g4) g4[3] = (raw[0][13] >= 0.0f && raw[0][13] <= 1.0f) ? (float)galpha : 0.0f;
-        return tot;
+        return const_layer_closed(prep[0], raw[0][13], S12, n, gscale, g4);
     };
 
     double sse = 0.0;
@@ -939,6 +954,69 @@ __global__ void __launch_bounds__(RF_THREADS, 3)
     }
 }
 
+// One thread per tile whose stack is one constant layer (register path, primitives-only loss,
+// the tiles' pixel sums given): the same arithmetic as refine_tiles_kernel's closed form for such a
+// tile — loss n q^2 - 2 q S1 + S2 and gradient from n q - S1 per channel, Adam with projection on
+// the row's colour and alpha (its other columns have zero gradient and stay where they are), the
+// row's step count and bias corrections as the group path keeps them.
+template <int MODE>
+__global__ void __launch_bounds__(128) refine_const_kernel(WeftStackSet set, float* __restrict__ params,
+                                                           const float* __restrict__ grad_loss,
+                                                           float* __restrict__ grad, float* __restrict__ loss,
+                                                           AdamArgs adam, int n_steps) {
+    constexpr bool BWD = MODE != RF_LOSS;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= set.n_tiles) return;
+    const int p0 = set.prim_off[t];
+    if (set.prim_off[t + 1] - p0 != 1 || set.kind[p0] != K_CONST) return;
+    const int ts = set.size[t];
+    if (ts < 1 || ts > 64) return;  // reported by refine_tiles_kernel
+    const int n = ts * ts;
+    double S[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) S[i] = set.moments[(size_t)t * 6 + i];
+    float* row = params + (size_t)p0 * 16;
+    float r[16], m[16], v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        r[i] = row[i];
+        m[i] = MODE == RF_STEP ? adam.m[(size_t)p0 * 16 + i] : 0.0f;
+        v[i] = MODE == RF_STEP ? adam.v[(size_t)p0 * 16 + i] : 0.0f;
+    }
+    const float scale = BWD ? grad_loss[t] * 2.0f / (3.0f * (float)n) : 0.0f;
+    double sse = 0.0;
+    float g4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int step = 0; step < n_steps; ++step) {
+        const Prep P = prep_prim(row_to_prim(r, K_CONST));
+        const double tot = const_layer_closed(P, r[13], S, n, scale, g4);
+        sse = tot;
+        if (MODE == RF_STEP) {
+            adam_bias(adam.b1, adam.b2, m[15] + 1.0f, m[14], v[14]);
+#pragma unroll
+            for (int j = 0; j < 14; ++j) {
+                const float gj = j >= 7 && j <= 9 ? g4[j - 7] : j == 13 ? g4[3] : 0.0f;
+                r[j] = adam_update_bc(r[j], gj, m[j], v[j], m[14], v[14], adam.lr, adam.b1, adam.b2, adam.eps,
+                                     K_CONST, j);
+            }
+            m[15] += 1.0f;
+        }
+    }
+    if (BWD && grad) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+            grad[(size_t)p0 * 16 + j] = j >= 7 && j <= 9 ? g4[j - 7] : j == 13 ? g4[3] : 0.0f;
+    }
+    if (MODE == RF_STEP) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            row[i] = r[i];
+            adam.m[(size_t)p0 * 16 + i] = i == 14 ? 0.0f : m[i];
+            adam.v[(size_t)p0 * 16 + i] = i == 14 ? 0.0f : v[i];
+        }
+    }
+    if (loss != nullptr) loss[t] = (float)(sse / (3.0 * n));
+}
+
 template <int MODE>
 static int launch_refine(const WeftStackSet& set, float* params, const float* grad_loss, float* grad, float* loss,
                          int flags, AdamArgs adam, cudaStream_t stream, const char* what, int n_steps = 1) {
@@ -995,6 +1073,9 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
             have = smem;
         }
     }
+    if (cl1 && set.moments != nullptr && !(flags & WEFTK_LOSS_RESIDUAL))
+        refine_const_kernel<MODE><<<(set.n_tiles + 127) / 128, 128, 0, stream>>>(set, params, grad_loss, grad, loss,
+                                                                                  adam, n_steps);
     if (cl1)
         refine_tiles_kernel<MODE, true><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags,
                                                                             plan, L, adam, n_steps);

@@ -708,7 +708,8 @@ class BatchedFit:
         params[:, 7:10] = f[:, 8:11]
         params[:, 10:13] = f[:, 11:14]
         params[:, 13] = f[:, 14]
-        ss = StackSet(self.t_src, self.t_px_off, self.t_size, prim_off, kinds.cpu().numpy(), self.device.index or 0)
+        ss = StackSet(self.t_src, self.t_px_off, self.t_size, prim_off, kinds.cpu().numpy(), self.device.index or 0,
+                      moments=self.t_moments if self.st.moments else None)
         return ss, params
 
     def objectives(self) -> np.ndarray:

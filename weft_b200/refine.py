@@ -53,11 +53,14 @@ class StackSet:
     """Per-tile stacks over tile pixels resident on the GPU."""
 
     def __init__(self, src: torch.Tensor, px_off: torch.Tensor, sizes: torch.Tensor, prim_off: np.ndarray,
-                 kinds, device: int = 0, kinds_mask: int | None = None, sizes_host: np.ndarray | None = None):
+                 kinds, device: int = 0, kinds_mask: int | None = None, sizes_host: np.ndarray | None = None,
+                 moments: torch.Tensor | None = None):
         """``kinds``: per-row primitive kinds, a numpy array or a device int32 tensor (kept by reference).
         ``kinds_mask`` (bit k = kind k may occur) is derived from a numpy ``kinds``; pass it with a
         device tensor whose contents change later.  ``sizes_host``: the tile sides on the host, when
-        the caller has them (saves reading ``sizes`` back)."""
+        the caller has them (saves reading ``sizes`` back).  ``moments``: the tiles' pixel sums
+        (``WeftStackSet.moments``, double[n_tiles * 6]) for the one-thread path of lone constant
+        layers, or None."""
         self.device = torch.device("cuda", device)
         self.lib = _lib.lib_for_device(device)
         self.n = int(sizes.numel())
@@ -84,7 +87,8 @@ class StackSet:
         n_big, n_mid, n_s16 = (int(c.sum()) for c in classes[:3])
         self.st = _lib.WeftStackSet(self.n, self.max_prims, _lib.ptr(src), _lib.ptr(px_off), _lib.ptr(sizes),
                                     _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind), _lib.ptr(self.t_order),
-                                    n_big, n_mid, n_s16, int(kinds_mask or 0))
+                                    n_big, n_mid, n_s16, int(kinds_mask or 0), _lib.ptr(moments))
+        self._moments = moments
         n_px = (sizes.to(torch.int64) ** 2)
         total = float((sz.astype(np.int64) ** 2).sum())
         self.weights = (n_px.to(torch.float32) / total) if self.n else n_px.float()
@@ -334,7 +338,7 @@ class RefinedFit:
         self.kinds = torch.zeros(n_rows, dtype=torch.int32, device=dev)
         mask = fit.init_kinds_mask()
         self.ss = StackSet(fit.t_src, fit.t_px_off, fit.t_size, prim_off, self.kinds, dev.index or 0, kinds_mask=mask,
-                           sizes_host=fit.sizes)
+                           sizes_host=fit.sizes, moments=fit.t_moments if fit.st.moments else None)
         self.refiner = FusedRefiner(self.ss, torch.zeros((n_rows, 16), dtype=torch.float32, device=dev), lr=lr,
                                     residual=residual)
         self.steps = int(steps)

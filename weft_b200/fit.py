@@ -321,8 +321,11 @@ class BatchedFit:
         blocks, largest tiles first.  Runs past a tile's filled slots end at once."""
         d = self.device
         cap = self.pool_cap.astype(np.int64)
-        local = np.arange(self.n_slots, dtype=np.int64) - np.repeat(self.pool_off, cap)
-        self.t_perm = torch.from_numpy(local.astype(np.int32)).to(d)
+        if self.n and np.all(cap == cap[0]):  # uniform stride: the identity order on the device
+            self.t_perm = torch.remainder(torch.arange(self.n_slots, dtype=torch.int32, device=d), int(cap[0]))
+        else:
+            local = np.arange(self.n_slots, dtype=np.int64) - np.repeat(self.pool_off, cap)
+            self.t_perm = torch.from_numpy(local.astype(np.int32)).to(d)
         items = {}
         for cls, members in ((8, (8,)), (16, (16,)), (32, (32, 64))):
             chunk = self.chunk[cls]

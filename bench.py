@@ -1069,21 +1069,26 @@ def run_weft(args, world, rank, local, executor, cores):
         return (int(pixels.nbytes + records.nbytes + 4 * 6 * f2.n),
                 int(q_rows.numel() * 4 + q_kind.numel() * 4 + 16 * len(f2.stats.per_round)))
 
+    e2e_wall = {}
+
     def timed_e2e(fn):
-        ms, io = [], (0, 0)
+        ms, wall, io = [], [], (0, 0)
         if args.e2e_steps > 0:
             for _ in range(args.warmup):  # untimed, like the device-timed steps
                 fn()
         for _ in range(args.e2e_steps):
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
             a.record(stream)
             io = fn()
             b.record(stream)
             torch.cuda.synchronize()
+            wall.append((time.perf_counter() - t0) * 1e3)
             ms.append(a.elapsed_time(b))
         if not ms:
             return None, io
+        e2e_wall[fn.__name__] = {"event_ms": ms, "host_wall_ms": wall}
         return world * n_px / (max_over_ranks(statistics.mean(ms), world) * 1e-3) / 1e6, io
 
     plain_e2e_val, (p_h2d, p_d2h) = timed_e2e(plain_e2e)
@@ -1153,6 +1158,11 @@ def run_weft(args, world, rank, local, executor, cores):
 
     ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
     tiles_e2e_val, _ = timed_e2e(tiles_e2e)
+    # where the end-to-end time goes: one more call, synchronised between its phases (untimed)
+    from weft_b200.frontend import refine_image
+
+    e2e_phases: dict = {}
+    refine_image(u8_h, QUALITY, CAP, steps=args.refine_steps, lr=args.refine_lr, device=local, timings=e2e_phases)
 
     diff = differentiable_fit(args, executor, local, stream) if args.diff_steps > 0 and rank == 0 else None
     ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None
@@ -1232,7 +1242,8 @@ def run_weft(args, world, rank, local, executor, cores):
                                         for k, v in (drf.fit.tuning or {}).items()},
                            "pools_equal_host": [pools_equal, len(tiles)], "candidates": n_cand,
                            "e2e_from_tile_pixels": tiles_e2e_val,
-                           "e2e": "frontend.refine_image from the sRGB u8 image in page-locked memory"},
+                           "e2e": "frontend.refine_image from the sRGB u8 image in page-locked memory",
+                           "e2e_steps": e2e_wall, "e2e_phases_ms": e2e_phases},
         "refined_host_pools": {"ms": host_ref_ms, "mpix_per_s": world * n_px / (host_ref_ms * 1e-3) / 1e6,
                                "rd": host_ref_rd, "candidates": int(len(frec)),
                                "score_ms": r_score_ms, "refine_ms_per_step": r_step_ms,

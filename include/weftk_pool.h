@@ -43,6 +43,10 @@ extern "C" {
 
 #define WEFTK_POOL_MAX_SPECS 52            /* template split lines: n_ang (<= 16) + 36 */
 #define WEFTK_POOL_MAX_CONST_LINEAR 272    /* candidates per tile before de-duplication, bound */
+#define WEFTK_POOL_SPLITS (16 + WEFTK_POOL_MAX_SPECS)  /* split lines per tile side: 16 orientations,
+                                                          then the template lines */
+/* side-bit words of all four tile sides: WEFTK_POOL_SPLITS x (8^2 + 16^2 + 32^2 + 64^2) / 32 */
+#define WEFTK_POOL_SIDE_WORDS (WEFTK_POOL_SPLITS * 170)
 
 /* Host-built tables (device pointers), per tile side 8, 16, 32, 64 (index 0..3). */
 typedef struct WeftPoolTables {
@@ -56,6 +60,11 @@ typedef struct WeftPoolTables {
     const float* orient_mask;  /* [4][16][4] side test coefficients of the centre lines */
     const double* bin_edges;   /* [13] orientation histogram bin edges (np.linspace(0, pi, 13)) */
     const int32_t* cuts;       /* [4][3][5] palette run boundaries for 2, 3, 4 runs */
+    const uint32_t* side_bits; /* the side test of every split line over its tile's pixel grid:
+                                  per side (8, 16, 32, 64 in turn) WEFTK_POOL_SPLITS rows (the 16
+                                  orientations' centre lines, then the template lines) of
+                                  side^2 / 32 words, bit p % 32 of word p / 32 set when raster
+                                  pixel p is on side a; filled by weftk_pool_side_bits */
     int32_t n_spec;            /* template split lines (n_ang + 36) */
     int32_t n_centre;          /* the first n_centre of them are centre lines */
 } WeftPoolTables;
@@ -72,6 +81,11 @@ typedef struct WeftPoolJob {
     const int32_t* tiles[4];   /* indices of the tiles of side 8, 16, 32, 64 */
     int32_t n_tiles[4];
 } WeftPoolJob;
+
+/* Fill d_bits (WEFTK_POOL_SIDE_WORDS words, device) with the side test of tables->spec_mask
+ * and tables->orient_mask over each tile side's pixel grid (the layout of
+ * WeftPoolTables.side_bits; tables->side_bits itself is not read).  Once per table, on `stream`. */
+int weftk_pool_side_bits(const WeftPoolTables* tables, uint32_t* d_bits, void* stream);
 
 /* Generate the constant and linear candidates of every listed tile (one launch per tile
  * side, asynchronous on `stream`).  A tile whose pool would not fit pool_cap is truncated and

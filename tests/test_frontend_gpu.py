@@ -47,3 +47,26 @@ def test_refine_image_equals_the_fit_over_host_tiles():
     assert [tuple(r) for r in tiles.tolist()] == [(t.x, t.y, t.size) for t in qts]
     np.testing.assert_array_equal(rows, rows_h)
     np.testing.assert_array_equal(kinds, kinds_h)
+
+
+def test_refine_image_releases_its_device_memory_at_return():
+    """No reference cycle holds the fit's buffers after the call (the caching allocator gets
+    them back at once, with the cycle collector off)."""
+    import gc
+
+    from weft_b200 import frontend
+    from weft_b200.synth import make_image_u8
+
+    u8 = make_image_u8(256, 256, 30, 2)
+    frontend.refine_image(u8, 75, 16, steps=3)  # tables, lookup tables, streams
+    torch.cuda.synchronize()
+    gc.collect()
+    base = torch.cuda.memory_allocated()
+    gc.disable()
+    try:
+        for _ in range(3):
+            frontend.refine_image(u8, 75, 16, steps=3)
+        torch.cuda.synchronize()
+        assert torch.cuda.memory_allocated() == base
+    finally:
+        gc.enable()

@@ -152,3 +152,26 @@ def test_device_refined_fit_graph_replays_and_matches_host_pools():
     rf = RefinedFit(hf, steps=4, lr=1e-2, use_graph=False)
     rf.run()
     assert torch.equal(a, rf.q_rows)
+
+
+@pytest.mark.parametrize("quality", [75, 92])
+def test_side_bit_table_matches_the_host_side_tests(quality):
+    """The device's side-bit table against the split tests of ``candidates`` (the orientation
+    lines with Python-float endpoints on the float32 grid, the template lines as float32)."""
+    from weft_b200 import pools
+    from weft_b200.candidates import _int_grid
+
+    tb = pools.PoolTables(quality, 0)
+    for s in pools.SIDES:
+        got = tb.side_masks(s)
+        ys, xs = _int_grid(s, s)
+        for oi, th in enumerate(pools.orientation_angles()):
+            x0, y0, x1, y1 = pools.orientation_lines(s, th)[0]
+            want = (xs - x0) * (y1 - y0) - (ys - y0) * (x1 - x0) >= 0
+            assert np.array_equal(got[oi], want), (s, oi)
+        specs, _ = pools.template_specs(s, quality)
+        lines = np.array([sp[:4] for sp in specs], dtype=np.float32)
+        for k, (x0, y0, x1, y1) in enumerate(lines):
+            want = (xs - x0) * (y1 - y0) - (ys - y0) * (x1 - x0) >= 0
+            assert np.array_equal(got[16 + k], want), (s, k)
+        assert not got[16 + len(specs):].any()

@@ -116,6 +116,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_raster_resize": [_P, _I, _I, _P, _I, _I, _P, _P],
     "weftk_quantize_rows": [_P, _P, _I, _P, _P],
     "weftk_fit_selected_rows": [_P, _P, _P, _P],
+    "weftk_pool_side_bits": [_P, _P, _P],
     "weftk_gen_pools": [_P, _P, _P],
     "weftk_quadtree_work_bytes": [_I, _I, _I, _I, _P],
     "weftk_quadtree_variance": [_P, _I, _I, ctypes.c_double, _I, _I, _P, _I, _P, _P, _P],

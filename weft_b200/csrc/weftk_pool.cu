@@ -12,10 +12,15 @@
 //      percentiles; the np.gradient magnitude and its 75th percentile;
 //   5. every mean the two generators take, as numpy computes it: a sequential float32 sum per
 //      channel in the reference's pixel order (raster, or luminance order for palette runs),
-//      divided by the count in float32 — one thread per (region, channel);
-//   6. the candidate list in the reference's order (one thread), the coarse de-duplication
-//      key of every candidate, first occurrences kept (one thread per candidate), and the
-//      surviving records written to the tile's slots.
+//      divided by the count in float32 — one thread per region or split line (both of its
+//      sides in one pass over the pixels, the side test read from a table built once per
+//      quality), over all three channels for tiles up to 16 px and one channel above; each
+//      sum divided by its count in float32 there, once per region;
+//   6. the palettes (the colours' pairwise near tests in parallel, the keep walk on one
+//      thread) and the candidate list's segments;
+//   7. the coarse de-duplication key of every candidate, first occurrences kept through a
+//      shared-memory hash table (lowest index per key), and the surviving records written to
+//      the tile's slots.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -25,6 +30,8 @@
 #include "../../include/weftk_pool.h"
 #include "weftk_common.cuh"
 
+static_assert(sizeof(WeftPoolTables) == 64, "WeftPoolTables layout is part of the C ABI");
+
 namespace weftk {
 
 extern __device__ int g_device_status;
@@ -33,36 +40,45 @@ namespace {
 
 constexpr int NB = 12;                           // orientation histogram bins
 constexpr int MAXC = WEFTK_POOL_MAX_CONST_LINEAR;
-constexpr int MAXR = 33 + 2 * NB + 2 * WEFTK_POOL_MAX_SPECS;  // regions whose means are taken
+constexpr int NSPL = WEFTK_POOL_SPLITS;          // split rows per tile side in the side-bit table
+constexpr int NFIX = 33;                         // fixed regions (below)
 constexpr int MAXPAL = 16;
+constexpr int NCOL = 13;                         // palette colours tested: tile mean + regions 21..32
 constexpr int KEYS = 12;
+constexpr int HT = 512;                          // de-duplication hash table slots (> 2 * MAXC)
 
-enum : int { RG_ALL, RG_RECT, RG_RUN, RG_LUM_GT, RG_LUM_LT, RG_MAGT_GE, RG_SIDE_A, RG_SIDE_B };
-
-struct Region {
-    int type;
-    int a, b, c, d;  // rect rows [a, b) x cols [c, d); run [a, b) of the luminance order
-    float4 coef;     // threshold in x; side test coefficients x0, y0, y1 - y0, x1 - x0
-};
+// Fixed regions whose means are taken: 0 the tile, 1..4 its quadrants, 5..20 its 4x4 blocks
+// (row-major), 21..29 the palette runs of the luminance order (2, 3 and 4 equal runs), 30
+// luminance above its 75th percentile, 31 below its 25th, 32 np.gradient magnitude at or above
+// its 75th.  Split lines (both sides) are kept apart: the dominant orientations' centre lines,
+// then the template lines.
 
 // per-tile scratch besides the pixel planes (static part of the shared memory)
 struct Scratch {
-    Region reg[MAXR];
-    float rsum[MAXR][3];
-    int rcnt[MAXR];
-    int n_reg;
+    float rmean[NFIX][3];     // sum / count in float32 (0 for an empty region)
+    int rcnt[NFIX];
+    float smean[NSPL][2][3];  // per split line in use: side a, side b (0 for an empty side)
+    int scnt[NSPL];           // pixels on side a
+    double edges[NB + 1];
     float hist[NB];
     int bin_start[NB + 1];
     int peaks[NB];
-    int n_peaks;
+    int n_peaks, n_split;
     float p25, p75, pm75;
+    unsigned tmask[3][128];  // pixels above the 75th / below the 25th luminance percentile, gradient >= its 75th
     // palettes (the template palette extends the edge palette) and the candidate list's segments
+    float cpal[NCOL][3];
+    unsigned near_mask[NCOL];
     float pal[MAXPAL][3];
     int npal_e, npal_t;
     int seg[8];
     int n_cand;
     unsigned long long hash[MAXC];
-    int keep[MAXC];
+    unsigned long long klo[MAXC], khi[MAXC];
+    unsigned long long ht_hash[HT];
+    int ht_idx[HT];
+    unsigned keepw[(MAXC + 31) / 32];
+    int keep_pre[(MAXC + 31) / 32];
     int n_out;
     int wcnt[16][NB];
 };
@@ -71,30 +87,95 @@ __device__ __forceinline__ float clamp01(float v) { return fmaxf(0.0f, fminf(1.0
 
 // numpy's pairwise float32 summation of x[0..n) (the contiguous add-reduce loop: fewer than 8
 // sequentially, up to 128 with 8 accumulators combined pairwise, larger halves split at a
-// multiple of 8), each addition rounded on its own.
-__device__ float pairwise_sum(const float* x, int n) {
+// multiple of 8), each addition rounded on its own.  The split tree is walked with an explicit
+// stack (no recursion, so the kernel's stack size stays static): depth 6 covers n <= 8192.
+__device__ float pairwise_block(const float* x, int n) {
     if (n < 8) {
         float r = -0.0f;
         for (int i = 0; i < n; ++i) r = __fadd_rn(r, x[i]);
         return r;
     }
-    if (n <= 128) {
-        float r[8];
+    float r[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) r[j] = x[j];
-        int i = 8;
-        for (; i < n - (n % 8); i += 8) {
+    for (int j = 0; j < 8; ++j) r[j] = x[j];
+    int i = 8;
+    for (; i < n - (n % 8); i += 8) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], x[i + j]);
-        }
-        float res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
-                              __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
-        for (; i < n; ++i) res = __fadd_rn(res, x[i]);
-        return res;
+        for (int j = 0; j < 8; ++j) r[j] = __fadd_rn(r[j], x[i + j]);
     }
-    int n2 = n / 2;
-    n2 -= n2 % 8;
-    return __fadd_rn(pairwise_sum(x, n2), pairwise_sum(x + n2, n - n2));
+    float res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                          __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+    for (; i < n; ++i) res = __fadd_rn(res, x[i]);
+    return res;
+}
+
+// numpy's split tree over n elements, post-order: leaf(off, len) gives a leaf's sum (len <= 128),
+// the two halves of an inner node are added left + right
+template <class Leaf>
+__device__ float pairwise_tree(int n, Leaf leaf) {
+    constexpr int DEPTH = 8;
+    int off[DEPTH], len[DEPTH], state[DEPTH];
+    float left[DEPTH];
+    int sp = 0;
+    off[0] = 0;
+    len[0] = n;
+    state[0] = 0;
+    float ret = 0.0f;
+    while (sp >= 0) {
+        const int m = len[sp];
+        if (m <= 128 || sp == DEPTH - 1) {  // a leaf (n <= 8192 never reaches the depth bound)
+            ret = leaf(off[sp], m);
+            --sp;
+            continue;
+        }
+        int m2 = m / 2;
+        m2 -= m2 % 8;
+        if (state[sp] == 0) {  // left half first
+            state[sp] = 1;
+            off[sp + 1] = off[sp];
+            len[sp + 1] = m2;
+            state[sp + 1] = 0;
+            ++sp;
+        } else if (state[sp] == 1) {  // then the right half
+            left[sp] = ret;
+            state[sp] = 2;
+            off[sp + 1] = off[sp] + m2;
+            len[sp + 1] = m - m2;
+            state[sp + 1] = 0;
+            ++sp;
+        } else {
+            ret = __fadd_rn(left[sp], ret);
+            --sp;
+        }
+    }
+    return ret;
+}
+
+__device__ float pairwise_sum(const float* x, int n) {
+    return pairwise_tree(n, [&](int o, int m) { return pairwise_block(x + o, m); });
+}
+
+// the same sum by a whole warp (every lane gets it): the tree's leaves listed in order in lw
+// (3 * cap words: offsets, lengths, sums; cap >= the leaf count), summed by the lanes in
+// parallel, then the tree combined in numpy's order
+__device__ float warp_pairwise_sum(const float* x, int n, int* lw, int cap, int lane) {
+    int nl = 0;
+    pairwise_tree(n, [&](int o, int m) {
+        if (lane == 0) {
+            lw[nl] = o;
+            lw[cap + nl] = m;
+        }
+        ++nl;
+        return 0.0f;
+    });
+    __syncwarp();
+    float* sums = reinterpret_cast<float*>(lw + 2 * cap);
+    for (int k = lane; k < nl; k += 32) sums[k] = pairwise_block(x + lw[k], lw[cap + k]);
+    __syncwarp();
+    int k = 0;
+    const float r = pairwise_tree(n, [&](int, int) { return sums[k++]; });
+    __syncwarp();
+    return r;
 }
 
 // numpy's linear percentile of sorted float32 values (the whole computation in float32:
@@ -118,16 +199,13 @@ __device__ __forceinline__ bool side_a(float4 c, int x, int y) {
 }
 
 // sum over (a - b)^2 < 0.002 in float64, as the reference's palette test (Python floats)
-__device__ bool near_any(const float* c, const float (*pal)[3], int n) {
-    for (int i = 0; i < n; ++i) {
-        double s = 0.0;
-        for (int k = 0; k < 3; ++k) {
-            const double d = __dsub_rn((double)c[k], (double)pal[i][k]);
-            s = __dadd_rn(s, __dmul_rn(d, d));
-        }
-        if (s < 0.002) return true;
+__device__ bool near_pair(const float* c, const float* p) {
+    double s = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const double d = __dsub_rn((double)c[k], (double)p[k]);
+        s = __dadd_rn(s, __dmul_rn(d, d));
     }
-    return false;
+    return s < 0.002;
 }
 
 __device__ __forceinline__ int qkey(double v, double s) { return (int)(long long)__dadd_rn(__dmul_rn(v, s), 0.5); }
@@ -139,10 +217,48 @@ __host__ __device__ constexpr size_t pool_smem_bytes(int n) {
     return (size_t)n * (POOL_FLOAT_PLANES * sizeof(float) + sizeof(int) + sizeof(uint8_t));
 }
 
+// words of the side-bit table before tile side TS (8, 16, 32, 64), per split row
+template <int TS>
+__host__ __device__ constexpr int side_words_before() {
+    return TS == 8 ? 0 : TS == 16 ? 2 : TS == 32 ? 10 : 42;
+}
+
+// run [a, b) of the luminance order behind palette region r (21..29: 2, 3 and 4 equal runs)
+__device__ __forceinline__ void run_bounds(const int32_t* cuts, int si, int r, int& a, int& b) {
+    const int j = r - 21;
+    const int k = j < 2 ? 0 : j < 5 ? 1 : 2;
+    const int jj = j - (k == 0 ? 0 : k == 1 ? 2 : 5);
+    const int32_t* cut = cuts + (si * 3 + k) * 5;
+    a = cut[jj];
+    b = cut[jj + 1];
+}
+
+// the 12 key fields packed into 123 bits when each lies in its field's range (kind 1 bit, alpha
+// 6, geometry 11 each, colours 12 each, signed by offset); bit 63 of hi marks a key that does
+// not pack, whose equality is then decided on the unpacked fields
+__device__ void pack_key(const int (&key)[KEYS], unsigned long long& lo, unsigned long long& hi) {
+    bool ok = key[0] >= 0 && key[0] <= 1 && key[8] >= 0 && key[8] < 64;
+    auto field = [&](int v, int bits) -> unsigned long long {
+        const int off = 1 << (bits - 1);
+        ok = ok && v >= -off && v < off;
+        return (unsigned long long)(unsigned)(v + off) & ((1ull << bits) - 1ull);
+    };
+    lo = (unsigned long long)key[0] | ((unsigned long long)(key[8] & 63) << 1);
+    for (int j = 0; j < 4; ++j) lo |= field(key[1 + j], 11) << (7 + 11 * j);
+    lo |= field(key[5], 12) << 51;
+    hi = field(key[6], 12) | (field(key[7], 12) << 12);
+    for (int j = 0; j < 3; ++j) hi |= field(key[9 + j], 12) << (24 + 12 * j);
+    if (!ok) hi |= 1ull << 63;
+}
+
 template <int TS, int NT>
-__global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoolJob job, int si, int quality) {
+__global__ void __launch_bounds__(NT, 1024 / NT) gen_pool_kernel(WeftPoolTables tb, WeftPoolJob job, int si) {
     constexpr int N = TS * TS;
     constexpr int NW = NT / 32;
+    constexpr int WPS = N / 32;             // side-bit words per split row
+    constexpr int CH = TS <= 16 ? 3 : 1;    // channels summed by one thread
+    constexpr int G = 3 / CH;
+    constexpr int LOG_TS = TS == 8 ? 3 : TS == 16 ? 4 : TS == 32 ? 5 : 6;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* col = reinterpret_cast<float*>(smem_raw);  // [3][N]
     float* lum = col + 3 * N;                         // [N]
@@ -153,14 +269,15 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     uint8_t* bin = reinterpret_cast<uint8_t*>(sidx + N);  // [N]
     static_assert(POOL_FLOAT_PLANES == 7, "the planes above are col[3], lum, magt, mags, skey");
     static_assert(NW <= 16, "the histogram's per-warp counters hold 16 warps");
+    static_assert(N % 32 == 0 && NT % 32 == 0, "whole words and warps");
     __shared__ Scratch S;
-    (void)quality;
 
     const int t = job.tiles[si][blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool want0 = job.kinds_mask & 1, want1 = job.kinds_mask & 2;
 
     // 1. pixels and luminance 0.2126 r + 0.7152 g + 0.0722 b (float32, left to right)
+    if (tid <= NB) S.edges[tid] = tb.bin_edges[tid];
     const float4* src = reinterpret_cast<const float4*>(job.src) + job.px_off[t];
     for (int p = tid; p < N; p += NT) {
         const float4 v = src[p];
@@ -207,7 +324,7 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
         int b = NB;  // no bin (NaN)
         const double md = (double)m;
         for (int i = 0; i < NB; ++i)
-            if (md >= tb.bin_edges[i] && md < tb.bin_edges[i + 1]) {
+            if (md >= S.edges[i] && md < S.edges[i + 1]) {
                 b = i;
                 break;
             }
@@ -223,6 +340,7 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
         magt[p] = __fsqrt_rn(__fadd_rn(__fmul_rn(tx, tx), __fmul_rn(ty, ty)));
     }
     for (int i = tid; i < 16 * NB; i += NT) (&S.wcnt[0][0])[i] = 0;
+    if (tid == 0) S.n_peaks = 0;
     __syncthreads();
 
     // 3. histogram: stable counting sort of the Sobel magnitudes by bin into skey
@@ -258,7 +376,18 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
             __syncwarp();
         }
         __syncthreads();
-        if (tid < NB) S.hist[tid] = pairwise_sum(skey + S.bin_start[tid], S.bin_start[tid + 1] - S.bin_start[tid]);
+        if (N <= 128) {  // every bin is one leaf
+            if (tid < NB) S.hist[tid] = pairwise_sum(skey + S.bin_start[tid], S.bin_start[tid + 1] - S.bin_start[tid]);
+        } else {  // a warp per bin; its leaf list in the Sobel-magnitude plane (free until step 4)
+            constexpr int CAP = N / 64;  // leaves of numpy's tree for n <= N
+            int* lw = reinterpret_cast<int*>(mags) + warp * 3 * CAP;
+            static_assert(NW * 3 * CAP <= N, "leaf lists fit the plane");
+            for (int b = warp; b < NB; b += NW) {
+                const float h = warp_pairwise_sum(skey + S.bin_start[b], S.bin_start[b + 1] - S.bin_start[b], lw, CAP,
+                                                  lane);
+                if (lane == 0) S.hist[b] = h;
+            }
+        }
         __syncthreads();
         if (tid == 0) {
             float hmax = S.hist[0];
@@ -311,120 +440,163 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
         S.p25 = percentile_sorted(skey, N, 25);
         S.p75 = percentile_sorted(skey, N, 75);
         S.pm75 = percentile_sorted(mags, N, 75);
-        // regions, in a fixed order
-        int r = 0;
-        S.reg[r++] = Region{RG_ALL, 0, TS, 0, TS, make_float4(0, 0, 0, 0)};
-        const int qh = TS / 2, sh = TS / 4;
-        for (int a = 0; a < 2; ++a)
-            for (int c = 0; c < 2; ++c)
-                S.reg[r++] = Region{RG_RECT, a * qh, (a + 1) * qh, c * qh, (c + 1) * qh, make_float4(0, 0, 0, 0)};
-        for (int a = 0; a < 4; ++a)
-            for (int c = 0; c < 4; ++c)
-                S.reg[r++] = Region{RG_RECT, a * sh, (a + 1) * sh, c * sh, (c + 1) * sh, make_float4(0, 0, 0, 0)};
-        for (int k = 0; k < 3; ++k)
-            for (int j = 0; j < k + 2; ++j) {
-                const int* cut = tb.cuts + (si * 3 + k) * 5;
-                S.reg[r++] = Region{RG_RUN, cut[j], cut[j + 1], 0, 0, make_float4(0, 0, 0, 0)};
-            }
-        S.reg[r++] = Region{RG_LUM_GT, 0, 0, 0, 0, make_float4(S.p75, 0, 0, 0)};
-        S.reg[r++] = Region{RG_LUM_LT, 0, 0, 0, 0, make_float4(S.p25, 0, 0, 0)};
-        S.reg[r++] = Region{RG_MAGT_GE, 0, 0, 0, 0, make_float4(S.pm75, 0, 0, 0)};
-        if (want1) {
-            for (int i = 0; i < S.n_peaks; ++i) {
-                const float* m = tb.orient_mask + (si * 16 + S.peaks[i]) * 4;
-                const float4 c = make_float4(m[0], m[1], m[2], m[3]);
-                S.reg[r++] = Region{RG_SIDE_A, 0, 0, 0, 0, c};
-                S.reg[r++] = Region{RG_SIDE_B, 0, 0, 0, 0, c};
-            }
-            for (int i = 0; i < tb.n_spec; ++i) {
-                const float* m = tb.spec_mask + (si * WEFTK_POOL_MAX_SPECS + i) * 4;
-                const float4 c = make_float4(m[0], m[1], m[2], m[3]);
-                S.reg[r++] = Region{RG_SIDE_A, 0, 0, 0, 0, c};
-                S.reg[r++] = Region{RG_SIDE_B, 0, 0, 0, 0, c};
-            }
+        S.n_split = want1 ? S.n_peaks + tb.n_spec : 0;
+    }
+    __syncthreads();
+    // membership of the three percentile regions, one bit per pixel
+    for (int base = warp * 32; base < N; base += NT) {
+        const int p = base + lane;
+        const float l = lum[p], g = magt[p];
+        const unsigned gt = __ballot_sync(0xffffffffu, l > S.p75);
+        const unsigned lt = __ballot_sync(0xffffffffu, l < S.p25);
+        const unsigned ge = __ballot_sync(0xffffffffu, g >= S.pm75);
+        if (lane == 0) {
+            S.tmask[0][base >> 5] = gt;
+            S.tmask[1][base >> 5] = lt;
+            S.tmask[2][base >> 5] = ge;
         }
-        S.n_reg = r;
     }
     __syncthreads();
 
-    // 5. one thread per (region, channel): sequential float32 sum in the reference's order
-    for (int ch = tid; ch < S.n_reg * 3; ch += NT) {
-        const int ri = ch / 3, c = ch % 3;
-        const Region R = S.reg[ri];
-        const float* pl = col + c * N;
-        float s = 0.0f;
-        int cnt = 0;
-        switch (R.type) {
-            case RG_ALL:
-            case RG_RECT:
-                for (int y = R.a; y < R.b; ++y)
-                    for (int x = R.c; x < R.d; ++x) s = __fadd_rn(s, pl[y * TS + x]);
-                cnt = (R.b - R.a) * (R.d - R.c);
-                break;
-            case RG_RUN:
-                for (int k = R.a; k < R.b; ++k) s = __fadd_rn(s, pl[sidx[k]]);
-                cnt = R.b - R.a;
-                break;
-            case RG_LUM_GT:
-                for (int p = 0; p < N; ++p)
-                    if (lum[p] > R.coef.x) {
-                        s = __fadd_rn(s, pl[p]);
-                        ++cnt;
-                    }
-                break;
-            case RG_LUM_LT:
-                for (int p = 0; p < N; ++p)
-                    if (lum[p] < R.coef.x) {
-                        s = __fadd_rn(s, pl[p]);
-                        ++cnt;
-                    }
-                break;
-            case RG_MAGT_GE:
-                for (int p = 0; p < N; ++p)
-                    if (magt[p] >= R.coef.x) {
-                        s = __fadd_rn(s, pl[p]);
-                        ++cnt;
-                    }
-                break;
-            default: {
-                const bool want_a = R.type == RG_SIDE_A;
-                for (int y = 0; y < TS; ++y)
-                    for (int x = 0; x < TS; ++x)
-                        if (side_a(R.coef, x, y) == want_a) {
-                            s = __fadd_rn(s, pl[y * TS + x]);
-                            ++cnt;
+    // 5. every mean's sum, as numpy takes it: a sequential float32 sum per channel in the
+    //    reference's pixel order.  One thread per split line (both sides: the side test read from
+    //    the side-bit table) or fixed region, over CH channels; split lines are the dominant
+    //    orientations' centre lines, then the template lines.  Jobs come in three groups, each
+    //    starting on a warp boundary so a warp runs one loop shape: split lines; whole-tile
+    //    scans (the three percentile regions and the tile); index runs (palette runs of the
+    //    luminance order, quadrants, 4x4 blocks).  Adding +0.0f for a pixel outside a region
+    //    leaves a sum that starts at +0.0f unchanged (round to nearest never makes it -0.0f), so
+    //    the scans run without per-pixel branches.
+    {
+        const int nsplit = S.n_split;
+        constexpr int NSCAN = 4, NRUN = NFIX - NSCAN;
+        const int la = (nsplit * G + 31) & ~31, lb = (NSCAN * G + 31) & ~31, lc = (NRUN * G + 31) & ~31;
+        const uint32_t* sbits = tb.side_bits + side_words_before<TS>() * NSPL;
+        for (int slot = tid; slot < la + lb + lc; slot += NT) {
+            const int grp = slot < la ? 0 : slot < la + lb ? 1 : 2;
+            const int j = slot - (grp == 0 ? 0 : grp == 1 ? la : la + lb);
+            const int nj = grp == 0 ? nsplit : grp == 1 ? NSCAN : NRUN;
+            if (j >= nj * G) continue;  // padding up to the warp boundary
+            const int cg = j / nj, u = j - cg * nj, c0 = cg * CH;  // channel-major with one channel per thread
+            float sa[CH], sb[CH];
+#pragma unroll
+            for (int c = 0; c < CH; ++c) sa[c] = sb[c] = 0.0f;
+            if (grp == 0) {
+                const int row = u < S.n_peaks ? S.peaks[u] : 16 + (u - S.n_peaks);
+                const uint32_t* m = sbits + row * WPS;
+                int ca = 0;
+                uint32_t next = __ldg(m);
+                for (int w = 0; w < WPS; ++w) {
+                    const uint32_t word = next;
+                    if (w + 1 < WPS) next = __ldg(m + w + 1);
+                    ca += __popc(word);
+#pragma unroll 8
+                    for (int b = 0; b < 32; ++b) {
+                        const int p = w * 32 + b;
+                        const bool in_a = (word >> b) & 1u;
+#pragma unroll
+                        for (int c = 0; c < CH; ++c) {
+                            const float v = col[(c0 + c) * N + p];
+                            sa[c] = __fadd_rn(sa[c], in_a ? v : 0.0f);
+                            sb[c] = __fadd_rn(sb[c], in_a ? 0.0f : v);
                         }
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    S.smean[u][0][c0 + c] = ca > 0 ? __fdiv_rn(sa[c], (float)ca) : 0.0f;
+                    S.smean[u][1][c0 + c] = ca < N ? __fdiv_rn(sb[c], (float)(N - ca)) : 0.0f;
+                }
+                if (c0 == 0) S.scnt[u] = ca;
+            } else if (grp == 1) {  // above the 75th / below the 25th luminance percentile, gradient
+                                    // at or above its 75th, the whole tile: raster order
+                const int r = u < 3 ? 30 + u : 0;
+                int cnt = 0;
+                for (int w = 0; w < WPS; ++w) {
+                    const uint32_t word = r == 0 ? 0xffffffffu : S.tmask[r - 30][w];
+                    cnt += __popc(word);
+#pragma unroll 8
+                    for (int b = 0; b < 32; ++b) {
+                        const bool in = (word >> b) & 1u;
+#pragma unroll
+                        for (int c = 0; c < CH; ++c) {
+                            const float v = col[(c0 + c) * N + w * 32 + b];
+                            sa[c] = __fadd_rn(sa[c], in ? v : 0.0f);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < CH; ++c) S.rmean[r][c0 + c] = cnt > 0 ? __fdiv_rn(sa[c], (float)cnt) : 0.0f;
+                if (c0 == 0) S.rcnt[r] = cnt;
+            } else {  // palette run [a, b) of the luminance order, or a quadrant / 4x4 block row by row
+                const int r = u < 9 ? 21 + u : u - 8;
+                const bool run = r >= 21;
+                int a = 0, len, y0 = 0, x0 = 0, lg = 0;
+                if (run) {
+                    int b;
+                    run_bounds(tb.cuts, si, r, a, b);
+                    len = b > a ? b - a : 0;
+                } else {
+                    lg = r <= 4 ? LOG_TS - 1 : LOG_TS - 2;  // side TS/2 or TS/4
+                    const int q = r <= 4 ? r - 1 : r - 5, per = r <= 4 ? 2 : 4;
+                    y0 = (q / per) << lg;
+                    x0 = (q % per) << lg;
+                    len = 1 << (2 * lg);
+                }
+                const int msk = (1 << lg) - 1;
+#pragma unroll 4
+                for (int k = 0; k < len; ++k) {
+                    const int ps = sidx[a + k];  // in range for a rect too (a = 0, len <= N / 4)
+                    const int p = run ? ps : (y0 + (k >> lg)) * TS + x0 + (k & msk);
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) sa[c] = __fadd_rn(sa[c], col[(c0 + c) * N + p]);
+                }
+#pragma unroll
+                for (int c = 0; c < CH; ++c) S.rmean[r][c0 + c] = len > 0 ? __fdiv_rn(sa[c], (float)len) : 0.0f;
+                if (c0 == 0) S.rcnt[r] = len;
             }
         }
-        S.rsum[ri][c] = s;
-        if (c == 0) S.rcnt[ri] = cnt;
     }
     __syncthreads();
 
-    // 6. palettes (one thread; a handful of means and distance tests), then the candidate list's
-    //    segment sizes: the list is (edge pool) palette x 4 alphas, quadrants x 2, orientations x 5,
-    //    (template pool) palette x 4, quadrants x 2, blocks, splits x 3 or x 1, so candidate i is
-    //    a function of i that any thread can evaluate (cand_at below)
+    // 6. palettes: the 13 colours (tile mean, then regions 21..32 in order), their pairwise
+    //    near tests in parallel, then one thread keeps each colour that is not near one kept
+    //    before it; then the candidate list's segment sizes: the list is (edge pool) palette x 4
+    //    alphas, quadrants x 2, orientations x 5, (template pool) palette x 4, quadrants x 2,
+    //    blocks, splits x 3 or x 1, so candidate i is a function of i that any thread can
+    //    evaluate (cand_at below)
+    if (tid < NCOL) {
+        float m[3];
+        const int r = 20 + tid;
+        int a = 0, b = 1;
+        if (tid >= 1 && r < 30) run_bounds(tb.cuts, si, r, a, b);
+        if (tid >= 1 && r < 30 && b <= a) {
+            const int p = sidx[min(a, N - 1)];
+            for (int c = 0; c < 3; ++c) m[c] = col[c * N + p];
+        } else if (tid >= 1 && S.rcnt[r] > 0) {
+            for (int c = 0; c < 3; ++c) m[c] = S.rmean[r][c];
+        } else {
+            for (int c = 0; c < 3; ++c) m[c] = S.rmean[0][c];
+        }
+        for (int c = 0; c < 3; ++c) S.cpal[tid][c] = clamp01(m[c]);
+    }
+    __syncthreads();
+    if (tid < NCOL) {
+        unsigned near = 0;
+        for (int a = 0; a < tid; ++a)
+            if (near_pair(S.cpal[tid], S.cpal[a])) near |= 1u << a;
+        S.near_mask[tid] = near;
+    }
+    __syncthreads();
     if (tid == 0) {
-        float avg[3];
-        for (int c = 0; c < 3; ++c) avg[c] = clamp01(__fdiv_rn(S.rsum[0][c], (float)S.rcnt[0]));
+        unsigned kept = 1u;
         int npal = 1;
-        for (int c = 0; c < 3; ++c) S.pal[0][c] = avg[c];
-        for (int r = 21; r < 33; ++r) {
-            if (r == 30) S.npal_e = npal;  // the template palette adds bright / dark / edge colours
-            const Region R = S.reg[r];
-            float m[3];
-            if (r < 30 && R.b <= R.a) {
-                const int p = sidx[min(R.a, N - 1)];
-                for (int c = 0; c < 3; ++c) m[c] = col[c * N + p];
-            } else if (S.rcnt[r] > 0) {
-                for (int c = 0; c < 3; ++c) m[c] = __fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]);
-            } else {
-                for (int c = 0; c < 3; ++c) m[c] = avg[c];
-            }
-            for (int c = 0; c < 3; ++c) m[c] = clamp01(m[c]);
-            if (!near_any(m, S.pal, npal) && npal < MAXPAL) {
-                for (int c = 0; c < 3; ++c) S.pal[npal][c] = m[c];
+        for (int c = 0; c < 3; ++c) S.pal[0][c] = S.cpal[0][c];
+        for (int i = 1; i < NCOL; ++i) {
+            if (i == 10) S.npal_e = npal;  // the template palette adds bright / dark / edge colours
+            if (!(S.near_mask[i] & kept) && npal < MAXPAL) {
+                kept |= 1u << i;
+                for (int c = 0; c < 3; ++c) S.pal[npal][c] = S.cpal[i][c];
                 ++npal;
             }
         }
@@ -437,61 +609,62 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
         S.n_cand = min(S.seg[7], MAXC);
         if (S.seg[7] > MAXC) atomicCAS(&g_device_status, 0, WEFTK_E_RANGE);
     }
+    for (int i = tid; i < HT; i += NT) {
+        S.ht_hash[i] = 0ull;
+        S.ht_idx[i] = 0x7fffffff;
+    }
     __syncthreads();
 
     // candidate i: kind, float64 geometry (the reference's Python values), colours, alpha
     auto cand_at = [&](int i, int& kind, double (&g)[4], float (&c0)[3], float (&c1)[3], double& alpha) {
-        const double A4[4] = {1.0, 0.7, 0.4, 0.2};
-        const double A3[3] = {1.0, 0.7, 0.4};
-        auto mean_clamped = [&](int r, float (&m)[3]) {
-            for (int c = 0; c < 3; ++c) m[c] = clamp01(__fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]));
-        };
+        auto a4 = [](int q) { return q == 0 ? 1.0 : q == 1 ? 0.7 : q == 2 ? 0.4 : 0.2; };
         kind = 0;
         for (int k = 0; k < 4; ++k) g[k] = 0.0;
         for (int c = 0; c < 3; ++c) c1[c] = 0.0f;
         int k = 0;
-        while (i >= S.seg[k + 1]) ++k;
+        while (k < 6 && i >= S.seg[k + 1]) ++k;
         const int j = i - S.seg[k];
         switch (k) {
             case 0:
             case 3:  // palette colour x alphas 1, .7, .4, .2
                 for (int c = 0; c < 3; ++c) c0[c] = S.pal[j >> 2][c];
-                alpha = A4[j & 3];
+                alpha = a4(j & 3);
                 break;
             case 1:
-            case 4:  // quadrant mean x alphas .5, .3
-                mean_clamped(1 + (j >> 1), c0);
+            case 4: {  // quadrant mean x alphas .5, .3
+                const int r = 1 + (j >> 1);
+                for (int c = 0; c < 3; ++c) c0[c] = clamp01(S.rmean[r][c]);
                 alpha = (j & 1) ? 0.3 : 0.5;
                 break;
+            }
             case 2: {  // orientation split: centre x 1, .7, .4, offsets at 0.25 and 0.75 x .5
-                const int pk = j / 5, m = j - pk * 5, r = 33 + 2 * pk;
-                float avg[3];
-                for (int c = 0; c < 3; ++c) avg[c] = clamp01(__fdiv_rn(S.rsum[0][c], (float)S.rcnt[0]));
-                if (S.rcnt[r] > 0) mean_clamped(r, c0);
-                else
-                    for (int c = 0; c < 3; ++c) c0[c] = avg[c];
-                if (S.rcnt[r + 1] > 0) mean_clamped(r + 1, c1);
-                else
-                    for (int c = 0; c < 3; ++c) c1[c] = avg[c];
+                const int pk = j / 5, m = j - pk * 5;
+                const int na = S.scnt[pk], nb = N - na;
+                for (int c = 0; c < 3; ++c) {
+                    const float avg = clamp01(S.rmean[0][c]);
+                    c0[c] = na > 0 ? clamp01(S.smean[pk][0][c]) : avg;
+                    c1[c] = nb > 0 ? clamp01(S.smean[pk][1][c]) : avg;
+                }
                 const double* gg = tb.orient_geom + ((size_t)(si * 16 + S.peaks[pk]) * 3 + (m < 3 ? 0 : m - 2)) * 4;
                 for (int q = 0; q < 4; ++q) g[q] = gg[q];
-                alpha = m < 3 ? A3[m] : 0.5;
+                alpha = m < 3 ? a4(m) : 0.5;
                 kind = 1;
                 break;
             }
             case 5:  // 4x4 block mean x .25
-                mean_clamped(5 + j, c0);
+                for (int c = 0; c < 3; ++c) c0[c] = clamp01(S.rmean[5 + j][c]);
                 alpha = 0.25;
                 break;
             default: {  // template split: batched side means, not clamped; an empty side takes the
                         // (unclamped) tile mean
                 const int sp = j < tb.n_centre * 3 ? j / 3 : tb.n_centre + (j - tb.n_centre * 3);
-                alpha = j < tb.n_centre * 3 ? A3[j % 3] : 0.5;
-                const int r = 33 + 2 * S.n_peaks + 2 * sp;
+                alpha = j < tb.n_centre * 3 ? a4(j % 3) : 0.5;
+                const int u = S.n_peaks + sp;
+                const int na = S.scnt[u], nb = N - na;
                 for (int c = 0; c < 3; ++c) {
-                    const float fb = __fdiv_rn(S.rsum[0][c], (float)S.rcnt[0]);
-                    c0[c] = S.rcnt[r] > 0 ? __fdiv_rn(S.rsum[r][c], (float)S.rcnt[r]) : fb;
-                    c1[c] = S.rcnt[r + 1] > 0 ? __fdiv_rn(S.rsum[r + 1][c], (float)S.rcnt[r + 1]) : fb;
+                    const float fb = S.rmean[0][c];
+                    c0[c] = na > 0 ? S.smean[u][0][c] : fb;
+                    c1[c] = nb > 0 ? S.smean[u][1][c] : fb;
                 }
                 const double* gg = tb.spec_geom + (size_t)(si * WEFTK_POOL_MAX_SPECS + sp) * 4;
                 for (int q = 0; q < 4; ++q) g[q] = gg[q];
@@ -512,8 +685,22 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
         key[8] = qkey(alpha, 32.0);
         for (int j = 0; j < 3; ++j) key[9 + j] = kind == 1 ? qkey((double)c1[j], 64.0) : 0;
     };
+    auto same_key = [&](int i, int j) {
+        const bool pi = !(S.khi[i] >> 63), pj = !(S.khi[j] >> 63);
+        if (pi && pj) return S.klo[i] == S.klo[j] && S.khi[i] == S.khi[j];
+        if (pi != pj) return false;  // a field in range against one out of range
+        int a[KEYS], b[KEYS];
+        key_of(i, a);
+        key_of(j, b);
+        bool same = true;
+        for (int k = 0; k < KEYS; ++k) same = same && a[k] == b[k];
+        return same;
+    };
 
-    // 7. first occurrences kept: 64-bit hashes of the keys, the full keys compared on a match
+    // 7. first occurrences kept: every candidate's key, its 64-bit hash entered in a shared
+    //    hash table that keeps the lowest candidate index per hash; a candidate is a repeat when
+    //    that index is lower than its own and the keys agree (on a bare hash match, every earlier
+    //    candidate of the hash is compared)
     const int nc = S.n_cand;
     for (int i = tid; i < nc; i += NT) {
         int key[KEYS];
@@ -523,30 +710,50 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
             h = (h ^ (unsigned long long)(unsigned)key[k]) * 0xff51afd7ed558ccdull;
             h ^= h >> 33;
         }
+        h |= h == 0ull;  // 0 marks an empty slot
         S.hash[i] = h;
+        pack_key(key, S.klo[i], S.khi[i]);
+        int s = (int)(h & (HT - 1));
+        for (int probe = 0; probe < HT; ++probe) {  // the table holds at most MAXC < HT hashes
+            const unsigned long long prev = atomicCAS(&S.ht_hash[s], 0ull, h);
+            if (prev == 0ull || prev == h) {
+                atomicMin(&S.ht_idx[s], i);
+                break;
+            }
+            s = (s + 1) & (HT - 1);
+        }
     }
     __syncthreads();
-    for (int i = tid; i < nc; i += NT) {
-        const unsigned long long h = S.hash[i];
-        bool dup = false;
-        for (int j = 0; j < i && !dup; ++j) {
-            if (S.hash[j] != h) continue;
-            int a[KEYS], b[KEYS];
-            key_of(i, a);
-            key_of(j, b);
-            bool same = true;
-            for (int k = 0; k < KEYS; ++k) same = same && a[k] == b[k];
-            dup = same;
+    for (int base = 0; base < nc; base += NT) {  // every lane of a warp reaches the ballot
+        const int i = base + tid;
+        bool keep = false;
+        if (i < nc) {
+            const unsigned long long h = S.hash[i];
+            int s = (int)(h & (HT - 1));
+            for (int probe = 0; probe < HT && S.ht_hash[s] != h; ++probe) s = (s + 1) & (HT - 1);
+            const int j = S.ht_idx[s];
+            keep = true;
+            if (j < i) {
+                if (same_key(i, j)) {
+                    keep = false;
+                } else {
+                    for (int j2 = 0; j2 < i; ++j2)
+                        if (S.hash[j2] == h && same_key(i, j2)) {
+                            keep = false;
+                            break;
+                        }
+                }
+            }
         }
-        S.keep[i] = !dup;
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0 && base + warp * 32 < nc) S.keepw[(base + warp * 32) >> 5] = bal;
     }
     __syncthreads();
     if (tid == 0) {
         int n = 0;
-        for (int i = 0; i < nc; ++i) {
-            const int k = S.keep[i];
-            S.keep[i] = k ? n : -1;  // output position, -1 = dropped
-            n += k;
+        for (int w = 0; w < (nc + 31) / 32; ++w) {
+            S.keep_pre[w] = n;
+            n += __popc(S.keepw[w]);
         }
         if (n > job.pool_cap) {
             atomicCAS(&g_device_status, 0, WEFTK_E_RANGE);
@@ -558,8 +765,10 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
     __syncthreads();
     WeftPrim* out = job.cand + job.pool_off[t];
     for (int i = tid; i < nc; i += NT) {
-        const int pos = S.keep[i];
-        if (pos < 0 || pos >= S.n_out) continue;
+        const unsigned w = S.keepw[i >> 5];
+        if (!((w >> (i & 31)) & 1u)) continue;
+        const int pos = S.keep_pre[i >> 5] + __popc(w & ((1u << (i & 31)) - 1u));
+        if (pos >= S.n_out) continue;
         int kind;
         double g[4], alpha;
         float c0[3], c1[3];
@@ -574,6 +783,29 @@ __global__ void __launch_bounds__(NT) gen_pool_kernel(WeftPoolTables tb, WeftPoo
         p.alpha = (float)alpha;
         out[pos] = p;
     }
+}
+
+// the side test of every split row over every tile side's pixel grid, one thread per word
+__global__ void side_bits_kernel(WeftPoolTables tb, uint32_t* out) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= WEFTK_POOL_SIDE_WORDS) return;
+    int si = 0;
+    while (si < 3 && gid >= (si == 0 ? 2 : si == 1 ? 10 : 42) * NSPL) ++si;
+    const int before = si == 0 ? 0 : si == 1 ? 2 : si == 2 ? 10 : 42;
+    const int ts = 8 << si, wps = ts * ts / 32;
+    const int local = gid - before * NSPL, row = local / wps, w = local - row * wps;
+    const float* m = row < 16 ? tb.orient_mask + (si * 16 + row) * 4
+                     : row - 16 < tb.n_spec ? tb.spec_mask + (si * WEFTK_POOL_MAX_SPECS + (row - 16)) * 4
+                                            : nullptr;
+    uint32_t word = 0;
+    if (m) {
+        const float4 c = make_float4(m[0], m[1], m[2], m[3]);
+        for (int b = 0; b < 32; ++b) {
+            const int p = w * 32 + b;
+            if (side_a(c, p % ts, p / ts)) word |= 1u << b;
+        }
+    }
+    out[gid] = word;
 }
 
 template <int TS, int NT>
@@ -596,7 +828,7 @@ int launch_gen(const WeftPoolTables& tb, const WeftPoolJob& job, int si, cudaStr
             done.insert(dev);
         }
     }
-    gen_pool_kernel<TS, NT><<<n, NT, dyn, stream>>>(tb, job, si, 0);
+    gen_pool_kernel<TS, NT><<<n, NT, dyn, stream>>>(tb, job, si);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }
@@ -633,6 +865,16 @@ int side_streams(SideStreams** out) {
     return WEFTK_OK;
 }
 
+extern "C" int weftk_pool_side_bits(const WeftPoolTables* tables, uint32_t* d_bits, void* stream) {
+    WEFTK_REQUIRE(tables && d_bits, "pool_side_bits: null argument");
+    WEFTK_REQUIRE(tables->n_spec >= 0 && tables->n_spec <= WEFTK_POOL_MAX_SPECS, "pool_side_bits: bad template table");
+    WEFTK_REQUIRE(tables->orient_mask && (tables->n_spec == 0 || tables->spec_mask), "pool_side_bits: null table");
+    constexpr int block = 256;
+    side_bits_kernel<<<(WEFTK_POOL_SIDE_WORDS + block - 1) / block, block, 0, (cudaStream_t)stream>>>(*tables, d_bits);
+    WEFTK_CUDA(cudaGetLastError());
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_gen_pools(const WeftPoolTables* tables, const WeftPoolJob* job, void* stream) {
     WEFTK_REQUIRE(tables && job, "gen_pools: null argument");
     WEFTK_REQUIRE(tables->n_spec >= 0 && tables->n_spec <= WEFTK_POOL_MAX_SPECS &&
@@ -649,7 +891,7 @@ extern "C" int weftk_gen_pools(const WeftPoolTables* tables, const WeftPoolJob* 
     if (!any) return WEFTK_OK;
     WEFTK_REQUIRE(job->src && job->px_off && job->pool_off && job->cand && job->pool_cnt, "gen_pools: null pointer");
     WEFTK_REQUIRE(tables->bin_edges && tables->cuts && tables->orient_geom && tables->orient_mask &&
-                      (tables->n_spec == 0 || (tables->spec_geom && tables->spec_mask)),
+                      tables->side_bits && (tables->n_spec == 0 || (tables->spec_geom && tables->spec_mask)),
                   "gen_pools: null table");
     cudaStream_t s = (cudaStream_t)stream;
     SideStreams* ss = nullptr;

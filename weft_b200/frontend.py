@@ -70,19 +70,43 @@ def extract_device(img_u8: torch.Tensor, tiles: torch.Tensor, sizes: np.ndarray)
 
 
 def refine_image(u8: np.ndarray, quality: int = 75, cap: int = 16, steps: int = 10, lr: float = 1e-2,
-                 threshold: float = 100.0, device: int = 0):
+                 threshold: float = 100.0, device: int = 0, timings: dict | None = None):
     """The refined fit of one sRGB u8 image (host array, page-locked memory copies fastest), end to
     end on the GPU.  Returns (tiles int32 (n, 3) of (x, y, side), rows float32 (n, 16) on the wire
-    grid, kinds int32 (n,), -1 = no primitive) as host arrays."""
+    grid, kinds int32 (n,), -1 = no primitive) as host arrays.  ``timings``: a dict that receives
+    the host wall milliseconds of each phase (the device is synchronised between phases, which
+    the plain call does not do)."""
+    import time
+
     from .pools import DeviceRefinedFit
 
     dev = torch.device("cuda", device)
+    marks = []
+
+    def mark(name):
+        if timings is not None:
+            torch.cuda.synchronize(dev)
+            marks.append((name, time.perf_counter()))
+
+    mark("start")
     img = torch.from_numpy(np.ascontiguousarray(u8, np.uint8)).to(dev, non_blocking=True)
+    mark("h2d")
     tiles, n = decompose_device(img, threshold)
+    mark("quadtree")
     tiles_h = tiles.cpu().numpy()
     sizes = tiles_h[:, 2].copy()
+    mark("tiles_d2h")
     src4, _ = extract_device(img, tiles, sizes)
+    mark("extract")
     drf = DeviceRefinedFit(src4, sizes, quality, caps=[cap] * n, steps=steps, lr=lr, use_graph=False,
                            autotune=False)
+    mark("setup")
     rows = drf.run()
-    return tiles_h, rows.cpu().numpy(), drf.rf.kinds.cpu().numpy()
+    mark("fit")
+    out = tiles_h, rows.cpu().numpy(), drf.rf.kinds.cpu().numpy()
+    mark("d2h")
+    if timings is not None:
+        for (_, a), (name, b) in zip(marks, marks[1:]):
+            timings[name] = (b - a) * 1e3
+        timings["total"] = (marks[-1][1] - marks[0][1]) * 1e3
+    return out

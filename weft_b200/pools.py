@@ -30,9 +30,17 @@ MAX_CONST_LINEAR = 272
 ORIENT_FALLBACK = (0.0, np.pi / 4, np.pi / 2, 3 * np.pi / 4)
 
 
+SPLITS = 16 + MAX_SPECS
+SIDE_WORDS = SPLITS * sum(s * s // 32 for s in SIDES)
+
+
 class WeftPoolTables(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in ("spec_geom", "spec_mask", "orient_geom", "orient_mask", "bin_edges",
-                                               "cuts")] + [("n_spec", ctypes.c_int32), ("n_centre", ctypes.c_int32)]
+                                               "cuts", "side_bits")] + [("n_spec", ctypes.c_int32),
+                                                                        ("n_centre", ctypes.c_int32)]
+
+
+assert ctypes.sizeof(WeftPoolTables) == 64
 
 
 class WeftPoolJob(ctypes.Structure):
@@ -120,9 +128,25 @@ class PoolTables:
         host = build_tables(self.quality)
         self._t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(self.device) for k, v in host.items()
                    if isinstance(v, np.ndarray)}
+        self.side_bits = torch.zeros(SIDE_WORDS, dtype=torch.int32, device=self.device)
         self.st = WeftPoolTables(*[_lib.ptr(self._t[k]) for k in ("spec_geom", "spec_mask", "orient_geom",
                                                                   "orient_mask", "bin_edges", "cuts")],
-                                 int(host["n_spec"]), int(host["n_centre"]))
+                                 None, int(host["n_spec"]), int(host["n_centre"]))
+        lib = _lib.lib_for_device(self.device.index or 0)
+        _lib.check(lib.weftk_pool_side_bits(ctypes.addressof(self.st), _lib.ptr(self.side_bits),
+                                            torch.cuda.current_stream(self.device).cuda_stream),
+                   "weftk_pool_side_bits")
+        torch.cuda.current_stream(self.device).synchronize()
+        self.st.side_bits = _lib.ptr(self.side_bits)
+
+    def side_masks(self, side: int) -> np.ndarray:
+        """The side-bit table of tile side ``side`` unpacked: bool (SPLITS, side, side), True on
+        side a (rows: the 16 orientations' centre lines, then the template lines)."""
+        si = SIDES.index(int(side))
+        before = SPLITS * sum(s * s // 32 for s in SIDES[:si])
+        words = self.side_bits[before:before + SPLITS * side * side // 32].cpu().numpy().view(np.uint32)
+        bits = (words[:, None] >> np.arange(32, dtype=np.uint32)[None, :]) & 1
+        return bits.reshape(SPLITS, side, side).astype(bool)
 
 
 _TABLES: dict[tuple[int, int], PoolTables] = {}
@@ -195,18 +219,28 @@ class DeviceRefinedFit:
         self.fit = BatchedFit.from_device_pools(src4, self.sizes, self.cand, self.cnt, self.stride, quality, caps,
                                                 kinds_mask=mask)
         self.fit.use_closed_form_init(True)
+        self._gen = self._generator()
         if autotune or not generate_in_run:
             self.generate()  # the autotuner times scoring launches over real pools
         if autotune:
             self.fit.autotune()
+        # the prelude holds the generation's arguments, not this object: no reference cycle keeps
+        # the device buffers alive past the last reference
         self.rf = RefinedFit(self.fit, steps=steps, lr=lr, use_graph=use_graph,
-                             prelude=self.generate if generate_in_run else None)
+                             prelude=self._gen if generate_in_run else None)
+
+    def _generator(self):
+        src4, f, sizes, cand, cnt = self.src4, self.fit, self.sizes, self.cand, self.cnt
+        quality, kinds, stride, lists = self.quality, self.kinds, self.stride, self.lists
+
+        def gen() -> None:
+            generate_pools(src4, f.t_px_off, sizes, f.t_pool_off, cand, cnt, quality, kinds, stride, lists)
+
+        return gen
 
     def generate(self) -> None:
         """Enqueue the pool generation (device work only)."""
-        f = self.fit
-        generate_pools(self.src4, f.t_px_off, self.sizes, f.t_pool_off, self.cand, self.cnt, self.quality,
-                       self.kinds, self.stride, self.lists)
+        self._gen()
 
     def run(self) -> torch.Tensor:
         self.rf.run()

@@ -1158,11 +1158,13 @@ def run_weft(args, world, rank, local, executor, cores):
 
     ref_e2e_val, (r_h2d, r_d2h) = timed_e2e(refined_e2e)
     tiles_e2e_val, _ = timed_e2e(tiles_e2e)
-    # where the end-to-end time goes: one more call, synchronised between its phases (untimed)
-    from weft_b200.frontend import refine_image
+    # where the time of the same fit driven from Python goes: one call of the stepwise front end,
+    # synchronised between its phases (untimed)
+    from weft_b200.frontend import refine_image_steps
 
     e2e_phases: dict = {}
-    refine_image(u8_h, QUALITY, CAP, steps=args.refine_steps, lr=args.refine_lr, device=local, timings=e2e_phases)
+    refine_image_steps(u8_h, QUALITY, CAP, steps=args.refine_steps, lr=args.refine_lr, device=local,
+                       timings=e2e_phases)
 
     diff = differentiable_fit(args, executor, local, stream) if args.diff_steps > 0 and rank == 0 else None
     ibatch = image_batch_fit(args, executor, local, stream) if args.batch_images and rank == 0 else None

@@ -49,7 +49,7 @@ def test_refine_image_equals_the_fit_over_host_tiles():
     np.testing.assert_array_equal(kinds, kinds_h)
 
 
-def test_refine_image_releases_its_device_memory_at_return():
+def test_refine_image_steps_releases_its_device_memory_at_return():
     """No reference cycle holds the fit's buffers after the call (the caching allocator gets
     them back at once, with the cycle collector off)."""
     import gc
@@ -58,15 +58,53 @@ def test_refine_image_releases_its_device_memory_at_return():
     from weft_b200.synth import make_image_u8
 
     u8 = make_image_u8(256, 256, 30, 2)
-    frontend.refine_image(u8, 75, 16, steps=3)  # tables, lookup tables, streams
+    frontend.refine_image_steps(u8, 75, 16, steps=3)  # tables, lookup tables, streams
     torch.cuda.synchronize()
     gc.collect()
     base = torch.cuda.memory_allocated()
     gc.disable()
     try:
         for _ in range(3):
-            frontend.refine_image(u8, 75, 16, steps=3)
+            frontend.refine_image_steps(u8, 75, 16, steps=3)
         torch.cuda.synchronize()
         assert torch.cuda.memory_allocated() == base
     finally:
         gc.enable()
+
+
+def test_native_pipeline_equals_the_stepwise_calls_across_image_sizes():
+    """``weftk_refine_image`` (one native call, a workspace kept and grown between images) against
+    the same steps driven one entry point at a time: equal tiles, rows and kinds, bit for bit, on
+    a sequence of images whose sizes grow and shrink."""
+    from weft_b200 import frontend
+    from weft_b200.synth import make_image_u8
+
+    r = frontend.Refiner(75, 16, steps=5)
+    for w, h, n, seed in [(256, 256, 30, 1), (520, 392, 70, 2), (72, 264, 9, 5), (256, 256, 30, 1), (130, 200, 20, 3)]:
+        u8 = make_image_u8(w, h, n, seed)
+        tiles, rows, kinds = r(u8)
+        t2, r2, k2 = frontend.refine_image_steps(u8, 75, 16, steps=5)
+        np.testing.assert_array_equal(tiles, t2)
+        np.testing.assert_array_equal(kinds, k2)
+        np.testing.assert_array_equal(rows, r2)
+        assert (kinds >= 0).all()
+    r.close()
+
+
+def test_native_pipeline_reports_too_many_tiles():
+    import ctypes
+
+    from weft_b200 import frontend
+    from weft_b200.synth import make_image_u8
+
+    r = frontend.Refiner(75, 16, steps=2)
+    u8 = make_image_u8(128, 128, 30, 4)
+    tiles = np.empty((1, 3), np.int32)
+    rows = np.empty((1, 16), np.float32)
+    kinds = np.empty(1, np.int32)
+    n = ctypes.c_int(0)
+    rc = r.lib.weftk_refine_image(r.handle, u8.ctypes.data, 128, 128, tiles.ctypes.data, rows.ctypes.data,
+                                  kinds.ctypes.data, 1, ctypes.addressof(n), torch.cuda.current_stream().cuda_stream)
+    assert rc == -3  # WEFTK_E_RANGE: more tiles than max_tiles, the count reported
+    assert n.value > 1
+    r.close()

@@ -57,6 +57,18 @@ class WeftStackSet(ctypes.Structure):
         ("kinds_mask", ctypes.c_int32), ("moments", ctypes.c_void_p)]
 
 
+class WeftRefineParams(ctypes.Structure):
+    """Parameters of a per-image refiner (include/weftk_pipeline.h)."""
+    _fields_ = [("cap", ctypes.c_int32), ("steps", ctypes.c_int32), ("min_tile", ctypes.c_int32),
+                ("max_tile", ctypes.c_int32), ("chunk", ctypes.c_int32 * 3), ("variant", ctypes.c_int32 * 3),
+                ("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("threshold", ctypes.c_double), ("lam", ctypes.c_double), ("complex_threshold", ctypes.c_double),
+                ("tables", ctypes.c_void_p), ("srgb_lut", ctypes.c_void_p)]
+
+
+assert ctypes.sizeof(WeftRefineParams) == 96
+
+
 # numpy mirrors of the C structs (same byte layout)
 PRIM_DTYPE = np.dtype([("kind", np.int32), ("geom", np.float32, 7), ("color0", np.float32, 3),
                        ("color1", np.float32, 3), ("alpha", np.float32)])
@@ -121,6 +133,9 @@ SIGNATURES: dict[str, list] = {
     "weftk_quadtree_work_bytes": [_I, _I, _I, _I, _P],
     "weftk_quadtree_variance": [_P, _I, _I, ctypes.c_double, _I, _I, _P, _I, _P, _P, _P],
     "weftk_extract_tiles": [_P, _I, _I, _P, _P, _I, _P, _P, _P],
+    "weftk_refiner_create": [_P, _P],
+    "weftk_refiner_destroy": [_P],
+    "weftk_refine_image": [_P, _P, _I, _I, _P, _P, _P, _I, _P, _P],
 }
 
 _lock = threading.Lock()

@@ -69,13 +69,11 @@ def extract_device(img_u8: torch.Tensor, tiles: torch.Tensor, sizes: np.ndarray)
     return src4, px_off
 
 
-def refine_image(u8: np.ndarray, quality: int = 75, cap: int = 16, steps: int = 10, lr: float = 1e-2,
-                 threshold: float = 100.0, device: int = 0, timings: dict | None = None):
-    """The refined fit of one sRGB u8 image (host array, page-locked memory copies fastest), end to
-    end on the GPU.  Returns (tiles int32 (n, 3) of (x, y, side), rows float32 (n, 16) on the wire
-    grid, kinds int32 (n,), -1 = no primitive) as host arrays.  ``timings``: a dict that receives
-    the host wall milliseconds of each phase (the device is synchronised between phases, which
-    the plain call does not do)."""
+def refine_image_steps(u8: np.ndarray, quality: int = 75, cap: int = 16, steps: int = 10, lr: float = 1e-2,
+                       threshold: float = 100.0, device: int = 0, timings: dict | None = None):
+    """``refine_image`` driven one entry point at a time from Python (fresh fit objects per call):
+    the same results, bit for bit.  ``timings``: a dict that receives the host wall milliseconds
+    of each phase (the device is synchronised between phases, which the plain call does not do)."""
     import time
 
     from .pools import DeviceRefinedFit
@@ -110,3 +108,89 @@ def refine_image(u8: np.ndarray, quality: int = 75, cap: int = 16, steps: int = 
             timings[name] = (b - a) * 1e3
         timings["total"] = (marks[-1][1] - marks[0][1]) * 1e3
     return out
+
+
+class Refiner:
+    """The refined fit of whole images through the native per-image pipeline
+    (``weftk_refine_image``, include/weftk_pipeline.h): one call per image, a device workspace
+    kept between calls (it grows to the largest image seen)."""
+
+    def __init__(self, quality: int = 75, cap: int = 16, steps: int = 10, lr: float = 1e-2, threshold: float = 100.0,
+                 device: int = 0, min_tile: int = 8, max_tile: int = 64):
+        from . import rate
+        from .fit import CHUNK
+        from .pools import tables_for
+
+        self.device = torch.device("cuda", device)
+        self.lib = _lib.lib_for_device(device)
+        self.tables = tables_for(quality, device)
+        self.lut = srgb_table(self.device)
+        p = _lib.WeftRefineParams()
+        p.cap, p.steps, p.min_tile, p.max_tile = int(cap), int(steps), int(min_tile), int(max_tile)
+        for i, cls in enumerate((8, 16, 32)):
+            p.chunk[i] = int(CHUNK[cls])
+            p.variant[i] = 0
+        p.lr, p.beta1, p.beta2, p.eps = float(lr), 0.9, 0.999, 1e-8
+        p.threshold = float(threshold)
+        p.lam = float(rate.tile_lambda(quality))
+        p.complex_threshold = float(rate.complexity_threshold(quality))
+        p.tables = ctypes.addressof(self.tables.st)
+        p.srgb_lut = _lib.ptr(self.lut)
+        self.params = p
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.weftk_refiner_create(ctypes.addressof(p), ctypes.addressof(handle)),
+                       "weftk_refiner_create")
+        self.handle = handle
+        self._cap_tiles = 0
+        self._out = None
+
+    def __call__(self, u8: np.ndarray):
+        """(tiles int32 (n, 3) of (x, y, side), rows float32 (n, 16) on the wire grid, kinds int32 (n,))."""
+        img = np.ascontiguousarray(u8, np.uint8)
+        if img.ndim != 3 or img.shape[2] != 3:
+            raise ValueError("expected an (h, w, 3) uint8 image")
+        h, w = int(img.shape[0]), int(img.shape[1])
+        p = self.params
+        cap = (-(-h // p.max_tile)) * (-(-w // p.max_tile)) * (p.max_tile // p.min_tile) ** 2
+        if self._out is None or self._cap_tiles < cap:
+            self._out = (np.empty((cap, 3), np.int32), np.empty((cap, 16), np.float32), np.empty(cap, np.int32))
+            self._cap_tiles = cap
+        tiles, rows, kinds = self._out
+        n = ctypes.c_int(0)
+        with torch.cuda.device(self.device):
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+            _lib.check(self.lib.weftk_refine_image(self.handle, img.ctypes.data, h, w, tiles.ctypes.data,
+                                                   rows.ctypes.data, kinds.ctypes.data, cap, ctypes.addressof(n),
+                                                   stream), "weftk_refine_image")
+        k = n.value
+        return tiles[:k].copy(), rows[:k].copy(), kinds[:k].copy()
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) and self.handle.value:
+            self.lib.weftk_refiner_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_REFINERS: dict[tuple, Refiner] = {}
+
+
+def refine_image(u8: np.ndarray, quality: int = 75, cap: int = 16, steps: int = 10, lr: float = 1e-2,
+                 threshold: float = 100.0, device: int = 0):
+    """The refined fit of one sRGB u8 image (host array, page-locked memory copies fastest), end to
+    end on the GPU through the native pipeline: quadtree, tile extraction, pool generation, init
+    round, ``steps`` Adam steps and the wire-grid snap, one host read of the tile list in between.
+    Returns (tiles int32 (n, 3) of (x, y, side), rows float32 (n, 16) on the wire grid, kinds int32
+    (n,), -1 = no primitive) as host arrays.  The refiner (and its device workspace) is kept per
+    device and settings."""
+    key = (int(device), int(quality), int(cap), int(steps), float(lr), float(threshold))
+    r = _REFINERS.get(key)
+    if r is None:
+        r = _REFINERS[key] = Refiner(quality, cap, steps, lr, threshold, device)
+    return r(u8)

@@ -89,9 +89,11 @@ class StackSet:
                                     _lib.ptr(self.t_prim_off), _lib.ptr(self.t_kind), _lib.ptr(self.t_order),
                                     n_big, n_mid, n_s16, int(kinds_mask or 0), _lib.ptr(moments))
         self._moments = moments
-        n_px = (sizes.to(torch.int64) ** 2)
-        total = float((sz.astype(np.int64) ** 2).sum())
-        self.weights = (n_px.to(torch.float32) / total) if self.n else n_px.float()
+        # each tile's share of the pixels, float32(side^2) / float32(total) as IEEE single division
+        # (the native per-image pipeline computes the same bits)
+        px = (sz.astype(np.int64) ** 2)
+        w = px.astype(np.float32) / np.float32(px.sum()) if self.n else px.astype(np.float32)
+        self.weights = torch.from_numpy(np.ascontiguousarray(w, np.float32)).to(self.device)
 
     @classmethod
     def from_fit(cls, fit) -> tuple["StackSet", torch.Tensor]:

@@ -248,7 +248,7 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
     n_res1 = 0 if res1_tab is None else len(res1_tab)
     t_r = torch.from_numpy(np.ascontiguousarray(res1_tab)).to(dev) if n_res1 else None
     out = torch.empty((th, tw, 3), dtype=torch.float32, device=dev)
-    items = decode_items(descs)
+    items = decode_items(descs, th, tw, prims)
     t_i = torch.from_numpy(items).to(dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     lib = _lib.lib_for_device(dev.index)
@@ -365,7 +365,7 @@ def raster_bench(fit, tiles, patches, size, out_w, out_h, iters, peak):
     t_p = torch.from_numpy(prims.view(np.uint8)).to(dev)
     t_c = torch.from_numpy(np.ascontiguousarray(cp48)).to(dev) if len(cp48) else None
     t_r = torch.from_numpy(np.ascontiguousarray(res1_tab)).to(dev)
-    items = decode_items(descs)
+    items = decode_items(descs, th, tw, prims)
     t_i = torch.from_numpy(items).to(dev)
     img = torch.zeros((th, tw, 3), dtype=torch.float32, device=dev)
     base = torch.empty_like(img)
@@ -754,7 +754,7 @@ def differentiable_fit(args, executor, local, stream):
 
 def image_batch_fit(args, executor, local, stream):
     """The multi-image workload (``--batch-images``, e.g. "16x256,16x512,16x1024,16x2048"): images
-    of the canonical generator (seeds 0.., primitives scaled with area, 50-2500), all tiles in one
+    of the canonical generator (seeds 0.., primitives rising from 50 to 2500 over the list), all tiles in one
     plain batched fit and in one refined fit; MPix/s of both and each image's RD."""
     import torch
 
@@ -767,7 +767,8 @@ def image_batch_fit(args, executor, local, stream):
     ims = []
     t0 = time.perf_counter()
     for seed, side in enumerate(specs):
-        n_prims = int(min(2500, max(50, round(2500 * (side / 2048) ** 2))))
+        # image i of n: 50 + 2450 i / (n - 1) primitives (50 .. 2500; seeds 0 .. n - 1)
+        n_prims = 50 + (2450 * seed) // max(1, len(specs) - 1)
         ims.append(prepare_image(make_image_u8(side, side, n_prims, seed), QUALITY, executor))
     cand_s = time.perf_counter() - t0
     batch = ImageBatch(ims, QUALITY, CAP, device=local)

@@ -116,22 +116,24 @@ int weftk_score_evals_host(const WeftEval* h_evals, int n_evals, const WeftPrim*
  * are left untouched.  Replaces decode_tile_pixels (src/weft/gpu_render.py:179-237)
  * behind gpu_render_tiles_to_image (:594-690) with the semantics of
  * render_scene_adaptive (src/weft/render.py:270-358).
- *   d_items [n_items] work items (tile index, first chunk).  Each row of a tile's
- *                     target rect is covered by 4-pixel groups aligned to output x
- *                     multiples of 4: G = floor((x0 + w + 3) / 4) - floor(x0 / 4)
- *                     groups per row, G * h per tile, row-major; a chunk is
- *                     WEFTK_DECODE_CHUNK_GROUPS groups and an item covers
- *                     WEFTK_DECODE_ITEM_CHUNKS consecutive chunks, i.e. tile t
- *                     contributes items (t, 0), (t, 8), ... below
- *                     ceil(G * h / WEFTK_DECODE_CHUNK_GROUPS)
+ *   d_items [n_items] work items (tile index, first row).  Each row of a tile's
+ *                     target rect touches G = floor((x0 + w + 3) / 4) - floor(x0 / 4)
+ *                     4-pixel groups aligned to output x multiples of 4; an item
+ *                     covers R = max(1, WEFTK_DECODE_ITEM_GROUPS / G) consecutive rows
+ *                     of its tile, i.e. tile t contributes items (t, r0), (t, r0 + R),
+ *                     ... for the rows r0 <= r < r1 of its rect that lie inside the
+ *                     image (r0 = max(0, -y0), r1 = min(h, out_h - y0)).  Rows of an
+ *                     item outside the image are skipped.  Any order renders the same
+ *                     image; in descending order of cost (pixels, times 4 for a tile
+ *                     evaluated per pixel, i.e. anything but a lone constant layer
+ *                     without a RES1 grid) the warps finish together.
  *   d_cp48  [n_cp48 * 48]  control grids for kind-5 tiles (may be NULL)
  *   d_res1  [n_res1 * 48]  RES1 grids, (4, 4, 3) row-major, float (may be NULL;
  *                          res1_index is ignored when n_res1 == 0)
  * Tiles with more than 48 primitives, a rect side outside 1..8192 or an
  * out-of-range grid index are skipped and reported through weftk_device_status.
  */
-#define WEFTK_DECODE_CHUNK_GROUPS 32
-#define WEFTK_DECODE_ITEM_CHUNKS 8
+#define WEFTK_DECODE_ITEM_GROUPS 256
 int weftk_render_tiles(const WeftTileDecodeDesc* d_descs, int n_tiles, const int32_t* d_items, int n_items,
                        const WeftPrim* d_prims, const float* d_cp48, int n_cp48, const float* d_res1, int n_res1,
                        float* d_out, int out_h, int out_w, int flags, void* stream);

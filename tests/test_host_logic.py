@@ -13,22 +13,37 @@ from weft_b200 import render
 from weft_b200._lib import TILE_DECODE_DTYPE
 
 
-def test_decode_items_cover_every_chunk_once():
+def test_decode_items_cover_every_visible_row_once():
     rng = np.random.default_rng(3)
     n = 200
+    out_h, out_w = 1500, 2500
     d = np.zeros(n, TILE_DECODE_DTYPE)
-    d["target_x0"] = rng.integers(-5, 3000, n)
-    d["target_y0"] = rng.integers(0, 2000, n)
+    d["target_x0"] = rng.integers(-40, 3000, n)
+    d["target_y0"] = rng.integers(-40, 2000, n)
     d["target_w"] = rng.integers(1, 300, n)
     d["target_h"] = rng.integers(1, 300, n)
-    items = render.decode_items(d)
-    k = render.DECODE_ITEM_CHUNKS
+    items = render.decode_items(d, out_h, out_w)
     for t in range(n):
-        x0, w, h = int(d["target_x0"][t]), int(d["target_w"][t]), int(d["target_h"][t])
-        groups = ((x0 + w + 3) // 4 - x0 // 4) * h  # floor division, as the kernel
-        chunks = -(-groups // render.DECODE_CHUNK_GROUPS)
-        starts = sorted(int(c) for tt, c in items if tt == t)
-        assert starts == list(range(0, chunks, k))
+        x0, y0, w, h = (int(d[k][t]) for k in ("target_x0", "target_y0", "target_w", "target_h"))
+        groups = (x0 + w + 3) // 4 - x0 // 4  # floor division, as the kernel
+        rows = max(1, render.DECODE_ITEM_GROUPS // groups)
+        covered = []
+        for tt, r in items:
+            if tt == t:
+                covered += range(int(r), min(int(r) + rows, h))
+        visible = x0 < out_w and x0 + w > 0
+        expect = [r for r in range(h) if 0 <= y0 + r < out_h] if visible else []
+        assert sorted(c for c in covered if 0 <= y0 + c < out_h) == expect
+        assert len(covered) == len(set(covered))
+        assert all(0 <= c < h for c in covered)
+    # descending cost: rows x width (every tile without a RES1 grid and prims counts as a fill)
+    x = d["target_x0"].astype(np.int64)
+    g = (x + d["target_w"] + 3) // 4 - x // 4
+    rows = np.maximum(1, render.DECODE_ITEM_GROUPS // g)
+    t_, r_ = items[:, 0], items[:, 1].astype(np.int64)
+    n_rows = np.minimum(r_ + rows[t_], np.minimum(d["target_h"][t_], out_h - d["target_y0"][t_])) - r_
+    cost = n_rows * d["target_w"][t_]
+    assert np.all(np.diff(cost) <= 0)
 
 
 def test_refine_flop_count_follows_the_per_kind_table():

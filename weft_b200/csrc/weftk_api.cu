@@ -167,14 +167,23 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
     (void)flags;
     WEFTK_REQUIRE(n_tiles >= 0 && out_h > 0 && out_w > 0 && h_out && n_prims >= 0 && n_cp48 >= 0 && n_res1 >= 0,
                   "render_tiles_host: bad arguments");
-    std::vector<int2> items;
+    // work items (tile, first row) in descending cost order (pixels, times 4 for a tile
+    // evaluated per pixel: anything but a lone constant layer without a RES1 grid)
+    std::vector<std::pair<long long, int2>> costed;
     for (int i = 0; i < n_tiles; ++i) {
         const WeftTileDecodeDesc& d = h_descs[i];
-        if (d.target_w > 0 && d.target_h > 0) {
+        if (d.target_w > 0 && d.target_h > 0 && d.target_w <= 8192 && d.target_h <= 8192) {
             auto fdiv4 = [](long long v) { return v >= 0 ? v / 4 : -((-v + 3) / 4); };
             const long long G = fdiv4((long long)d.target_x0 + d.target_w + 3) - fdiv4(d.target_x0);
-            const long long chunks = (G * d.target_h + WEFTK_DECODE_CHUNK_GROUPS - 1) / WEFTK_DECODE_CHUNK_GROUPS;
-            for (long long c = 0; c < chunks; c += WEFTK_DECODE_ITEM_CHUNKS) items.push_back(make_int2(i, (int)c));
+            const long long R = std::max(1LL, WEFTK_DECODE_ITEM_GROUPS / G);
+            const long long r0 = std::max(0LL, -(long long)d.target_y0);
+            const long long r1 = std::min((long long)d.target_h, (long long)out_h - d.target_y0);
+            const bool cols = (long long)d.target_x0 < out_w && (long long)d.target_x0 + d.target_w > 0;
+            const bool fill = d.res1_index < 0 && d.prim_count == 1 && d.prim_offset >= 0 &&
+                              d.prim_offset < n_prims && h_prims[d.prim_offset].kind == 0;
+            if (cols)
+                for (long long r = r0; r < r1; r += R)
+                    costed.push_back({std::min(R, r1 - r) * d.target_w * (fill ? 1 : 4), make_int2(i, (int)r)});
         }
         if (d.prim_count < 0 || d.prim_count > 48 || d.prim_offset < 0 || (int64_t)d.prim_offset + d.prim_count > n_prims ||
             d.target_w <= 0 || d.target_h <= 0 || d.target_w > 8192 || d.target_h > 8192 || d.source_size <= 0 ||
@@ -185,6 +194,10 @@ int weftk_render_tiles_host(const WeftTileDecodeDesc* h_descs, int n_tiles, cons
             if (idx < 0 || idx >= n_cp48) return fail(WEFTK_E_ARG, "render_tiles_host: bad bicubic grid index");
         }
     }
+    std::stable_sort(costed.begin(), costed.end(),
+                     [](const std::pair<long long, int2>& x, const std::pair<long long, int2>& y) { return x.first > y.first; });
+    std::vector<int2> items(costed.size());
+    for (size_t k = 0; k < costed.size(); ++k) items[k] = costed[k].second;
     std::lock_guard<std::mutex> lock(g_arena_mu);
     Arena* a = nullptr;
     int rc = arena_for_current(&a);

@@ -21,22 +21,40 @@ from . import _lib
 from ._lib import PRIM_DTYPE, TILE_DECODE_DTYPE
 
 MAX_TILE_PRIMS = 48
-DECODE_CHUNK_GROUPS = 32   # WEFTK_DECODE_CHUNK_GROUPS
-DECODE_ITEM_CHUNKS = 8     # WEFTK_DECODE_ITEM_CHUNKS
+DECODE_ITEM_GROUPS = 256   # WEFTK_DECODE_ITEM_GROUPS
+ITEM_PIXEL_WORK = 4        # cost of a pixel evaluated per pixel, in pixels of a constant fill
 
 
-def decode_items(descs: np.ndarray) -> np.ndarray:
-    """Work items (tile, first chunk) of weftk_render_tiles, int32 (n, 2).
+def decode_items(descs: np.ndarray, out_h: int, out_w: int, prims: np.ndarray | None = None) -> np.ndarray:
+    """Work items (tile, first row) of weftk_render_tiles, int32 (n, 2), in descending cost order.
 
-    A tile's rect rows are covered by 4-pixel groups aligned to output x multiples of 4.
+    A rect row touches G 4-pixel groups aligned to output x multiples of 4; an item covers
+    max(1, DECODE_ITEM_GROUPS // G) rows of its tile.  Only the rows inside the out_h x out_w
+    image get items.  The cost of an item is its pixel count, times ITEM_PIXEL_WORK for a tile
+    that is evaluated per pixel (anything but a lone constant layer without a RES1 grid; with
+    ``prims`` None every tile without a RES1 grid counts as a lone constant layer).
     """
     x0 = descs["target_x0"].astype(np.int64)
-    groups = (np.floor_divide(x0 + descs["target_w"] + 3, 4) - np.floor_divide(x0, 4)) * descs["target_h"]
-    chunks = (groups + DECODE_CHUNK_GROUPS - 1) // DECODE_CHUNK_GROUPS
-    per = (chunks + DECODE_ITEM_CHUNKS - 1) // DECODE_ITEM_CHUNKS
+    y0 = descs["target_y0"].astype(np.int64)
+    w = descs["target_w"].astype(np.int64)
+    h = descs["target_h"].astype(np.int64)
+    g = np.floor_divide(x0 + w + 3, 4) - np.floor_divide(x0, 4)
+    rows = np.maximum(1, DECODE_ITEM_GROUPS // np.maximum(g, 1))
+    r0 = np.maximum(0, -y0)
+    r1 = np.minimum(h, out_h - y0)
+    visible = (w > 0) & (h > 0) & (x0 < out_w) & (x0 + w > 0) & (r1 > r0)
+    per = np.where(visible, (r1 - r0 + rows - 1) // rows, 0)
     tile = np.repeat(np.arange(len(descs)), per)
     k = np.arange(int(per.sum())) - np.repeat(np.concatenate([[0], np.cumsum(per)[:-1]]), per)
-    return np.stack([tile, k * DECODE_ITEM_CHUNKS], axis=1).astype(np.int32)
+    first = np.repeat(r0, per) + k * np.repeat(rows, per)
+    per_pixel = descs["res1_index"] >= 0
+    if prims is not None and len(prims):
+        off = np.clip(descs["prim_offset"], 0, len(prims) - 1)
+        per_pixel = per_pixel | (descs["prim_count"] != 1) | (prims["kind"][off] != 0)
+    n_rows = np.minimum(first + np.repeat(rows, per), np.repeat(r1, per)) - first
+    cost = n_rows * np.repeat(w, per) * np.where(np.repeat(per_pixel, per), ITEM_PIXEL_WORK, 1)
+    order = np.argsort(-cost, kind="stable")
+    return np.stack([tile[order], first[order]], axis=1).astype(np.int32)
 
 
 def pack_records(stacks) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
@@ -152,7 +170,7 @@ def render_scene_device(records, quad_tiles, width: int, height: int, residual_m
     out = torch.zeros((th, tw, 3), dtype=torch.float32, device=dev)
     if len(descs) == 0:
         return out
-    items = decode_items(descs)
+    items = decode_items(descs, th, tw, prims)
     t_d = torch.from_numpy(np.ascontiguousarray(descs, TILE_DECODE_DTYPE).view(np.uint8)).to(dev)
     t_i = torch.from_numpy(items).to(dev)
     t_p = torch.from_numpy(np.ascontiguousarray(prims, PRIM_DTYPE).view(np.uint8)).to(dev)

@@ -914,6 +914,8 @@ def main():
     ap.add_argument("--batch-images", default="",
                     help='multi-image batch, e.g. "16x256,16x512,16x1024,16x2048" (empty: skip)')
     ap.add_argument("--batch-steps", type=int, default=100, help="Adam steps of the multi-image refined fit")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="only the multi-image batch (--batch-images, default the 64-image set), one JSON line")
     ap.add_argument("--profile-refined", action="store_true",
                     help="only the refined fit with device pool generation (eager launches), for profilers")
     args = ap.parse_args()
@@ -956,9 +958,33 @@ def profile_refined(args, local, patches):
     print(json.dumps({"profile_refined": {"tiles": len(sizes), "steps": args.warmup + args.steps}}), flush=True)
 
 
+def batch_only(args, local, executor, cores):
+    """The multi-image workload alone: 64 images (16 each of 256^2, 512^2, 1024^2, 2048^2) unless
+    --batch-images names another set; all tiles in one plain fit and one refined fit."""
+    import torch
+
+    torch.cuda.set_device(local)
+    if not args.batch_images:
+        args.batch_images = "16x256,16x512,16x1024,16x2048"
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(local)
+    sampler.start()
+    r = image_batch_fit(args, executor, local, stream)
+    clocks = sampler.stop()
+    iso = r["images_within_0.05db"] == r["n_images"]
+    print(json.dumps({"metric": METRIC, "value": r["refined_mpix_per_s"] if iso else r["plain_mpix_per_s"],
+                      "unit": "MPix/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": f"multi-image batch {r['images']}, seeds 0..{r['n_images'] - 1}, "
+                                             f"q=75, cap {CAP}", "tiles": r["tiles"], "mpix": r["mpix"]},
+                      "clocks": clocks, "host_processes": cores, "image_batch": r}), flush=True)
+
+
 def run_weft(args, world, rank, local, executor, cores):
     import torch
 
+    if args.batch_only:
+        batch_only(args, local, executor, cores)
+        return
     if args.profile_refined:
         u8 = make_image_u8(args.size, args.size, args.prims, rank)
         img = srgb_u8_to_linear(u8)

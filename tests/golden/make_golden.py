@@ -742,6 +742,66 @@ def gen_container_dct(ref) -> None:
     _save("container_dct.npz", **out)
 
 
+def gen_bicubic(ref) -> None:
+    """The per-tile bicubic R-D swap of ``_fit_adaptive_state`` (src/weft/encoder.py:2841-2873).
+
+    (a) ``bicubic.fit_tile`` / ``eval_tile`` (src/weft/bicubic.py:65-110) on tiles of every size
+    (noise, smooth, step edges, values beyond [0, 1] that the fit clips), with the control grid
+    rounded to u8 steps as the swap does; (b) three fits whose state's ``bicubic_replaced_per_tile``
+    gives the swap decisions: the selected stacks, the tile patches and lambda go in, the swapped
+    flags and control grids come out."""
+    from weft_b200.synth import make_image_u8
+
+    bic = ref["bicubic"]
+    rng = np.random.default_rng(17)
+    tiles, cps, cpq, mse = [], [], [], []
+    for ts in (8, 16, 32, 64):
+        yy, xx = np.meshgrid(np.linspace(0, 1, ts), np.linspace(0, 1, ts), indexing="ij")
+        cases = [rng.random((ts, ts, 3)),
+                 np.stack([0.2 + 0.6 * xx, 0.1 + 0.5 * yy * xx, 0.9 - 0.7 * yy], -1),
+                 np.where((xx + 0.3 * yy > 0.55)[..., None], [0.9, 0.2, 0.1], [0.05, 0.6, 0.95]),
+                 np.clip(rng.normal(0.5, 0.6, (ts, ts, 3)), -0.2, 1.3)]
+        for c in cases:
+            t = np.ascontiguousarray(c, np.float32)
+            cp = bic.fit_tile(t)
+            q = np.round(np.clip(cp, 0.0, 1.0) * 255.0) / 255.0
+            r = bic.eval_tile(q, ts)
+            tiles.append(t.reshape(-1))
+            cps.append(cp.reshape(-1))
+            cpq.append(q.reshape(-1))
+            mse.append(float(np.mean((t - r) ** 2)))
+    sizes = np.repeat([8, 16, 32, 64], 4).astype(np.int32)
+    out = dict(tile_sizes=sizes, tiles=np.concatenate(tiles), cp=np.stack(cps).astype(np.float32),
+               cp_q=np.stack(cpq).astype(np.float32),
+               mse=np.array(mse, np.float64))
+    from PIL import Image
+
+    for name, size, n_prims, seed, quality in (("a", 64, 10, 5, 75), ("b", 64, 30, 11, 92), ("c", 64, 40, 2, 97)):
+        img_u8 = make_image_u8(size, size, n_prims, seed)
+        with _FitCapture(ref) as cap, tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "in.png")
+            Image.fromarray(img_u8).save(path)
+            ref["encoder"]._fit_adaptive_state(path, ref["EncodeConfig"](quality=quality))
+        st = cap.state
+        sel = st.selected_per_tile
+        swapped = np.array([len(b) == 1 and b[0].kind == 5 and not (len(s) == 1 and s[0] is b[0])
+                            for s, b in zip(sel, st.bicubic_replaced_per_tile)], np.int8)
+        grids = np.zeros((len(sel), 48), np.float32)
+        for i, b in enumerate(st.bicubic_replaced_per_tile):
+            if swapped[i]:
+                grids[i] = np.asarray(b[0].geom, np.float32)
+        packed = _concat_packs([_pack_full(s) for s in sel])
+        print(f"bicubic {name}: q={quality}, {len(sel)} tiles, {int(swapped.sum())} swapped "
+              f"(state says {st.n_bicubic_tiles})")
+        assert int(swapped.sum()) == st.n_bicubic_tiles
+        out.update({f"{name}_image": st.image.astype(np.float32),
+                    f"{name}_qt": np.array([(q.x, q.y, q.size) for q in st.quad_tiles], np.int32),
+                    f"{name}_lam": np.float64(st.lam), f"{name}_quality": np.int32(quality),
+                    f"{name}_swapped": swapped, f"{name}_grids": grids,
+                    **{f"{name}_sel_{k}": v for k, v in packed.items()}})
+    _save("bicubic.npz", **out)
+
+
 def main() -> None:
     args = sys.argv[1:]
     src = os.environ.get("WEFT_REFERENCE_SRC")
@@ -750,6 +810,7 @@ def main() -> None:
     if not src:
         sys.exit("usage: make_golden.py REFERENCE_SRC [fixture ...]  (or set WEFT_REFERENCE_SRC)")
     sys.path.insert(0, src)
+    import weft.bicubic as bicubic
     import weft.bitstream as bitstream_mod
     import weft.dct_residual as dct_residual
     import weft.decoder as decoder
@@ -766,7 +827,7 @@ def main() -> None:
         "encoder": encoder, "entropy": entropy, "gpu_render": gpu_render, "prim_chunks": prim_chunks,
         "primitives": primitives, "quadtree": quadtree, "render": render,
         "Primitive": primitives.Primitive, "TileRecord": primitives.TileRecord, "EncodeConfig": EncodeConfig,
-        "decoder": decoder, "bitstream": bitstream_mod, "dct_residual": dct_residual,
+        "decoder": decoder, "bitstream": bitstream_mod, "dct_residual": dct_residual, "bicubic": bicubic,
     }
     which = set(args) if args else None
     for name, fn in (("render_tiles", gen_render_tiles), ("render_scene", gen_render_scene), ("rate", gen_rate),
@@ -774,7 +835,7 @@ def main() -> None:
                      ("candidates", gen_candidates), ("fit", gen_fit),
                      ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("fit_cfg256", gen_fit_cfg256),
                      ("container", gen_container),
-                     ("dct", gen_dct), ("container_dct", gen_container_dct)):
+                     ("dct", gen_dct), ("container_dct", gen_container_dct), ("bicubic", gen_bicubic)):
         if which is None or name in which:
             fn(ref)
 

@@ -187,3 +187,41 @@ def test_greedy_fit_matches_reference_on_fixed_32px_tiles(golden):
                                      lambda i, patch, pred: queue[i].pop(0), caps=[8] * n)
     assert sel == [[int(v) for v in row if v >= 0] for row in g["selected"][:n]]
     assert stats["reseeds"] == 3 * n and all(len(v) == 0 for v in queue.values())
+
+
+def bicubic_swap_inputs(g, name: str):
+    """Patches, selected stacks and lambda of one of the bicubic fixture's fits."""
+    tiles = [quadtree.QTile(int(x), int(y), int(s)) for x, y, s in g[f"{name}_qt"]]
+    patches = quadtree.extract(g[f"{name}_image"], tiles)
+    sel = _pack(g, f"{name}_sel_")
+    stacks = [prims_from_pack(sel, int(sel["offsets"][i]), int(sel["offsets"][i + 1])) for i in range(len(tiles))]
+    return patches, stacks, float(g[f"{name}_lam"])
+
+
+def test_bicubic_fit_matches_reference(golden):
+    from oracle import bicubic
+
+    g = golden("bicubic.npz")
+    off = 0
+    for i, ts in enumerate(g["tile_sizes"]):
+        ts = int(ts)
+        tile = g["tiles"][off:off + ts * ts * 3].reshape(ts, ts, 3)
+        off += ts * ts * 3
+        cp = bicubic.fit_tile(tile)
+        np.testing.assert_array_equal(cp.reshape(-1), g["cp"][i])
+        q = bicubic.quantize_grid(cp)
+        np.testing.assert_array_equal(q.reshape(-1), g["cp_q"][i])
+        assert float(np.mean((tile - render.bicubic_tile(q, ts)) ** 2)) == float(g["mse"][i])
+
+
+@pytest.mark.parametrize("name", ["a", "b", "c"])
+def test_bicubic_swap_matches_reference(golden, name):
+    """The swap decisions and control grids of the reference's fit at q=75 / 92 / 97."""
+    from oracle import bicubic
+
+    g = golden("bicubic.npz")
+    patches, stacks, lam = bicubic_swap_inputs(g, name)
+    flags, grids, _, _ = bicubic.swap(patches, stacks, lam)
+    np.testing.assert_array_equal(flags, g[f"{name}_swapped"].astype(bool))
+    np.testing.assert_array_equal(grids[flags], g[f"{name}_grids"][flags])
+    assert 0 < flags.sum() < len(flags)

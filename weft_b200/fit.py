@@ -691,6 +691,16 @@ class BatchedFit:
         """The selected primitives of every tile as ``Cand`` objects (float32-rounded values)."""
         return [unpack_cands(r) for r in self.selected_records()]
 
+    def bicubic_swap(self):
+        """The reference fit's per-tile bicubic alternative (``bicubic_replaced_per_tile``,
+        src/weft/encoder.py:2841-2873) for this fit's selections: (replace flags, u8-rounded
+        control grids (n, 48), the stacks with the replaced tiles as kind-5 primitives)."""
+        from . import bicubic
+
+        stacks = self.selected()
+        flags, grids, _ = bicubic.swap(self.t_src, self.t_px_off, self.t_size, stacks, self.quality)
+        return flags, grids, bicubic.replaced_stacks(stacks, flags, grids)
+
     def stack_set(self):
         """The selected stacks as a ``refine.StackSet`` over this fit's resident tiles, with the
         parameter rows gathered on the device (no host round trip of the records)."""

@@ -290,14 +290,19 @@ __host__ __device__ __forceinline__ GroupLayout group_layout(int L, int wpt, boo
 // Adam (PyTorch's update rule, FP32) for one value at step t (1-based), then the
 // projection onto what the wire format carries: colours and alpha in [0, 1],
 // coordinates in [0, 15], thickness in [0, 4] (src/weft/primitives.py:102-177).
+// Projection of column col of a row onto its valid range (colours and alpha [0, 1], thickness
+// [0, 4], other geometry [0, 15]).
+__device__ __forceinline__ float adam_project(float x, int kind, int col) {
+    if (col >= 7) return fminf(fmaxf(x, 0.0f), 1.0f);
+    const bool thick = (kind == K_LINE && col == 4) || (kind == K_CURVE && col == 6);
+    return fminf(fmaxf(x, 0.0f), thick ? 4.0f : 15.0f);
+}
+
 __device__ __forceinline__ float adam_update_bc(float p, float g, float& m, float& v, float bc1, float bc2, float lr,
                                                 float b1, float b2, float eps, int kind, int col) {
     m = fmaf(b1, m, (1.0f - b1) * g);
     v = fmaf(b2, v, (1.0f - b2) * g * g);
-    float x = p - lr * (m / bc1) / (sqrtf(v / bc2) + eps);
-    if (col >= 7) return fminf(fmaxf(x, 0.0f), 1.0f);
-    const bool thick = (kind == K_LINE && col == 4) || (kind == K_CURVE && col == 6);
-    return fminf(fmaxf(x, 0.0f), thick ? 4.0f : 15.0f);
+    return adam_project(p - lr * (m / bc1) / (sqrtf(v / bc2) + eps), kind, col);
 }
 
 // Bias corrections 1 - beta^t of step t (1-based).
@@ -984,6 +989,13 @@ __global__ void __launch_bounds__(128) refine_const_kernel(WeftStackSet set, flo
         v[i] = MODE == RF_STEP ? adam.v[(size_t)p0 * 16 + i] : 0.0f;
     }
     const float scale = BWD ? grad_loss[t] * 2.0f / (3.0f * (float)n) : 0.0f;
+    // Columns other than the colour (7..9) and alpha (13) have zero gradient.  Where their moments
+    // start at zero an Adam update leaves them at zero and moves the value by exactly 0, so such a
+    // column only takes the projection, at the first step.
+    unsigned idle = 0;
+#pragma unroll
+    for (int j = 0; j < 14; ++j)
+        if (!(j >= 7 && j <= 9) && j != 13 && m[j] == 0.0f && v[j] == 0.0f) idle |= 1u << j;
     double sse = 0.0;
     float g4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     for (int step = 0; step < n_steps; ++step) {
@@ -994,6 +1006,10 @@ __global__ void __launch_bounds__(128) refine_const_kernel(WeftStackSet set, flo
             adam_bias(adam.b1, adam.b2, m[15] + 1.0f, m[14], v[14]);
 #pragma unroll
             for (int j = 0; j < 14; ++j) {
+                if ((idle >> j) & 1u) {
+                    if (step == 0) r[j] = adam_project(r[j], K_CONST, j);
+                    continue;
+                }
                 const float gj = j >= 7 && j <= 9 ? g4[j - 7] : j == 13 ? g4[3] : 0.0f;
                 r[j] = adam_update_bc(r[j], gj, m[j], v[j], m[14], v[14], adam.lr, adam.b1, adam.b2, adam.eps,
                                      K_CONST, j);
@@ -1015,6 +1031,28 @@ __global__ void __launch_bounds__(128) refine_const_kernel(WeftStackSet set, flo
         }
     }
     if (loss != nullptr) loss[t] = (float)(sse / (3.0 * n));
+}
+
+// A side stream of the current device for the calling host thread, with the two events that fork
+// work onto it and join it back.  Created on first use and kept for the life of the process (one
+// per host thread and device, so concurrent callers never share the events).
+struct SideStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+static int side_stream(SideStream** out) {
+    thread_local std::map<int, SideStream> per_device;
+    int dev = 0;
+    WEFTK_CUDA(cudaGetDevice(&dev));
+    SideStream& s = per_device[dev];
+    if (s.stream == nullptr) {
+        WEFTK_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        WEFTK_CUDA(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+        WEFTK_CUDA(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
+    }
+    *out = &s;
+    return WEFTK_OK;
 }
 
 template <int MODE>
@@ -1073,9 +1111,21 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
             have = smem;
         }
     }
-    if (cl1 && set.moments != nullptr && !(flags & WEFTK_LOSS_RESIDUAL))
-        refine_const_kernel<MODE><<<(set.n_tiles + 127) / 128, 128, 0, stream>>>(set, params, grad_loss, grad, loss,
-                                                                                  adam, n_steps);
+    // lone constant layers (closed form, a thread per tile) run beside the other tiles' launch, on
+    // this thread's side stream of the device (forked from and joined back into `stream`, which a
+    // CUDA graph capture follows)
+    const bool const_side = cl1 && set.moments != nullptr && !(flags & WEFTK_LOSS_RESIDUAL);
+    SideStream* side = nullptr;
+    if (const_side) {
+        int rc = side_stream(&side);
+        if (rc) return rc;
+        WEFTK_CUDA(cudaEventRecord(side->fork, stream));
+        WEFTK_CUDA(cudaStreamWaitEvent(side->stream, side->fork, 0));
+        refine_const_kernel<MODE><<<(set.n_tiles + 127) / 128, 128, 0, side->stream>>>(set, params, grad_loss, grad,
+                                                                                        loss, adam, n_steps);
+        WEFTK_CUDA(cudaGetLastError());
+        WEFTK_CUDA(cudaEventRecord(side->join, side->stream));
+    }
     if (cl1)
         refine_tiles_kernel<MODE, true><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss, flags,
                                                                             plan, L, adam, n_steps);
@@ -1083,6 +1133,7 @@ static int launch_refine(const WeftStackSet& set, float* params, const float* gr
         refine_tiles_kernel<MODE, false><<<ctas, RF_THREADS, smem, stream>>>(set, params, grad_loss, grad, loss,
                                                                              flags, plan, L, adam, n_steps);
     WEFTK_CUDA(cudaGetLastError());
+    if (side) WEFTK_CUDA(cudaStreamWaitEvent(stream, side->join, 0));
     return WEFTK_OK;
 }
 

@@ -46,6 +46,9 @@ What is captured (reference function -> fixture):
     smooth residuals whose low-frequency coefficients reach ~800)
     (src/weft/decoder.py:477-507), and Pillow ``Image.resize(BILINEAR)`` of u8
     images (src/weft/decoder.py:514-518)                    -> dct.npz
+  * the first three ``gpu_batch_score_prepacked`` calls of the reference's fit, arguments as
+    passed, with the CPU stand-in's MSEs (src/weft/encoder.py:2698-2811)
+                                                            -> launcher_calls.npz
   * ``encoder.encode_image`` with the DCT residual layer, decoded by
     ``decoder.decode_to_array`` at the encoded size and at up/down-scaled
     targets (the raster branch)                             -> container_dct.npz
@@ -802,6 +805,50 @@ def gen_bicubic(ref) -> None:
     _save("bicubic.npz", **out)
 
 
+def gen_launcher_calls(ref) -> None:
+    """The first three calls the reference's fit makes to ``gpu_batch_score_prepacked`` (the init
+    round, the selected stacks' current objective and the first greedy round of the fit_small
+    workload, src/weft/encoder.py:2698-2811),
+    with their arguments exactly as the fit passes them and the MSEs of the CPU stand-in (the
+    reference's ``render_tile`` at pixel centres)."""
+    from PIL import Image
+    from weft_b200.synth import make_image_u8
+
+    calls = []
+    img_u8 = make_image_u8(64, 64, 10, 5)
+    with _FitCapture(ref) as cap, tempfile.TemporaryDirectory() as td:
+        gr = ref["gpu_render"]
+        inner = gr.gpu_batch_score_prepacked
+
+        def recording(*args):
+            out = inner(*args)
+            if len(calls) < 3:
+                calls.append((args, out))
+            return out
+
+        gr.gpu_batch_score_prepacked = recording
+        path = os.path.join(td, "in.png")
+        Image.fromarray(img_u8).save(path)
+        ref["encoder"]._fit_adaptive_state(path, ref["EncodeConfig"](quality=75))
+    out = {"quality": np.int32(75), "selected": cap.arrays()["selected"], "n_calls": np.int32(len(calls))}
+    for i, (args, res) in enumerate(calls):
+        flat, offsets, tidx, tsizes, prim_arrays, prim_counts = args
+        keys = sorted(offsets)
+        out[f"c{i}_pixels"] = np.asarray(flat, np.float32)
+        out[f"c{i}_offset_keys"] = np.array(keys, np.int64)
+        out[f"c{i}_offset_vals"] = np.array([offsets[k] for k in keys], np.int64)
+        out[f"c{i}_tile_indices"] = np.array(tidx, np.int64)
+        out[f"c{i}_tile_sizes"] = np.array(tsizes, np.int64)
+        out[f"c{i}_prims"] = np.concatenate([np.ascontiguousarray(a).view(np.uint8) for a in prim_arrays])
+        out[f"c{i}_prim_len"] = np.array([len(a) for a in prim_arrays], np.int64)
+        out[f"c{i}_counts"] = np.concatenate([np.asarray(c, np.int32) for c in prim_counts])
+        out[f"c{i}_count_len"] = np.array([len(c) for c in prim_counts], np.int64)
+        out[f"c{i}_mse"] = np.concatenate([np.asarray(r, np.float32) for r in res])
+        print(f"launcher call {i}: {len(tidx)} tiles, {len(out[f'c{i}_counts'])} evals, "
+              f"{int(out[f'c{i}_prim_len'].sum())} records")
+    _save("launcher_calls.npz", **out)
+
+
 def main() -> None:
     args = sys.argv[1:]
     src = os.environ.get("WEFT_REFERENCE_SRC")
@@ -835,7 +882,8 @@ def main() -> None:
                      ("candidates", gen_candidates), ("fit", gen_fit),
                      ("fit_hq", lambda r: gen_fit(r, "fit_hq.npz", 40, 8, 3, 92)), ("fit_cfg256", gen_fit_cfg256),
                      ("container", gen_container),
-                     ("dct", gen_dct), ("container_dct", gen_container_dct), ("bicubic", gen_bicubic)):
+                     ("dct", gen_dct), ("container_dct", gen_container_dct), ("bicubic", gen_bicubic),
+                     ("launcher_calls", gen_launcher_calls)):
         if which is None or name in which:
             fn(ref)
 

@@ -225,3 +225,19 @@ def test_bicubic_swap_matches_reference(golden, name):
     np.testing.assert_array_equal(flags, g[f"{name}_swapped"].astype(bool))
     np.testing.assert_array_equal(grids[flags], g[f"{name}_grids"][flags])
     assert 0 < flags.sum() < len(flags)
+
+
+def test_recorded_launcher_calls_give_the_reference_decisions(golden):
+    """The recorded launcher calls of the reference's fit (what tests/test_dropin_gpu.py replays
+    through the installed drop-in) carry its decisions: the init round's argmin by mse + lambda * bits
+    is the first selection of every tile, and the first greedy round improves no tile."""
+    from tests.test_dropin_gpu import objectives, recorded_calls
+
+    g = golden("launcher_calls.npz")
+    lam = rate.tile_lambda(int(g["quality"]))
+    (a0, w0), (a1, w1), (a2, w2) = recorded_calls(g)
+    assert [int(np.argmin(objectives(m, a, c, lam))) for m, a, c in zip(w0, a0[4], a0[5])] == \
+        [int(row[0]) for row in g["selected"]]
+    cur = [objectives(m, a, c, lam)[0] for m, a, c in zip(w1, a1[4], a1[5])]
+    best = [objectives(m, a, c, lam).min() for m, a, c in zip(w2, a2[4], a2[5])]
+    assert all(b >= c for b, c in zip(best, cur))

@@ -168,7 +168,10 @@ struct ScoreSmem {
 };
 
 // One scoring work item (tile, 1024-pixel block, run of candidate slots) by the whole CTA.
-template <int PPL, int WPC>
+// INIT: the init round, over empty stacks: the cached composite is black, so it is not read and the
+// blend over it is the product s * a (the fused form over +0 differs only in the sign of a zero
+// result, which the clamp removes), the same values as the general form.
+template <int PPL, int WPC, bool INIT>
 __device__ __forceinline__ void score_item(const WeftFitState& st, const int* __restrict__ perm, const WeftFitItem w,
                                            int expect_min, int expect_max, bool mode_init, ScoreSmem<WPC>& sm) {
     constexpr int GROUPS = 4 / WPC;
@@ -255,9 +258,14 @@ __device__ __forceinline__ void score_item(const WeftFitState& st, const int* __
         const int p = pbase + j * 32 + lane;
         fx[j] = (float)(p % ts) + 0.5f;
         fy[j] = (float)(p / ts) + 0.5f;
-        const float4 a = src[p], b = bg[p];
+        const float4 a = src[p];
         s[j] = make_float3(a.x, a.y, a.z);
-        g[j] = make_float3(b.x, b.y, b.z);
+        if (INIT) {
+            g[j] = make_float3(0.0f, 0.0f, 0.0f);
+        } else {
+            const float4 b = bg[p];
+            g[j] = make_float3(b.x, b.y, b.z);
+        }
     }
     for (int c = group; c < m; c += GROUPS) {
         Prep P;
@@ -289,9 +297,9 @@ __device__ __forceinline__ void score_item(const WeftFitState& st, const int* __
         float e = 0.0f;
 #pragma unroll
         for (int j = 0; j < PPL; ++j) {
-            const float dr = clamp01(blend(sr[j], a[j], g[j].x)) - s[j].x;
-            const float dg = clamp01(blend(sg[j], a[j], g[j].y)) - s[j].y;
-            const float db = clamp01(blend(sb[j], a[j], g[j].z)) - s[j].z;
+            const float dr = clamp01(INIT ? __fmul_rn(sr[j], a[j]) : blend(sr[j], a[j], g[j].x)) - s[j].x;
+            const float dg = clamp01(INIT ? __fmul_rn(sg[j], a[j]) : blend(sg[j], a[j], g[j].y)) - s[j].y;
+            const float db = clamp01(INIT ? __fmul_rn(sb[j], a[j]) : blend(sb[j], a[j], g[j].z)) - s[j].z;
             e = fmaf(dr, dr, fmaf(dg, dg, fmaf(db, db, e)));
         }
         e = warp_sum_f(e);
@@ -329,7 +337,10 @@ __global__ void __launch_bounds__(128, MINB) fit_score_kernel(WeftFitState st, c
                                                         int expect_min, int expect_max, bool mode_init) {
     __shared__ ScoreSmem<WPC> sm;
     if ((int)blockIdx.x >= n_items) return;
-    score_item<PPL, WPC>(st, perm, items[blockIdx.x], expect_min, expect_max, mode_init, sm);
+    if (mode_init)
+        score_item<PPL, WPC, true>(st, perm, items[blockIdx.x], expect_min, expect_max, true, sm);
+    else
+        score_item<PPL, WPC, false>(st, perm, items[blockIdx.x], expect_min, expect_max, false, sm);
 }
 
 // Persistent form: a grid of about one wave of CTAs that pull the round's live items of the class
@@ -347,7 +358,10 @@ __global__ void __launch_bounds__(128, MINB) fit_score_queue_kernel(WeftFitState
         __syncthreads();
         const int i = s_i;
         if (i >= *q_len) break;
-        score_item<PPL, WPC>(st, perm, items[q_items[i]], expect_min, expect_max, mode_init, sm);
+        if (mode_init)
+            score_item<PPL, WPC, true>(st, perm, items[q_items[i]], expect_min, expect_max, true, sm);
+        else
+            score_item<PPL, WPC, false>(st, perm, items[q_items[i]], expect_min, expect_max, false, sm);
         __syncthreads();  // the item's shared buffers are free before the next pull
     }
 }

@@ -233,19 +233,68 @@ __device__ __forceinline__ void score_item(const WeftFitState& st, const int* __
     for (int k = 0; k < warp; ++k) base += s_wcount[k];
     const int m = s_wcount[0] + s_wcount[1] + s_wcount[2] + s_wcount[3];
     unsigned long long ops = 0;
+    int my_curve = 0;
     if (live) {
         const int pos = base + __popc(bal & ((1u << lane) - 1u));
         const float4* src4 = reinterpret_cast<const float4*>(st.prep) + my_slot * 4;
         const float4 head = __ldg(src4);
         ops = (unsigned long long)(WPC * 32 * PPL) * (unsigned long long)(kind_ops(__float_as_int(head.x)) + 9);
+        my_curve = __float_as_int(head.x) == K_CURVE;
         s_prep[pos][0] = head;
         s_prep[pos][1] = __ldg(src4 + 1);
         s_prep[pos][2] = __ldg(src4 + 2);
         s_prep[pos][3] = __ldg(src4 + 3);
         s_slot[pos] = (int)(my_slot - off);
     }
-    __syncthreads();
+    const int any_curve = __syncthreads_or(my_curve);
     if (m == 0) return;
+    // The closed-form init round of 8-px tiles without curves: half a warp per candidate, 4 pixels
+    // per lane, so the candidate's terms and its reduction are shared by twice the pixels per lane.
+    // Its pixel sums run in another order than the full-warp form's (equal to float rounding), so
+    // it serves only the fit with closed-form constants, which has no reference summation to match.
+    bool half_done = false;
+    if constexpr (INIT && PPL == 2 && WPC == 1) {
+        if (closed_form && !any_curve && ts == 8) {
+            const int half = lane >> 4, sub = lane & 15;
+            const float4* src = reinterpret_cast<const float4*>(st.src) + st.px_off[t];
+            float hx[4], hy[4];
+            float3 hs[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int p = j * 16 + sub;  // an 8-px tile's 64 pixels
+                hx[j] = (float)(p & 7) + 0.5f;
+                hy[j] = (float)(p >> 3) + 0.5f;
+                const float4 a = src[p];
+                hs[j] = make_float3(a.x, a.y, a.z);
+            }
+            for (int c0 = warp * 2; c0 < m; c0 += 8) {
+                const int c = min(c0 + half, m - 1);
+                Prep P;
+                {
+                    const float4 a = s_prep[c][0], b = s_prep[c][1], cc = s_prep[c][2], d = s_prep[c][3];
+                    P.kind = __float_as_int(a.x);
+                    P.a = a.y; P.cr = a.z; P.cg = a.w; P.cb = b.x;
+                    P.q[0] = b.y; P.q[1] = b.z; P.q[2] = b.w;
+                    P.q[3] = cc.x; P.q[4] = cc.y; P.q[5] = cc.z; P.q[6] = cc.w;
+                    P.q[7] = d.x; P.q[8] = d.y; P.q[9] = d.z; P.q[10] = d.w;
+                }
+                float a[4], sr[4], sg[4], sb[4];
+                prim_eval<4>(P, hx, hy, a, sr, sg, sb, lane);  // no curve: no shuffles inside
+                float e = 0.0f;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float dr = clamp01(__fmul_rn(sr[j], a[j])) - hs[j].x;
+                    const float dg = clamp01(__fmul_rn(sg[j], a[j])) - hs[j].y;
+                    const float db = clamp01(__fmul_rn(sb[j], a[j])) - hs[j].z;
+                    e = fmaf(dr, dr, fmaf(dg, dg, fmaf(db, db, e)));
+                }
+#pragma unroll
+                for (int o = 8; o > 0; o >>= 1) e += __shfl_xor_sync(FULL, e, o);
+                if (sub == 0 && c0 + half < m) st.partial[(off + s_slot[c]) * 4] = e;
+            }
+            half_done = true;
+        }
+    }
 
     const int group = warp / WPC, wig = warp % WPC;
     const float4* src = reinterpret_cast<const float4*>(st.src) + st.px_off[t];
@@ -267,7 +316,7 @@ __device__ __forceinline__ void score_item(const WeftFitState& st, const int* __
             g[j] = make_float3(b.x, b.y, b.z);
         }
     }
-    for (int c = group; c < m; c += GROUPS) {
+    for (int c = group; !half_done && c < m; c += GROUPS) {
         Prep P;
         {
             const float4 a = s_prep[c][0], b = s_prep[c][1], cc = s_prep[c][2], d = s_prep[c][3];

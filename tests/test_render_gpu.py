@@ -158,3 +158,86 @@ def test_bad_descriptor_raises_not_falls_back():
     descs[0] = (0, 99, 0, 0, 16, 16, 16, 0, 0, 0, 0, 0)  # 99 primitives > 48
     with pytest.raises(WeftkError):
         gpu_render.gpu_render_tiles_to_image(descs, np.zeros(99, gpu_render._PRIM_DTYPE), 16, 16)
+
+
+def _const_heavy_scene(rng, qts):
+    """Mostly lone constant layers (the decoder's common tile), some longer stacks, RES0 offsets."""
+    recs = []
+    for q in qts:
+        if rng.random() < 0.8:
+            c = tuple(float(v) for v in rng.random(3).astype(np.float32))
+            stack = [Prim(0, (), c, None, float(np.float32(0.3 + 0.7 * rng.random())))]
+        else:
+            stack = [_rand_prim(rng, int(k), q.size) for k in rng.integers(0, 5, int(rng.integers(1, 4)))]
+        recs.append(Record(stack, tuple(int(v) for v in rng.integers(-20, 21, 3))))
+    return recs
+
+
+@pytest.mark.parametrize("with_res1", [False, True])
+def test_walk_constant_fill_paths_against_oracle(with_res1):
+    """The walk's whole-slot paths for lone constant tiles (with and without the RES1 grid) and the
+    per-group path for the rest, at output widths of every residue mod 4 (the slot paths need rows
+    on 16-byte boundaries, so widths not a multiple of 4 take the per-group path) and at scales that
+    split 4-pixel groups between tiles."""
+    from weft_b200 import render
+    from weft_b200.synth import make_image_linear
+
+    rng = np.random.default_rng(33)
+    # images of every width mod 4 at their own size, and a square one at scaled targets: every
+    # width mod 4 without grids; with grids only scales that keep every tile square (the reference
+    # walk refuses a RES1 grid on a non-square rect, and cannot place the edge tiles of a source
+    # whose sides are not multiples of 32 at a scaled target)
+    scaled = ((256, 256), (64, 64)) if with_res1 else ((129, 129), (130, 130), (131, 131), (200, 200), (91, 91))
+    for iw, ih, targets in ((130, 98, ((130, 98),)), (131, 99, ((131, 99),)), (129, 97, ((129, 97),)),
+                            (128, 128, ((128, 128),) + scaled)):
+        img = make_image_linear(iw, ih, 20, 4)
+        qts = oq.decompose(img, 0.08, 8, 32)
+        recs = _const_heavy_scene(rng, qts)
+        maps = [rng.integers(-60, 61, (4, 4, 3)).astype(np.float32) / 255.0 for _ in qts] if with_res1 else None
+        for tw, th in targets:
+            got = render.render_scene_adaptive(recs, qts, iw, ih, maps, 4, tw, th)
+            want = orender.render_scene_adaptive(recs, qts, iw, ih, maps, 4, tw, th)
+            assert float(np.max(np.abs(got - want))) <= RENDER_TOL, (iw, ih, tw, th)
+
+
+def test_walk_rects_partly_outside_the_image():
+    """Lone constant rects (disjoint) that start left of / above the image or end past it, rects
+    narrower than a 16-byte slot, and rects wholly outside: only in-image pixels are written, with
+    the tile's colour (blend over black + RES0, clipped); the rest of the buffer is left as it was."""
+    import torch
+
+    from weft_b200 import _lib
+    from weft_b200.gpu_render import _PRIM_DTYPE, _TILE_DECODE_DTYPE
+    from weft_b200.render import decode_items
+
+    rng = np.random.default_rng(8)
+    H, W = 61, 100
+    rects = [(-7, -3, 20, 11), (90, 50, 25, 20), (5, 20, 1, 9), (17, 33, 2, 2), (31, 2, 3, 30), (120, 5, 10, 10),
+             (4, -40, 9, 20), (-13, 45, 130, 3), (40, 10, 37, 29), (80, 0, 5, 40)]
+    n = len(rects)
+    descs = np.zeros(n, _TILE_DECODE_DTYPE)
+    prims = np.zeros(n, _PRIM_DTYPE)
+    want = np.full((H, W, 3), -1.0, np.float32)
+    for i, (x0, y0, w, h) in enumerate(rects):
+        col = rng.random(3).astype(np.float32)
+        a = np.float32(0.4 + 0.6 * rng.random())
+        res0 = (rng.integers(-20, 21, 3).astype(np.float32) / np.float32(255.0))
+        prims[i]["kind"], prims[i]["color0"], prims[i]["alpha"] = 0, col, a
+        descs[i] = (i, 1, x0, y0, w, h, 16, -1, res0[0], res0[1], res0[2], 0.0)
+        # blend over black: fma(c, a, 0 * (1 - a)) = c * a, then + RES0, clipped
+        v = np.clip((col * a).astype(np.float32) + res0, 0.0, 1.0).astype(np.float32)
+        ya, yb, xa, xb = max(0, y0), min(H, y0 + h), max(0, x0), min(W, x0 + w)
+        if ya < yb and xa < xb:
+            want[ya:yb, xa:xb] = v
+    dev = torch.device("cuda", 0)
+    lib = _lib.lib_for_device(0)
+    items = decode_items(descs, H, W, prims)
+    out = torch.full((H, W, 3), -1.0, dtype=torch.float32, device=dev)
+    t_d = torch.from_numpy(descs.view(np.uint8)).to(dev)
+    t_p = torch.from_numpy(prims.view(np.uint8)).to(dev)
+    t_i = torch.from_numpy(items).to(dev)
+    _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), n, _lib.ptr(t_i), len(items), _lib.ptr(t_p), 0, 0, 0, 0,
+                                      _lib.ptr(out), H, W, 0, torch.cuda.current_stream().cuda_stream),
+               "weftk_render_tiles")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), want)

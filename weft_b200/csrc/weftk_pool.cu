@@ -840,19 +840,18 @@ using namespace weftk;
 
 // Side streams of the current device that run the larger tile classes beside the 8-px class
 // (forked from and joined back into the caller's stream with events, so a captured graph gets
-// parallel branches).  Created on the first call on a device.
+// parallel branches).  Created on a host thread's first call on a device and kept for the life of
+// the process; per host thread, so concurrent callers never share the events.
 struct SideStreams {
     cudaStream_t s[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
 
 int side_streams(SideStreams** out) {
-    static std::mutex mu;
-    static SideStreams per_dev[64];
+    thread_local SideStreams per_dev[64];
     int dev = 0;
     WEFTK_CUDA(cudaGetDevice(&dev));
     WEFTK_REQUIRE(dev >= 0 && dev < 64, "gen_pools: device index beyond 63");
-    std::lock_guard<std::mutex> lock(mu);
     SideStreams& ss = per_dev[dev];
     if (!ss.fork) {
         for (int i = 0; i < 3; ++i) {

@@ -376,9 +376,10 @@ __device__ __forceinline__ void render_item(const int2 item, const WeftTileDecod
                        clamp01(blend(sp[0].cb, sp[0].a, 0.0f) + d.res0_b), lane);
         return;
     }
-    if (n == 1 && sp[0].kind == K_CONST) {
-        // A lone constant layer with a RES1 grid: one colour plus the bilinear grid per
-        // pixel.  Each lane steps its group (row, column) by 32 groups instead of dividing.
+    if (n == 1 && sp[0].kind == K_CONST && has_res1) {
+        // A lone constant layer with a RES1 grid on rows that are not 16-byte aligned: one colour
+        // plus the bilinear grid per pixel.  Each lane steps its group (row, column) by 32 groups
+        // instead of dividing.  (Without a grid such a tile takes the general path below.)
         const float fr = clamp01(blend(sp[0].cr, sp[0].a, 0.0f) + d.res0_r);
         const float fg = clamp01(blend(sp[0].cg, sp[0].a, 0.0f) + d.res0_g);
         const float fb = clamp01(blend(sp[0].cb, sp[0].a, 0.0f) + d.res0_b);

@@ -34,7 +34,7 @@ extern "C" {
  *   d_pixels    float4 (r, g, b, -) per pixel, tile t's side x side pixels row-major from
  *               d_px_off[t]
  *   d_size      int32 [n_tiles] tile side: 8, 16, 32 or 64
- *   d_prims     the selected stacks, WeftPrim records; tile t's are
+ *   d_prims     the selected stacks, n_prims WeftPrim records; tile t's are
  *               [d_prim_off[t], d_prim_off[t + 1])
  *   d_basis     WEFTK_BICUBIC_BASIS_DOUBLES doubles (above)
  *   lam         the fit's lambda (encoder._tile_lambda)
@@ -42,11 +42,12 @@ extern "C" {
  *   d_grid      float [n_tiles * 48]: the u8-rounded control grid, (4, 4, 3) row-major
  *   d_swap      int32 [n_tiles]: 1 where the bicubic primitive scores lower, else 0
  *   d_score     double [n_tiles * 2]: (bicubic score, stack score)
- * A tile of another side or a stack longer than 48 primitives is reported through
- * weftk_device_status (WEFTK_E_ARG) and left unwritten.  Asynchronous on `stream`.
+ * A tile of another side, a stack longer than 48 primitives or a record range outside
+ * [0, n_prims) is reported through weftk_device_status (WEFTK_E_ARG) and left unwritten.
+ * Asynchronous on `stream`.
  */
 int weftk_bicubic_swap(const float* d_pixels, const int32_t* d_px_off, const int32_t* d_size, int n_tiles,
-                       const WeftPrim* d_prims, const int32_t* d_prim_off, const double* d_basis, double lam,
+                       const WeftPrim* d_prims, int n_prims, const int32_t* d_prim_off, const double* d_basis, double lam,
                        float* d_grid, int32_t* d_swap, double* d_score, void* stream);
 
 #ifdef __cplusplus

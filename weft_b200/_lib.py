@@ -136,7 +136,7 @@ SIGNATURES: dict[str, list] = {
     "weftk_refiner_create": [_P, _P],
     "weftk_refiner_destroy": [_P],
     "weftk_refine_image": [_P, _P, _I, _I, _P, _P, _P, _I, _P, _P],
-    "weftk_bicubic_swap": [_P, _P, _P, _I, _P, _P, _P, ctypes.c_double, _P, _P, _P, _P],
+    "weftk_bicubic_swap": [_P, _P, _P, _I, _P, _I, _P, _P, ctypes.c_double, _P, _P, _P, _P],
 }
 
 _lock = threading.Lock()

@@ -62,7 +62,7 @@ def swap(src4: torch.Tensor, px_off: torch.Tensor, sizes: torch.Tensor, stacks, 
     scores = torch.empty((n, 2), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
     _lib.check(lib.weftk_bicubic_swap(_lib.ptr(src4), _lib.ptr(px_off), _lib.ptr(sizes), n, _lib.ptr(t_prims),
-                                      _lib.ptr(t_off), _lib.ptr(t_basis), float(rate.tile_lambda(quality)),
+                                      len(recs), _lib.ptr(t_off), _lib.ptr(t_basis), float(rate.tile_lambda(quality)),
                                       _lib.ptr(grid), _lib.ptr(flags), _lib.ptr(scores), stream.cuda_stream),
                "weftk_bicubic_swap")
     torch.cuda.synchronize(dev)

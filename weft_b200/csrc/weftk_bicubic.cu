@@ -35,8 +35,9 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 
 __global__ void __launch_bounds__(BC_THREADS) bicubic_swap_kernel(
     const float4* __restrict__ px, const int32_t* __restrict__ px_off, const int32_t* __restrict__ size, int n_tiles,
-    const WeftPrim* __restrict__ prims, const int32_t* __restrict__ prim_off, const double* __restrict__ basis,
-    double lam, float* __restrict__ grid_out, int32_t* __restrict__ swap_out, double* __restrict__ score_out) {
+    const WeftPrim* __restrict__ prims, int n_prims, const int32_t* __restrict__ prim_off,
+    const double* __restrict__ basis, double lam, float* __restrict__ grid_out, int32_t* __restrict__ swap_out,
+    double* __restrict__ score_out) {
     __shared__ double L[4][64][3];   // pinv(B) @ T
     __shared__ double BQ[64][4][3];  // B @ Q
     __shared__ float Q[48];
@@ -45,7 +46,7 @@ __global__ void __launch_bounds__(BC_THREADS) bicubic_swap_kernel(
     const int t = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = size[t];
     const int s0 = prim_off[t], np = prim_off[t + 1] - s0;
-    if (!(n == 8 || n == 16 || n == 32 || n == 64) || np < 0 || np > BC_MAX_PRIMS) {
+    if (!(n == 8 || n == 16 || n == 32 || n == 64) || np < 0 || np > BC_MAX_PRIMS || s0 < 0 || s0 + np > n_prims) {
         if (tid == 0) atomicCAS(&g_device_status, 0, WEFTK_E_ARG);
         return;
     }
@@ -184,17 +185,18 @@ __global__ void __launch_bounds__(BC_THREADS) bicubic_swap_kernel(
 }  // namespace weftk
 
 extern "C" int weftk_bicubic_swap(const float* d_pixels, const int32_t* d_px_off, const int32_t* d_size, int n_tiles,
-                                  const WeftPrim* d_prims, const int32_t* d_prim_off, const double* d_basis, double lam,
-                                  float* d_grid, int32_t* d_swap, double* d_score, void* stream) {
+                                  const WeftPrim* d_prims, int n_prims, const int32_t* d_prim_off,
+                                  const double* d_basis, double lam, float* d_grid, int32_t* d_swap, double* d_score,
+                                  void* stream) {
     using namespace weftk;
     if (n_tiles == 0) return WEFTK_OK;
-    WEFTK_REQUIRE(n_tiles > 0 && d_pixels && d_px_off && d_size && d_prim_off && d_basis && d_grid && d_swap &&
-                      d_score,
+    WEFTK_REQUIRE(n_tiles > 0 && n_prims >= 0 && (n_prims == 0 || d_prims) && d_pixels && d_px_off && d_size &&
+                      d_prim_off && d_basis && d_grid && d_swap && d_score,
                   "bicubic_swap: bad arguments");
     WEFTK_REQUIRE((reinterpret_cast<uintptr_t>(d_pixels) & 15) == 0, "bicubic_swap: pixels must be 16-byte aligned");
     bicubic_swap_kernel<<<n_tiles, BC_THREADS, 0, (cudaStream_t)stream>>>(
-        reinterpret_cast<const float4*>(d_pixels), d_px_off, d_size, n_tiles, d_prims, d_prim_off, d_basis, lam, d_grid,
-        d_swap, d_score);
+        reinterpret_cast<const float4*>(d_pixels), d_px_off, d_size, n_tiles, d_prims, n_prims, d_prim_off, d_basis, lam,
+        d_grid, d_swap, d_score);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }

@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include <climits>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -821,6 +822,30 @@ extern "C" int weftk_fit_run(const WeftFitState* st, int max_rounds, double lamb
     return rc;
 }
 
+// Side streams of the current device for the calling host thread: the 16-px and 32/64-px classes'
+// scoring launches run beside the 8-px class's (forked from and joined back into the caller's
+// stream, which a CUDA graph capture follows).  Created on first use, kept for the process.
+struct ClassStreams {
+    cudaStream_t s[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+};
+
+static int class_streams(ClassStreams** out) {
+    thread_local std::map<int, ClassStreams> per_device;
+    int dev = 0;
+    WEFTK_CUDA(cudaGetDevice(&dev));
+    ClassStreams& cs = per_device[dev];
+    if (cs.fork == nullptr) {
+        for (int i = 0; i < 2; ++i) {
+            WEFTK_CUDA(cudaStreamCreateWithFlags(&cs.s[i], cudaStreamNonBlocking));
+            WEFTK_CUDA(cudaEventCreateWithFlags(&cs.join[i], cudaEventDisableTiming));
+        }
+        WEFTK_CUDA(cudaEventCreateWithFlags(&cs.fork, cudaEventDisableTiming));
+    }
+    *out = &cs;
+    return WEFTK_OK;
+}
+
 extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, double complex_threshold,
                                const int32_t* d_perm, const WeftFitItem* d_items8, int n_items8,
                                const WeftFitItem* d_items16, int n_items16, const WeftFitItem* d_items32,
@@ -852,22 +877,39 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
             fit_queue_kernel<<<ceil_div(total, 256), 256, 0, s>>>(*st, d_items8, n_items8, d_items16, n_items16,
                                                                   d_items32, n_items32);
     }
+    // the size classes score disjoint tiles: the 16-px and 32/64-px classes run on side streams
+    // beside the 8-px class (not while the scoring launches are being timed)
+    ClassStreams* cs = nullptr;
+    const bool side = !g_timing.enabled && (n_items16 > 0 || n_items32 > 0) && n_items8 + n_items16 + n_items32 > 0;
+    if (side) {
+        int rc = class_streams(&cs);
+        if (rc) return rc;
+        WEFTK_CUDA(cudaEventRecord(cs->fork, s));
+        for (int i = 0; i < 2; ++i) WEFTK_CUDA(cudaStreamWaitEvent(cs->s[i], cs->fork, 0));
+    }
+    if (n_items32) {
+        g_queue_class = queued ? 2 : -1;
+        g_queue_base = n_items8 + n_items16;
+        launch_score_class32(st->variant[2], *st, d_perm, d_items32, n_items32, side ? cs->s[1] : s);
+    }
+    if (n_items16) {
+        g_queue_class = queued ? 1 : -1;
+        g_queue_base = n_items8;
+        launch_score_class16(st->variant[1], *st, d_perm, d_items16, n_items16, side ? cs->s[0] : s);
+    }
     if (n_items8) {
         g_queue_class = queued ? 0 : -1;
         g_queue_base = 0;
         launch_score_class8(st->variant[0], *st, d_perm, d_items8, n_items8, s);
     }
-    if (n_items16) {
-        g_queue_class = queued ? 1 : -1;
-        g_queue_base = n_items8;
-        launch_score_class16(st->variant[1], *st, d_perm, d_items16, n_items16, s);
-    }
-    if (n_items32) {
-        g_queue_class = queued ? 2 : -1;
-        g_queue_base = n_items8 + n_items16;
-        launch_score_class32(st->variant[2], *st, d_perm, d_items32, n_items32, s);
-    }
     g_queue_class = -1;
+    if (side) {
+        WEFTK_CUDA(cudaGetLastError());
+        for (int i = 0; i < 2; ++i) {
+            WEFTK_CUDA(cudaEventRecord(cs->join[i], cs->s[i]));
+            WEFTK_CUDA(cudaStreamWaitEvent(s, cs->join[i], 0));
+        }
+    }
     if (g_timing.enabled) {
         WEFTK_CUDA(cudaEventRecord(g_timing.stop, s));
         g_timing.pending = true;

@@ -53,7 +53,9 @@ typedef struct WeftFitState {
     int64_t n_slots;         /* candidate slots in total */
     /* tiles */
     const float* src;        /* float4 per pixel */
-    float* bg;               /* float4 per pixel: composite of the selected stack */
+    float* bg;               /* float4 per pixel: composite of the selected stack; may be NULL for a
+                                fit that runs only its init round (then nothing is composited; greedy
+                                rounds and re-seeding refuse it) */
     const int32_t* px_off;   /* [n_tiles] pixel offset of the tile */
     const int32_t* size;     /* [n_tiles] tile side: 8, 16, 32 or 64 */
     const int32_t* cap;      /* [n_tiles] primitive cap */

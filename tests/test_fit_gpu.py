@@ -200,3 +200,28 @@ def test_queue_driven_rounds_equal_per_item_launches():
     g.replay()
     assert b.selected_indices() == a.selected_indices()
     np.testing.assert_array_equal(b.objectives(), a.objectives())
+
+
+def test_init_only_fit_skips_the_composite_and_refuses_rounds():
+    """A fit declared init-only (the refined fit) leaves the composite untouched, picks what the
+    full fit's init round picks, and refuses a greedy round, which would need the composite."""
+    from weft_b200 import candidates, quadtree
+    from weft_b200._lib import WeftkError
+    from weft_b200.fit import BatchedFit
+    from weft_b200.synth import make_image_u8, srgb_u8_to_linear
+
+    u8 = make_image_u8(128, 64, 3, 3)
+    img = srgb_u8_to_linear(u8)
+    qts = quadtree.decompose(img, rule="variance", threshold=100.0, min_tile=8, max_tile=64, image_u8=u8)
+    patches = quadtree.extract_tiles(img, qts, 64)
+    pools = [[c for c in candidates.tile_candidates(p, 75) if c.kind in (0, 1)] for p in patches]
+    full = BatchedFit(patches, pools, 75, caps=[16] * len(qts)).use_closed_form_init(True)
+    full.run_init_only()
+    lean = BatchedFit(patches, pools, 75, caps=[16] * len(qts)).use_closed_form_init(True).init_only()
+    lean.t_bg.fill_(0.25)
+    lean.run_init_only()
+    assert lean.selected_indices() == full.selected_indices()
+    np.testing.assert_array_equal(lean.objectives(), full.objectives())
+    assert bool((lean.t_bg == 0.25).all())
+    with pytest.raises(WeftkError):
+        lean.run(max_rounds=1)

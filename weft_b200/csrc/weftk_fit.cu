@@ -498,7 +498,9 @@ __global__ void __launch_bounds__(128) fit_select_kernel(WeftFitState st, int mo
         st.flags[t] |= WEFTK_TILE_IMPROVED;
         atomicAdd(&st.status[1], 1);
     }
-    // Composite the accepted candidate into the tile's bg.
+    // Composite the accepted candidate into the tile's bg (a fit without one runs no round
+    // after its init round, so nothing would read it).
+    if (st.bg == nullptr) return;
     const Prep P = load_prep(st.prep, slot);
     float4* bgp = reinterpret_cast<float4*>(st.bg) + st.px_off[t];
     constexpr int U = 4;
@@ -651,6 +653,7 @@ __global__ void fit_reset_kernel(WeftFitState st, const int* __restrict__ init_c
     const long long off = st.pool_off[t];
     for (int i = threadIdx.x; i < st.pool_cap[t]; i += blockDim.x) st.alive[off + i] = 0;
     const int ts = st.size[t];
+    if (st.bg == nullptr) return;
     float4* bg = reinterpret_cast<float4*>(st.bg) + st.px_off[t];
     for (int i = threadIdx.x; i < ts * ts; i += blockDim.x) bg[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
@@ -852,6 +855,7 @@ extern "C" int weftk_fit_round(const WeftFitState* st, int mode, double lambda, 
                                int n_items32, void* stream) {
     WEFTK_REQUIRE(st && d_perm, "fit_round: null argument");
     WEFTK_REQUIRE(mode == WEFTK_FIT_INIT || mode == WEFTK_FIT_ROUND, "fit_round: bad mode");
+    WEFTK_REQUIRE(mode == WEFTK_FIT_INIT || st->bg != nullptr, "fit_round: a greedy round needs the composite (bg)");
     WEFTK_REQUIRE(n_items8 >= 0 && n_items16 >= 0 && n_items32 >= 0, "fit_round: negative item count");
     for (int c = 0; c < 3; ++c)
         WEFTK_REQUIRE(st->variant[c] >= 0 && st->variant[c] < WEFTK_FIT_VARIANTS, "fit_round: bad scoring variant");

@@ -11,6 +11,8 @@
 // bits.
 #include <cuda_runtime.h>
 
+#include <map>
+
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -373,7 +375,7 @@ extern "C" int weftk_refine_image(WeftRefiner* r, const uint8_t* h_img, int h, i
     st.cap_max = p.cap;
     st.n_slots = slots;
     st.src = static_cast<const float*>(r->src4.p);
-    st.bg = static_cast<float*>(r->bg.p);
+    st.bg = nullptr;  // only the init round runs: nothing reads a composite
     st.px_off = d_px_off;
     st.size = lay(L.size);
     st.cap = lay(L.cap);
@@ -397,9 +399,23 @@ extern "C" int weftk_refine_image(WeftRefiner* r, const uint8_t* h_img, int h, i
     st.moments = moments;
     st.queue = static_cast<int32_t*>(r->queue.p);
     st.queue_ctl = queue_ctl;
-    if ((rc = weftk_fit_moments(&st, moments, stream))) return rc;
-    if ((rc = weftk_fit_reset(&st, gen_cnt, stream))) return rc;
-    if ((rc = weftk_fit_prepare(&st, zero_first, stream))) return rc;
+    // the tiles' pixel moments beside the reset and the preparation (a side stream of this host
+    // thread, joined before the round)
+    {
+        thread_local std::map<int, std::pair<cudaStream_t, cudaEvent_t[2]>> side_of;
+        auto& sd = side_of[r->device];
+        if (sd.first == nullptr) {
+            WEFTK_CUDA(cudaStreamCreateWithFlags(&sd.first, cudaStreamNonBlocking));
+            for (int i = 0; i < 2; ++i) WEFTK_CUDA(cudaEventCreateWithFlags(&sd.second[i], cudaEventDisableTiming));
+        }
+        WEFTK_CUDA(cudaEventRecord(sd.second[0], (cudaStream_t)stream));
+        WEFTK_CUDA(cudaStreamWaitEvent(sd.first, sd.second[0], 0));
+        if ((rc = weftk_fit_moments(&st, moments, sd.first))) return rc;
+        WEFTK_CUDA(cudaEventRecord(sd.second[1], sd.first));
+        if ((rc = weftk_fit_reset(&st, gen_cnt, stream))) return rc;
+        if ((rc = weftk_fit_prepare(&st, zero_first, stream))) return rc;
+        WEFTK_CUDA(cudaStreamWaitEvent((cudaStream_t)stream, sd.second[1], 0));
+    }
     const WeftFitItem* it[3];
     for (int ci = 0; ci < 3; ++ci)
         it[ci] = L.n_items[ci] ? reinterpret_cast<const WeftFitItem*>(lay(L.items[ci])) : nullptr;

@@ -428,6 +428,6 @@ int launch_fit_reseed(const WeftFitState& st, const int* gate, cudaStream_t stre
 
 extern "C" int weftk_fit_reseed(const WeftFitState* st, int quality, void* stream) {
     (void)quality;
-    WEFTK_REQUIRE(st, "fit_reseed: null state");
+    WEFTK_REQUIRE(st && st->bg, "fit_reseed: null state or no composite (bg)");
     return launch_fit_reseed(*st, nullptr, (cudaStream_t)stream);
 }

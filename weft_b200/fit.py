@@ -463,12 +463,26 @@ class BatchedFit:
     def run_init_only(self) -> None:
         """Reset and run only the init round (best single candidate per tile), launching
         device work only: no host copies or syncs, so it can be captured in a CUDA graph.
-        With the closed-form init on, the per-tile moments are computed first."""
+        With the closed-form init on, the per-tile moments are computed beside the reset and the
+        preparation (on a side stream, joined before the round)."""
         s = self._stream()
-        self._moments()
+        joined = None
+        if self.st.moments:
+            main = torch.cuda.current_stream(self.device)
+            if not hasattr(self, "_side"):
+                self._side = torch.cuda.Stream(self.device)
+            fork = torch.cuda.Event()
+            fork.record(main)
+            self._side.wait_event(fork)
+            _lib.check(self.lib.weftk_fit_moments(ctypes_ref(self.st), self.st.moments, self._side.cuda_stream),
+                       "weftk_fit_moments")
+            joined = torch.cuda.Event()
+            joined.record(self._side)
         _lib.check(self.lib.weftk_fit_reset(ctypes_ref(self.st), _lib.ptr(self.t_init_cnt), s), "weftk_fit_reset")
         _lib.check(self.lib.weftk_fit_prepare(ctypes_ref(self.st), _lib.ptr(self.t_zero_first), s),
                    "weftk_fit_prepare")
+        if joined is not None:
+            torch.cuda.current_stream(self.device).wait_event(joined)
         ti = self.t_items
         rc = self.lib.weftk_fit_round(ctypes_ref(self.st), FIT_INIT, self.lam, self.thr, _lib.ptr(self.t_perm),
                                       _lib.ptr(ti[8]), self.n_items[8], _lib.ptr(ti[16]), self.n_items[16],
@@ -535,6 +549,13 @@ class BatchedFit:
     def graph(self, max_rounds: int | None = None) -> "FitGraph":
         """The device-driven fit captured once in a CUDA graph (replay() refits from scratch)."""
         return FitGraph(self, max_rounds)
+
+    def init_only(self) -> "BatchedFit":
+        """Declare that this fit runs only its init round (the refined fit): accepted candidates
+        are then not composited into the per-pixel composite, which nothing reads afterwards;
+        greedy rounds and re-seeding refuse such a fit."""
+        self.st.bg = None
+        return self
 
     def use_closed_form_init(self, on: bool = True) -> "BatchedFit":
         """Score constant candidates of the init round in closed form from per-tile pixel

@@ -218,7 +218,7 @@ class DeviceRefinedFit:
         mask = sum(1 << int(k) for k in self.kinds)
         self.fit = BatchedFit.from_device_pools(src4, self.sizes, self.cand, self.cnt, self.stride, quality, caps,
                                                 kinds_mask=mask)
-        self.fit.use_closed_form_init(True)
+        self.fit.use_closed_form_init(True).init_only()
         self._gen = self._generator()
         if autotune or not generate_in_run:
             self.generate()  # the autotuner times scoring launches over real pools

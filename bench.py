@@ -733,6 +733,15 @@ def differentiable_fit(args, executor, local, stream):
     fit.run()  # warm-up
     fit.reset()
     _, plain_ms = timed(fit.run)
+    parity = None
+    if not args.no_cpu:
+        # the plain fit's selections against the oracle greedy on a sample of the tiles, replaying
+        # the device fit's round decisions (as the 1024^2 line's parity)
+        schedule = [imp > 0 for mode, ev, imp in fit.stats.per_round if mode == 1 and ev > 0]
+        pick = cpu_sample(im.patches, im.pools, 2.0, executor, seed=1)
+        results: dict = {}
+        run_cpu(im.patches, im.pools, pick, executor, os.cpu_count() or 1, schedule, results)
+        parity = {k: v for k, v in fit_parity(fit, results).items() if k != "what"}
     ss, p0 = fit.stack_set()
     steps = args.diff_steps
     refine(ss, p0, steps=3, lr=1e-2)  # warm-up
@@ -749,7 +758,7 @@ def differentiable_fit(args, executor, local, stream):
             "autograd_ms_per_step": auto_ms / steps, "fused_ms_per_step": fused_ms / steps,
             "loss_first_last": [hist[0], hist[-1]] if hist else None,
             "rd_plain": rd0["rd_score"], "rd_refined": rd1["rd_score"], "rd_delta_db": rd1["rd_score"] - rd0["rd_score"],
-            "psnr_plain_db": rd0["psnr_db"], "psnr_refined_db": rd1["psnr_db"]}
+            "psnr_plain_db": rd0["psnr_db"], "psnr_refined_db": rd1["psnr_db"], "parity": parity}
 
 
 def image_batch_fit(args, executor, local, stream):
@@ -1318,6 +1327,8 @@ def run_weft(args, world, rank, local, executor, cores):
                    "raster_resize_frac": frac((raster_line or {}).get("resize")),
                    "ms": None if not decode else round(decode["ms"], 4)},
         "parity": None if parity is None else {k: parity[k] for k in ("tiles", "equal_selections", "max_obj_rel")},
+        "parity_2048": None if not diff or not diff.get("parity") else
+        {k: diff["parity"][k] for k in ("tiles", "equal_selections", "max_obj_rel")},
         "image_batch": None if ibatch is None else {k: ibatch[k] for k in (
             "n_images", "mpix", "plain_mpix_per_s", "refined_mpix_per_s", "rd_delta_db_min", "rd_delta_db_mean",
             "images_within_0.05db")},

@@ -24,6 +24,7 @@ namespace {
 constexpr int QT_MAX = 64;                       // largest macro tile side
 constexpr int QT_MAX_TILES = (QT_MAX / 8) * (QT_MAX / 8);  // tiles per macro tile, bound
 constexpr int QT_SCAN_THREADS = 1024;
+static_assert(QT_SCAN_THREADS == 32 * 32, "the placement scan is two levels of 32");
 
 __device__ __forceinline__ double lum_u8(const uint8_t* p) {
     return __dadd_rn(__dadd_rn(__dmul_rn(0.2126, (double)p[0]), __dmul_rn(0.7152, (double)p[1])),
@@ -122,26 +123,38 @@ __global__ void __launch_bounds__(QT_SCAN_THREADS) qt_place_kernel(const int32_t
                                                                    const int32_t* __restrict__ counts, int n_macro,
                                                                    int32_t* __restrict__ tiles, int max_tiles,
                                                                    int32_t* __restrict__ n_out) {
-    __shared__ int part[QT_SCAN_THREADS];
-    const int tid = threadIdx.x;
+    __shared__ int wtot[QT_SCAN_THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int per = (n_macro + QT_SCAN_THREADS - 1) / QT_SCAN_THREADS;
     const int lo = min(n_macro, tid * per), hi = min(n_macro, lo + per);
     int s = 0;
     for (int i = lo; i < hi; ++i) s += counts[i];
-    part[tid] = s;
+    // exclusive prefix sum of the threads' counts: inclusive scans in each warp, then of the
+    // warps' totals
+    int v = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) wtot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int w = wtot[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        wtot[lane] = w;
+    }
     __syncthreads();
     if (tid == 0) {
-        int run = 0;
-        for (int i = 0; i < QT_SCAN_THREADS; ++i) {
-            const int c = part[i];
-            part[i] = run;
-            run += c;
-        }
+        const int run = wtot[QT_SCAN_THREADS / 32 - 1];
         *n_out = min(run, max_tiles);
         if (run > max_tiles) atomicCAS(&g_device_status, 0, WEFTK_E_RANGE);
     }
-    __syncthreads();
-    int off = part[tid];
+    int off = v - s + (warp ? wtot[warp - 1] : 0);
     for (int i = lo; i < hi; ++i) {
         const int c = counts[i];
         for (int j = 0; j < c; ++j, ++off) {

@@ -205,46 +205,88 @@ __device__ __forceinline__ int to_u8(float v) {
     return (int)p;  // truncation, as numpy's astype(uint8)
 }
 
-__global__ void __launch_bounds__(256) resize_rows_kernel(const float* __restrict__ src, int src_w, int src_h,
-                                                          uint8_t* __restrict__ tmp, int dst_w) {
-    const long long total = (long long)src_h * dst_w;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / dst_w), xx = (int)(i - (long long)y * dst_w);
-        const Taps t = resample_taps(src_w, dst_w, xx);
+// Both passes: a CTA covers RS_COLS output columns x RS_ROWS rows.  A sample's taps (Pillow's
+// bounds and 22-bit integer weights) depend on its output column (row pass) or output row (column
+// pass) only, so they are derived once per CTA column or row and reused, not once per pixel; a
+// sample with more than RS_MAXT taps (a downscale by more than about 3.5) derives each weight where
+// it is used.  The weights are the same integers either way.
+constexpr int RS_COLS = 128, RS_ROWS = 8, RS_MAXT = 8;
+
+__global__ void __launch_bounds__(RS_COLS) resize_rows_kernel(const float* __restrict__ src, int src_w, int src_h,
+                                                              uint8_t* __restrict__ tmp, int dst_w) {
+    const int xx = blockIdx.x * RS_COLS + threadIdx.x;
+    const int y0 = blockIdx.y * RS_ROWS;
+    if (xx >= dst_w) return;
+    const Taps t = resample_taps(src_w, dst_w, xx);
+    const bool cached = t.count <= RS_MAXT;
+    int k[RS_MAXT], sx[RS_MAXT];
+#pragma unroll
+    for (int j = 0; j < RS_MAXT; ++j) {
+        k[j] = cached && j < t.count ? tap_weight(t, j) : 0;
+        sx[j] = min(t.first + j, src_w - 1);
+    }
+    for (int r = 0; r < RS_ROWS; ++r) {
+        const int y = y0 + r;
+        if (y >= src_h) break;
         int a0 = 1 << (kResampleBits - 1), a1 = a0, a2 = a0;
         const float* row = src + (long long)y * src_w * 3;
-        for (int x = 0; x < t.count; ++x) {
-            const int sx = min(t.first + x, src_w - 1);
-            const int k = tap_weight(t, x);
-            a0 += to_u8(row[sx * 3 + 0]) * k;
-            a1 += to_u8(row[sx * 3 + 1]) * k;
-            a2 += to_u8(row[sx * 3 + 2]) * k;
+        if (cached) {
+#pragma unroll
+            for (int j = 0; j < RS_MAXT; ++j) {
+                if (j < t.count) {
+                    const float* q = row + sx[j] * 3;
+                    a0 += to_u8(q[0]) * k[j];
+                    a1 += to_u8(q[1]) * k[j];
+                    a2 += to_u8(q[2]) * k[j];
+                }
+            }
+        } else {
+            for (int x = 0; x < t.count; ++x) {
+                const int s = min(t.first + x, src_w - 1);
+                const int w = tap_weight(t, x);
+                a0 += to_u8(row[s * 3 + 0]) * w;
+                a1 += to_u8(row[s * 3 + 1]) * w;
+                a2 += to_u8(row[s * 3 + 2]) * w;
+            }
         }
-        uint8_t* o = tmp + i * 3;
+        uint8_t* o = tmp + ((long long)y * dst_w + xx) * 3;
         o[0] = (uint8_t)clip8(a0);
         o[1] = (uint8_t)clip8(a1);
         o[2] = (uint8_t)clip8(a2);
     }
 }
 
-__global__ void __launch_bounds__(256) resize_cols_kernel(const uint8_t* __restrict__ tmp, int src_h, int dst_w,
-                                                          float* __restrict__ dst, int dst_h) {
-    const long long total = (long long)dst_h * dst_w;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int yy = (int)(i / dst_w), xx = (int)(i - (long long)yy * dst_w);
-        const Taps t = resample_taps(src_h, dst_h, yy);
+__global__ void __launch_bounds__(RS_COLS) resize_cols_kernel(const uint8_t* __restrict__ tmp, int src_h, int dst_w,
+                                                              float* __restrict__ dst, int dst_h) {
+    __shared__ int s_first[RS_ROWS], s_count[RS_ROWS], s_k[RS_ROWS][RS_MAXT];
+    __shared__ Taps s_taps[RS_ROWS];
+    const int xx = blockIdx.x * RS_COLS + threadIdx.x;
+    const int y0 = blockIdx.y * RS_ROWS;
+    // the CTA's output rows' taps, once
+    if (threadIdx.x < RS_ROWS && y0 + (int)threadIdx.x < dst_h) {
+        const int r = threadIdx.x;
+        const Taps t = resample_taps(src_h, dst_h, y0 + r);
+        s_taps[r] = t;
+        s_first[r] = t.first;
+        s_count[r] = t.count;
+        for (int j = 0; j < RS_MAXT; ++j) s_k[r][j] = t.count <= RS_MAXT && j < t.count ? tap_weight(t, j) : 0;
+    }
+    __syncthreads();
+    if (xx >= dst_w) return;
+    for (int r = 0; r < RS_ROWS; ++r) {
+        const int yy = y0 + r;
+        if (yy >= dst_h) break;
+        const int first = s_first[r], count = s_count[r];
         int a0 = 1 << (kResampleBits - 1), a1 = a0, a2 = a0;
-        for (int y = 0; y < t.count; ++y) {
-            const int sy = min(t.first + y, src_h - 1);
-            const int k = tap_weight(t, y);
+        for (int y = 0; y < count; ++y) {
+            const int sy = min(first + y, src_h - 1);
+            const int k = count <= RS_MAXT ? s_k[r][y] : tap_weight(s_taps[r], y);
             const uint8_t* p = tmp + ((long long)sy * dst_w + xx) * 3;
             a0 += (int)p[0] * k;
             a1 += (int)p[1] * k;
             a2 += (int)p[2] * k;
         }
-        float* o = dst + i * 3;
+        float* o = dst + ((long long)yy * dst_w + xx) * 3;
         o[0] = __fdiv_rn((float)clip8(a0), 255.0f);
         o[1] = __fdiv_rn((float)clip8(a1), 255.0f);
         o[2] = __fdiv_rn((float)clip8(a2), 255.0f);
@@ -318,9 +360,12 @@ extern "C" int weftk_raster_resize(const float* d_src, int src_w, int src_h, flo
                       dst_w <= 65535 && dst_h <= 65535,
                   "raster_resize: sizes must be in 1..65535");
     cudaStream_t s = (cudaStream_t)stream;
-    resize_rows_kernel<<<grid_for((long long)src_h * dst_w), 256, 0, s>>>(d_src, src_w, src_h, d_tmp, dst_w);
+    const dim3 grid_r(ceil_div(dst_w, RS_COLS), ceil_div(src_h, RS_ROWS));
+    const dim3 grid_c(ceil_div(dst_w, RS_COLS), ceil_div(dst_h, RS_ROWS));
+    WEFTK_REQUIRE(grid_r.y <= 65535 && grid_c.y <= 65535, "raster_resize: image too tall");
+    resize_rows_kernel<<<grid_r, RS_COLS, 0, s>>>(d_src, src_w, src_h, d_tmp, dst_w);
     WEFTK_CUDA(cudaGetLastError());
-    resize_cols_kernel<<<grid_for((long long)dst_h * dst_w), 256, 0, s>>>(d_tmp, src_h, dst_w, d_dst, dst_h);
+    resize_cols_kernel<<<grid_c, RS_COLS, 0, s>>>(d_tmp, src_h, dst_w, d_dst, dst_h);
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;
 }

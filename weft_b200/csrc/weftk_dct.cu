@@ -15,6 +15,7 @@
 // output column) writes the 8-bit intermediate; pass 2 (one thread per output pixel) reads it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/weftk_dct.h"
@@ -340,7 +341,10 @@ extern "C" int weftk_dct_apply(const WeftDctTile* d_tiles, int n_tiles, const in
         const size_t smem = (size_t)max_size * max_size * (2 * sizeof(double) + 3 * sizeof(float));
         WEFTK_CUDA(cudaFuncSetAttribute(dct_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const double step = (double)quant_step;
-        dct_apply_kernel<<<n_tiles, 256, smem, s>>>(d_tiles, n_tiles, d_coeffs, (long long)n_coeffs, chroma_mode,
+        // a CTA of one thread per pixel of the launch's largest tile, at most 256: small tiles leave
+        // no threads idle and more of their CTAs stay resident (every loop strides by blockDim.x)
+        const int threads = std::min(256, std::max(32, max_size * max_size));
+        dct_apply_kernel<<<n_tiles, threads, smem, s>>>(d_tiles, n_tiles, d_coeffs, (long long)n_coeffs, chroma_mode,
                                                     band_layout, step, step * 1.5, (double)freq_alpha, max_size,
                                                     d_image, width, height);
         WEFTK_CUDA(cudaGetLastError());

@@ -167,14 +167,15 @@ __global__ void __launch_bounds__(QT_SCAN_THREADS) qt_place_kernel(const int32_t
     }
 }
 
-__global__ void __launch_bounds__(256) extract_tiles_kernel(const uint8_t* __restrict__ img, int h, int w,
-                                                            const float* __restrict__ lut,
-                                                            const int32_t* __restrict__ tiles, int n_tiles,
-                                                            const int32_t* __restrict__ px_off,
-                                                            float4* __restrict__ out) {
-    __shared__ float tab[256];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) tab[i] = lut[i];
-    __syncthreads();
+// one CTA of EX_THREADS per tile (most tiles are 8 px: 64 pixels); the 1 KB sRGB table is read
+// through the read-only cache
+constexpr int EX_THREADS = 64;
+
+__global__ void __launch_bounds__(EX_THREADS) extract_tiles_kernel(const uint8_t* __restrict__ img, int h, int w,
+                                                                   const float* __restrict__ tab,
+                                                                   const int32_t* __restrict__ tiles, int n_tiles,
+                                                                   const int32_t* __restrict__ px_off,
+                                                                   float4* __restrict__ out) {
     const int t = blockIdx.x;
     const int tx = tiles[t * 3], ty = tiles[t * 3 + 1], s = tiles[t * 3 + 2];
     if (s < 1 || s > 64) {
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(256) extract_tiles_kernel(const uint8_t* __res
     for (int i = threadIdx.x; i < s * s; i += blockDim.x) {
         const int yy = min(ty + i / s, h - 1), xx = min(tx + i % s, w - 1);
         const uint8_t* p = img + ((size_t)yy * w + xx) * 3;
-        dst[i] = make_float4(tab[p[0]], tab[p[1]], tab[p[2]], 0.0f);
+        dst[i] = make_float4(__ldg(tab + p[0]), __ldg(tab + p[1]), __ldg(tab + p[2]), 0.0f);
     }
 }
 
@@ -230,7 +231,7 @@ extern "C" int weftk_extract_tiles(const uint8_t* d_img, int h, int w, const flo
     WEFTK_REQUIRE(h > 0 && w > 0 && n_tiles >= 0, "extract_tiles: bad size");
     if (n_tiles == 0) return WEFTK_OK;
     WEFTK_REQUIRE(d_img && d_lut && d_tiles && d_px_off && d_src4, "extract_tiles: null pointer");
-    extract_tiles_kernel<<<n_tiles, 256, 0, (cudaStream_t)stream>>>(d_img, h, w, d_lut, d_tiles, n_tiles, d_px_off,
+    extract_tiles_kernel<<<n_tiles, EX_THREADS, 0, (cudaStream_t)stream>>>(d_img, h, w, d_lut, d_tiles, n_tiles, d_px_off,
                                                                      reinterpret_cast<float4*>(d_src4));
     WEFTK_CUDA(cudaGetLastError());
     return WEFTK_OK;

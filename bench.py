@@ -208,6 +208,9 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+B2B_LAUNCHES, B2B_BUFFERS = 9, 3
+
+
 def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=None):
     """Decoder primitive walk of the fitted stacks at out_w x out_h (one launch renders the image),
     with each tile's RES0 offset and RES1 grid (computed from ``patches`` as the encoder does)
@@ -215,7 +218,9 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
 
     Each launch is timed alone with CUDA events; a 256 MiB buffer is written between launches so the
     99.5 MB output is not served from L2, and a short GPU sleep after it keeps the stream busy while
-    the host enqueues the timed launch (host launch latency is not counted).
+    the host enqueues the timed launch (host launch latency is not counted).  ``back_to_back`` times
+    the same launch in the steady state of a frame-after-frame decoder (rotating output buffers
+    larger than L2 together, one event pair around all launches).
     """
     import ctypes
 
@@ -254,10 +259,10 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
     lib = _lib.lib_for_device(dev.index)
     stream = torch.cuda.current_stream()
 
-    def launch():
+    def launch(o=out):
         _lib.check(lib.weftk_render_tiles(_lib.ptr(t_d), len(descs), _lib.ptr(t_i), len(items), _lib.ptr(t_p),
                                           _lib.ptr(t_c), len(cp48), _lib.ptr(t_r) if n_res1 else 0, n_res1,
-                                          _lib.ptr(out), th, tw, 0,
+                                          _lib.ptr(o), th, tw, 0,
                                           stream.cuda_stream), "weftk_render_tiles")
 
     for _ in range(3):
@@ -284,6 +289,24 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
         torch.cuda.synchronize()
         fill_times.append(a.elapsed_time(b))
     fill_ms = statistics.median(fill_times)
+    # steady state, as a decoder rendering one frame after another: B2B_LAUNCHES launches back to
+    # back into three rotating output buffers (3 x 99.5 MB at 3840x2160, more than L2, so no
+    # launch finds its buffer in L2), one event pair around all of them; the fixed cost of an event
+    # pair and a launch (an empty kernel measures about 6 us this way) is paid once, not per launch
+    outs = [out] + [torch.empty_like(out) for _ in range(B2B_BUFFERS - 1)]
+    b2b, b2b_fill = [], []
+    for _ in range(max(3, iters // 2)):
+        for fn, acc in ((launch, b2b), (lambda o: o.fill_(0.5), b2b_fill)):
+            flush.fill_(1.0)
+            torch.cuda._sleep(1000000)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for i in range(B2B_LAUNCHES):
+                fn(outs[i % B2B_BUFFERS])
+            b.record(stream)
+            torch.cuda.synchronize()
+            acc.append(a.elapsed_time(b) / B2B_LAUNCHES)
+    del outs
     launch()  # the timed output, not the fill, is what the status check follows
     torch.cuda.synchronize()
     st = ctypes.c_int(0)
@@ -300,6 +323,11 @@ def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=N
             "fill_reference": {"ms": fill_ms, "gbs": 12 * tw * th / (fill_ms * 1e-3) / 1e9,
                                "what": "torch fill_ of the same output buffer, timed the same way"},
             "frac_of_fill": (12 * tw * th / (ms * 1e-3)) / (12 * tw * th / (fill_ms * 1e-3)),
+            "back_to_back": {"ms": statistics.median(b2b), "frac": nbytes / (statistics.median(b2b) * 1e-3) / 1e9 / peak_gbs,
+                             "fill_ms": statistics.median(b2b_fill), "launches": B2B_LAUNCHES,
+                             "buffers": B2B_BUFFERS,
+                             "what": "launches back to back into rotating output buffers larger than L2 together, "
+                                     "one event pair around them; ms per launch"},
             "l2": "256 MiB written between timed launches", "tiles": len(descs), "prims": int(len(prims)),
             "residuals": "RES0 + RES1 grids" if n_res1 else "none"}
 
@@ -1324,6 +1352,8 @@ def run_weft(args, world, rank, local, executor, cores):
                       "host_gen_s": {"constlin": cl_gen_s, "full": gen_s, "processes": cores},
                       "device_pools_equal_host": f"{pools_equal}/{len(tiles)} tiles"},
         "decode": {"frac": frac(decode), "frac_with_residuals": frac(decode_res),
+                   "frac_back_to_back": frac((decode or {}).get("back_to_back")),
+                   "frac_with_residuals_back_to_back": frac((decode_res or {}).get("back_to_back")),
                    "raster_resize_frac": frac((raster_line or {}).get("resize")),
                    "ms": None if not decode else round(decode["ms"], 4)},
         "parity": None if parity is None else {k: parity[k] for k in ("tiles", "equal_selections", "max_obj_rel")},

@@ -403,16 +403,23 @@ __global__ void __launch_bounds__(128, MINB) fit_score_queue_kernel(WeftFitState
                                                               int expect_max, bool mode_init) {
     __shared__ ScoreSmem<WPC> sm;
     __shared__ int s_i;
+    if (threadIdx.x == 0) s_i = atomicAdd(q_next, 1);
+    __syncthreads();
+    const int len = *q_len;
     for (;;) {
-        if (threadIdx.x == 0) s_i = atomicAdd(q_next, 1);
-        __syncthreads();
         const int i = s_i;
-        if (i >= *q_len) break;
+        if (i >= len) break;
+        // the next pull is issued now and its result consumed only after this item, so the
+        // atomic's round trip overlaps the scoring
+        int next = 0;
+        if (threadIdx.x == 0) next = atomicAdd(q_next, 1);
         if (mode_init)
             score_item<PPL, WPC, true>(st, perm, items[q_items[i]], expect_min, expect_max, true, sm);
         else
             score_item<PPL, WPC, false>(st, perm, items[q_items[i]], expect_min, expect_max, false, sm);
-        __syncthreads();  // the item's shared buffers are free before the next pull
+        __syncthreads();  // every thread has read s_i and the item's shared buffers are free
+        if (threadIdx.x == 0) s_i = next;
+        __syncthreads();
     }
 }
 

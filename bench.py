@@ -210,6 +210,13 @@ class ClockSampler:
 
 B2B_LAUNCHES, B2B_BUFFERS = 9, 3
 
+# DRAM bytes (read + write) of one init round's three scoring launches and of one refine launch
+# pair (constant + tiles kernels), 1024^2 workload, from one ncu capture of the eager pipeline
+INIT_ROUND_TRAFFIC = 82_512_384 + 2_255_104
+REFINE_TRAFFIC = 1_919_232 + 930_048
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, summed over the kernel's launches "
+                  "(python bench.py --profile-refined --steps 1 --warmup 1)")
+
 
 def decode_bench(fit, tiles, width, height, out_w, out_h, iters, peak, patches=None):
     """Decoder primitive walk of the fitted stacks at out_w x out_h (one launch renders the image),
@@ -1266,12 +1273,14 @@ def run_weft(args, world, rank, local, executor, cores):
                   "candidate_pixels_per_step": cand_px // args.steps}
     fp32_src = "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)"
     refine_roof = {"bound": "fp32", "achieved": d_refine_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
-                   "frac": d_refine_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+                   "frac": d_refine_tflops / peak_tflops if peak_tflops else None, "traffic": REFINE_TRAFFIC,
+                   "traffic_source": TRAFFIC_SOURCE,
                    "kernel": "refine_tiles_kernel (loss + gradient + Adam; all steps of a fit in one launch)",
                    "peak_source": fp32_src, "ms": dbd["refine_ms"], "adam_steps_per_launch": args.refine_steps,
                    "flops_per_adam_step": d_flops}
     init_roof = {"bound": "fp32", "achieved": d_init_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
-                 "frac": d_init_tflops / peak_tflops if peak_tflops else None, "traffic": None,
+                 "frac": d_init_tflops / peak_tflops if peak_tflops else None, "traffic": INIT_ROUND_TRAFFIC,
+                 "traffic_source": TRAFFIC_SOURCE,
                  "kernel": "fit_score_kernel, init round of the refined fit", "ms": dbd["init_score_ms"],
                  "launches": dbd["init_score_launches"], "peak_source": fp32_src}
     n_cand = int(sum(len(p) for p in dev_cl))

@@ -209,6 +209,7 @@ class ClockSampler:
 
 
 B2B_LAUNCHES, B2B_BUFFERS = 9, 3
+INIT_SAMPLES = 5
 
 # DRAM bytes (read + write) of one init round's three scoring launches and of one refine launch
 # pair (constant + tiles kernels), 1024^2 workload, from one ncu capture of the eager pipeline
@@ -697,11 +698,16 @@ def device_breakdown(args, drf, lib, stream) -> dict:
     b.record(stream)
     torch.cuda.synchronize()
     gen_ms = a.elapsed_time(b)
-    lib.weftk_fit_timing(1, None, None)
-    drf.fit.run_init_only()
-    torch.cuda.synchronize()
-    score_ms, n_score = ctypes.c_double(0), ctypes.c_int(0)
-    lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
+    # the init round's scoring launches, median of INIT_SAMPLES eager runs (each run resets the
+    # fit and its work counters, so every sample is one round)
+    samples = []
+    for _ in range(INIT_SAMPLES):
+        lib.weftk_fit_timing(1, None, None)
+        drf.fit.run_init_only()
+        torch.cuda.synchronize()
+        score_ms, n_score = ctypes.c_double(0), ctypes.c_int(0)
+        lib.weftk_fit_timing(0, ctypes.addressof(score_ms), ctypes.addressof(n_score))
+        samples.append(score_ms.value)
     fr = drf.rf.refiner
     fr.restart(drf.rf.start)
     torch.cuda.synchronize()
@@ -710,7 +716,8 @@ def device_breakdown(args, drf, lib, stream) -> dict:
     fr.run(args.refine_steps)
     b.record(stream)
     torch.cuda.synchronize()
-    return {"gen_ms": gen_ms, "init_score_ms": score_ms.value, "init_score_launches": n_score.value,
+    return {"gen_ms": gen_ms, "init_score_ms": statistics.median(samples), "init_score_samples": samples,
+            "init_score_launches": n_score.value,
             "refine_ms": a.elapsed_time(b), "work": drf.fit.work_counters()}
 
 
@@ -1282,6 +1289,7 @@ def run_weft(args, world, rank, local, executor, cores):
                  "frac": d_init_tflops / peak_tflops if peak_tflops else None, "traffic": INIT_ROUND_TRAFFIC,
                  "traffic_source": TRAFFIC_SOURCE,
                  "kernel": "fit_score_kernel, init round of the refined fit", "ms": dbd["init_score_ms"],
+                 "ms_samples": [round(v, 4) for v in dbd["init_score_samples"]],
                  "launches": dbd["init_score_launches"], "peak_source": fp32_src}
     n_cand = int(sum(len(p) for p in dev_cl))
     gen_bytes = 16 * n_px + 60 * n_cand + 4 * len(tiles)

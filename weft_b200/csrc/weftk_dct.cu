@@ -8,11 +8,12 @@
 // added to the image and clipped.  The transform is the orthonormal DCT-III written as a
 // matrix product with the DCT-II basis A[k][x] = c_k cos(pi (2x + 1) k / (2n)).
 //
-// Resize: Pillow's ImagingResample for 8-bit images.  Each thread derives its own output
-// pixel's taps (bounds, float64 triangle weights normalised by their sum, rounded to 22-bit
-// fixed point) exactly as Pillow's precompute_coeffs / normalize_coeffs_8bpc do, then
-// accumulates in int32 and rounds with the same clip.  Pass 1 (one thread per source row and
-// output column) writes the 8-bit intermediate; pass 2 (one thread per output pixel) reads it.
+// Resize: Pillow's ImagingResample for 8-bit images.  A sample's taps (bounds, float64 triangle
+// weights normalised by their sum, rounded to 22-bit fixed point) are derived exactly as Pillow's
+// precompute_coeffs / normalize_coeffs_8bpc do, once per CTA column (pass 1) or output row
+// (pass 2), then accumulated in int32 and rounded with the same clip.  Pass 1 (a thread per output
+// column over 8 source rows) writes the 8-bit intermediate; pass 2 (a thread per output column
+// over 8 output rows) reads it.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -1288,7 +1288,7 @@ def run_weft(args, world, rank, local, executor, cores):
     init_roof = {"bound": "fp32", "achieved": d_init_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
                  "frac": d_init_tflops / peak_tflops if peak_tflops else None, "traffic": INIT_ROUND_TRAFFIC,
                  "traffic_source": TRAFFIC_SOURCE,
-                 "kernel": "fit_score_kernel, init round of the refined fit", "ms": dbd["init_score_ms"],
+                 "kernel": "fit_score_queue_kernel, init round of the refined fit (three tile-size classes)", "ms": dbd["init_score_ms"],
                  "ms_samples": [round(v, 4) for v in dbd["init_score_samples"]],
                  "launches": dbd["init_score_launches"], "peak_source": fp32_src}
     n_cand = int(sum(len(p) for p in dev_cl))

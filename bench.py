@@ -1274,7 +1274,7 @@ def run_weft(args, world, rank, local, executor, cores):
         decode["cpu_baseline"] = dec_cpu
     score_roof = {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops, "unit": "TFLOP/s",
                   "frac": achieved_tflops / peak_tflops if peak_tflops else None, "traffic": None,
-                  "kernel": "fit_score_kernel (3 tile-size classes), plain fit",
+                  "kernel": "fit_score_queue_kernel (3 tile-size classes, all rounds), plain fit",
                   "peak_source": "measured FMA-loop probe on this GPU (weftk_measure_fp32_peak)",
                   "score_ms_per_step": score_ms.value / args.steps, "score_launches": n_score.value,
                   "candidate_pixels_per_step": cand_px // args.steps}

@@ -154,7 +154,11 @@ class Refiner:
         p = self.params
         cap = (-(-h // p.max_tile)) * (-(-w // p.max_tile)) * (p.max_tile // p.min_tile) ** 2
         if self._out is None or self._cap_tiles < cap:
-            self._out = (np.empty((cap, 3), np.int32), np.empty((cap, 16), np.float32), np.empty(cap, np.int32))
+            # page-locked, so the results come back by DMA (the caller gets copies of them)
+            self._out_t = (torch.empty((cap, 3), dtype=torch.int32, pin_memory=True),
+                           torch.empty((cap, 16), dtype=torch.float32, pin_memory=True),
+                           torch.empty(cap, dtype=torch.int32, pin_memory=True))
+            self._out = tuple(t.numpy() for t in self._out_t)
             self._cap_tiles = cap
         tiles, rows, kinds = self._out
         n = ctypes.c_int(0)

@@ -57,7 +57,8 @@ int weftk_refiner_destroy(WeftRefiner* refiner);
  * Refine one h x w x 3 sRGB u8 image (host memory, row-major; page-locked copies fastest).
  * On success *n_tiles tiles were written: h_tiles int32[n][3] (x, y, side) in the quadtree's
  * order, h_rows float32[n][16] the refined primitive of each tile on the wire grid
- * (weftk_refine.h row layout), h_kinds int32[n] its kind (-1: none).  More than max_tiles
+ * (weftk_refine.h row layout), h_kinds int32[n] its kind (-1: none); page-locked h_rows and
+ * h_kinds come back by DMA, faster than pageable ones.  More than max_tiles
  * tiles: WEFTK_E_RANGE with *n_tiles set and nothing written.  Device work on `stream`;
  * returns after the results are on the host.
  */

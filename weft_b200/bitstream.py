@@ -27,6 +27,12 @@ import numpy as np
 
 MAGIC = b"WEFT"
 MAJOR, MINOR = 1, 4
+
+
+class BitstreamError(ValueError):
+    """A malformed WEFT file (the reference's ``weft.bitstream.BitstreamError``,
+    src/weft/bitstream.py:44; the same checks in the same order as its ``decode_weft``,
+    :839-870, ``_unpack_head`` :177-200 and ``_unpack_toc`` :222-233)."""
 FLAG_DETERMINISTIC, FLAG_HAS_RES0, FLAG_HAS_RES1, FLAG_CHUNKED_PRIM = 1, 2, 4, 8
 FLAG_HAS_DCT = 1 << 9
 PROB_BITS = 12
@@ -308,24 +314,49 @@ def ctypes_addr_of(v) -> int:
 
 
 def decode_weft(blob: bytes, device: int | None = None) -> WeftFile:
-    """Parse a WEFT file; with ``device`` the PRIM chunks are entropy-decoded on that GPU."""
+    """Parse a WEFT file; with ``device`` the PRIM chunks are entropy-decoded on that GPU.
+    A malformed file raises ``BitstreamError``."""
+    if len(blob) < 12:
+        raise BitstreamError("truncated file header")
     magic, major, minor, n_blocks, _ = struct.unpack_from("<4sBBHI", blob, 0)
-    if magic != MAGIC or major != MAJOR:
-        raise ValueError("not a WEFT v1 file")
+    if magic != MAGIC:
+        raise BitstreamError("invalid magic")
+    if major != MAJOR:
+        raise BitstreamError(f"unsupported major version: {major}")
+    if 12 + 20 * n_blocks > len(blob):
+        raise BitstreamError("truncated block directory")
     blocks = {}
     off = 12
     for _ in range(n_blocks):
         tag, b_off, b_len = struct.unpack_from("<4sQQ", blob, off)
         off += 20
         if b_off + b_len > len(blob):
-            raise ValueError("block extends past EOF")
+            raise BitstreamError("block extends past EOF")
         blocks[tag] = blob[b_off:b_off + b_len]
+    for tag in (b"HEAD", b"TOC ", b"PRIM", b"META", b"QTRE"):
+        if tag not in blocks:
+            raise BitstreamError(f"missing required block: {tag.decode('ascii').strip()}")
     for tag in blocks:
         if blocks[tag][:4] == b"\x28\xb5\x2f\xfd":
-            raise ValueError("zstd-compressed blocks are not supported")
-    w, h, _ts, _mp, _cs, _qm, flags, _tc, _tr, quality, _pid, _ = struct.unpack("<IIHHBBHIIBBH", blocks[b"HEAD"])
-    n_toc = struct.unpack_from("<I", blocks[b"TOC "], 0)[0]
-    toc = list(np.frombuffer(blocks[b"TOC "], "<u4", n_toc, 4).astype(np.int64))
+            raise BitstreamError("zstd-compressed blocks are not supported")
+    if len(blocks[b"HEAD"]) != struct.calcsize("<IIHHBBHIIBBH"):
+        raise BitstreamError("invalid HEAD size")
+    w, h, ts, mp, _cs, _qm, flags, _tc, _tr, quality, _pid, _ = struct.unpack("<IIHHBBHIIBBH", blocks[b"HEAD"])
+    if w <= 0 or h <= 0:
+        raise BitstreamError("invalid dimensions")
+    if ts <= 0 or ts > 64:
+        raise BitstreamError("invalid tile size")
+    if mp <= 0 or mp > 255:
+        raise BitstreamError("invalid max primitives")
+    toc_b = blocks[b"TOC "]
+    if len(toc_b) < 4:
+        raise BitstreamError("truncated TOC")
+    n_toc = struct.unpack_from("<I", toc_b, 0)[0]
+    if len(toc_b) != 4 + 4 * n_toc:
+        raise BitstreamError("invalid TOC length")
+    toc = list(np.frombuffer(toc_b, "<u4", n_toc, 4).astype(np.int64))
+    if any(b < a for a, b in zip(toc, toc[1:])):
+        raise BitstreamError("TOC offsets must be monotonic")
     prim = blocks[b"PRIM"]
     if b"CIDX" in blocks and device is not None:
         nc = struct.unpack_from("<I", blocks[b"CIDX"], 0)[0]
@@ -338,7 +369,7 @@ def decode_weft(blob: bytes, device: int | None = None) -> WeftFile:
             _st, _tc2, ro, rl, co, cl = struct.unpack_from("<IIIIII", blocks[b"CIDX"], 4 + 24 * i)
             part = decode_bytes(prim[co:co + cl])
             if len(part) != rl:
-                raise ValueError("chunk length mismatch")
+                raise BitstreamError("chunk length mismatch")
             raw[ro:ro + rl] = part
         prim_raw = bytes(raw)
     else:
@@ -355,7 +386,7 @@ def decode_weft(blob: bytes, device: int | None = None) -> WeftFile:
     qtree = [struct.unpack_from("<HHB", blocks[b"QTRE"], 4 + 5 * i) for i in range(qn)]
     meta = json.loads(blocks[b"META"][4:].decode())
     if (flags & FLAG_HAS_DCT) and b"DCT " not in blocks:
-        raise ValueError("HEAD indicates DCT but DCT block is missing")
+        raise BitstreamError("HEAD indicates DCT but DCT block is missing")
     return WeftFile(w, h, quality, toc, prim_raw, residuals, res1, qtree, meta, blocks.get(b"DCT "))
 
 

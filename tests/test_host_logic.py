@@ -101,3 +101,39 @@ def test_init_kinds_mask_matches_kinds_mask_of():
         f = BatchedFit.__new__(BatchedFit)
         f._init_kinds = k
         assert f.init_kinds_mask() == kinds_mask_of(f.init_kinds()), k
+
+
+def test_tile_lambda_branches():
+    """The reference's locked-down λ(q) properties (tests/test_rd_scoring.py): base (101 - q)^2 / 1e4
+    times 0.0002 from q = 90, times 0.001 below; a cliff at 90 and monotone within each branch."""
+    import pytest
+
+    from weft_b200 import rate
+
+    for q in (95, 90):
+        assert rate.tile_lambda(q) == pytest.approx(((101 - q) / 100.0) ** 2 * 0.0002, rel=1e-9)
+    for q in (89, 75, 50):
+        assert rate.tile_lambda(q) == pytest.approx(((101 - q) / 100.0) ** 2 * 0.001, rel=1e-9)
+    assert rate.tile_lambda(89) / rate.tile_lambda(90) > 2.0
+    assert all(rate.tile_lambda(q) >= rate.tile_lambda(q + 1) for q in range(50, 89))
+    assert all(rate.tile_lambda(q) >= rate.tile_lambda(q + 1) for q in range(90, 100))
+
+
+def test_bicubic_basis_and_exact_fits():
+    """The reference's bicubic properties (tests/test_bicubic.py) for the basis table the swap
+    kernel reads and for the oracle fit it is checked against: every Bernstein row sums to 1, a
+    constant tile and a linear gradient are fitted exactly."""
+    from oracle import bicubic as obic
+    from oracle import render as orender
+    from weft_b200 import bicubic
+
+    tab = bicubic.basis_table()
+    for n in bicubic.SIDES:
+        B = tab[12 * (n - 8) + 8 * n:12 * (n - 8) + 12 * n].reshape(n, 4)
+        assert np.allclose(B.sum(axis=1), 1.0, atol=1e-10)
+        assert np.array_equal(B, orender.bernstein_basis(n))
+    tile = np.full((16, 16, 3), 0.4, dtype=np.float32)
+    assert np.allclose(orender.bicubic_tile(obic.fit_tile(tile), 16), tile, atol=1e-5)
+    yy, xx = np.mgrid[0:16, 0:16].astype(np.float32) / 15
+    tile = np.stack([xx, yy, np.zeros_like(xx)], axis=-1)
+    assert np.max(np.abs(orender.bicubic_tile(obic.fit_tile(tile), 16) - tile)) < 1e-4
